@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Benchmark of the EU3D reacting-Euler timestep on B200.
+
+Workload: the 3-D reacting shock-bubble case, 256 x 128 x 128 nodes over
+64 x 32 x 32 mm (4,194,304 cells), H2_JA919 kinetics (9 species, 19 reactions),
+Mach 2.83 shock in N2 at 101.325 kPa / 300 K hitting a perturbed 2H2+O2 sphere
+(radius 8 mm, seed 3), fixed dt from the reference's CFL rule at 0.5 on the
+initial state. Synthetic inputs built by eu3d_cases.shock_bubble.
+
+A step is one full timestep: RSBI ghost fill, MUSCL/AUSM flux divergence in x,
+y, z with the explicit update, state recovery with Newton temperature
+inversion, Nchem prediction and the adaptive trapezoid kinetics.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0 (see the keys below). Multi-GPU runs (torchrun, one
+rank per GPU) advance independent replicas of the workload: the timestep has
+no exchange between instances, so per-GPU work is fixed ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "eu3d-gpu_b200"))
+
+import eu3d  # noqa: E402
+import eu3d_cases as cases  # noqa: E402
+
+METRIC = "Mcell-steps/s reacting, learned+mixed vs plain FP64 on same B200 at ≤1e-3 Y err"
+GRID = (256, 128, 128)
+EXTENT = (0.0, 0.064, 0.0, 0.032, 0.0, 0.032)
+CFL = 0.5
+L2_BYTES = 126 * 2 ** 20
+# Algorithmic bytes per cell-step of the flux + update kernel: 16 primitives
+# read, 13 conserved read and written (FP64); FP32 primitives in mixed mode.
+FLUX_BYTES = {"fp64": (16 + 26) * 8, "mixed": 16 * 4 + 26 * 8}
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = str(device_index)
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(prefix="eu3d_clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", self.idx, "-lms", "100"], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def build_workload(grid, seed=3):
+    ni, nj, nk = grid
+    x = cases.node_coordinates(ni, EXTENT[0], EXTENT[1])
+    y = cases.node_coordinates(nj, EXTENT[2], EXTENT[3])
+    z = cases.node_coordinates(nk, EXTENT[4], EXTENT[5])
+    mech = eu3d.parse_mechanism(cases.MECH_JA919, cases.THERMO)
+    scale = EXTENT[1] / 0.064
+    prim = cases.shock_bubble(x, y, z, mech["mw"], mech["ns"], radius=8e-3 * scale, shock_x=4e-3 * scale,
+                              standoff=16e-3 * scale, seed=seed)
+    p, cs, T, E = eu3d.initial_state(mech, ni, nj, nk, *prim)
+    dt = cases.cfl_dt(x, y, p[0], p[1], p[2], p[3], p[6], CFL)
+    return mech, prim, (p, cs, T, E), dt
+
+
+def state_dict(st):
+    p, cs, T, E = st
+    return {"CS": cs, "T": T, "E": E, "P": p[0], "D": p[1], "U": p[2], "V": p[3], "W": p[4], "H": p[5],
+            "Gamma": p[6], "Yi": p[7:]}
+
+
+def dist_setup(args):
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local = env_int("LOCAL_RANK", 0)
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
+    return world, rank, local, dist
+
+
+def reduce_max(dist, value, device):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, device):
+    if dist is not None:
+        import torch
+        if device.startswith("cuda"):
+            dist.barrier(device_ids=[int(device.split(":")[1])])
+        else:
+            dist.barrier()
+
+
+# ---------------------------------------------------------------- reference arm
+
+def _ref_worker(task):
+    """One host process: the reference's own CPU timestep on a sub-box sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    ni, nj, nk, steps, warmup, dt, seed = task
+    ext = (0.0, EXTENT[1] * (ni - 1) / (GRID[0] - 1), 0.0, EXTENT[3] * (nj - 1) / (GRID[1] - 1), 0.0,
+           EXTENT[5] * (nk - 1) / (GRID[2] - 1))
+    ref = oracle.RefOracle.from_grid(ni, nj, nk, ext, cases.MECH_JA919, cases.THERMO)
+    x, y, z = ref.nodes()
+    prim = cases.shock_bubble(x, y, z, ref.mechanism().mw, ref.ns, radius=min(ext[1], ext[3]) * 0.3,
+                              shock_x=ext[1] * 0.15, standoff=ext[1] * 0.45, seed=seed)
+    ref.set_primitive(*prim)
+    if warmup:
+        ref.step(warmup, dt)
+    t0 = time.perf_counter()
+    ref.step(steps, dt)
+    return time.perf_counter() - t0
+
+
+def reference_sample(nproc, steps, warmup, dt, box=(32, 32, 32)):
+    """Time the reference's CPU timestep (oracle/_ref) in nproc host processes,
+    each advancing its own sub-box of the workload at the workload's node
+    spacing. Returns Mcell-steps/s of the aggregate."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    tasks = [(box[0], box[1], box[2], steps, warmup, dt, 3 + r) for r in range(nproc)]
+    with ctx.Pool(nproc) as pool:
+        times = pool.map(_ref_worker, tasks)
+    cells = box[0] * box[1] * box[2]
+    return cells * steps * nproc / max(times) / 1e6, max(times)
+
+
+def reference_arm(args):
+    world, rank, local, dist = dist_setup(args)
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not os.path.exists(oracle.REF_LIB):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libeu3d_ref.so not built"}))
+        return 0
+    ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    nproc = max(1, min(ncores, 64))
+    _, _, _, dt = build_workload((64, 32, 32))
+    steps = max(1, args.steps)
+    warmup = max(0, args.warmup)
+    box = (24, 24, 24)
+    value, secs = reference_sample(nproc, steps, warmup, dt, box)
+    sample = (f"{nproc} host processes x reference CPU timestep (oracle/_ref, unmodified sources) on "
+              f"{box[0]}x{box[1]}x{box[2]}-node sub-boxes of the shock-bubble workload at its node spacing, "
+              f"{steps} timed steps after {warmup} warm-up; aggregate of independent single-rank runs")
+    line = {"metric": METRIC, "value": round(value, 6), "unit": "Mcell-steps/s", "n_gpus": world,
+            "steps": steps, "warmup": warmup, "ms_per_step": round(secs / steps * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": "3-D reacting shock-bubble 256x128x128 (H2_JA919), sampled", "grid": list(GRID),
+                       "chemistry": "stiff", "precision": "fp64"},
+            "cpu_baseline": {"value": round(value, 6), "unit": "Mcell-steps/s", "cores": nproc,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": round(value, 6), "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------- our arm
+
+def cpu_baseline(dt):
+    """The reference's CPU timestep on one core, on a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    try:
+        import oracle
+        if not os.path.exists(oracle.REF_LIB):
+            return None
+    except ImportError:
+        return None
+    box = (48, 48, 48)
+    steps = 6
+    secs = _ref_worker((box[0], box[1], box[2], steps, 1, dt, 3))
+    cells = box[0] * box[1] * box[2]
+    return {"value": round(cells * steps / secs / 1e6, 6), "unit": "Mcell-steps/s", "cores": 1,
+            "kind": "reference",
+            "sample": f"reference CPU timestep (oracle/_ref) on a {box[0]}x{box[1]}x{box[2]}-node sub-box of the "
+                      f"workload at its node spacing, {steps} steps after 1 warm-up, single thread ({secs:.1f} s)"}
+
+
+def our_arm(args):
+    import torch
+    world, rank, local, dist = dist_setup(args)
+    device = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    grid = tuple(args.grid)
+    ncell = grid[0] * grid[1] * grid[2]
+    mech, prim, st0, dt = build_workload(grid)
+    sd = state_dict(st0)
+
+    def make_solver(profile):
+        s = eu3d.Solver(*grid, (EXTENT[0], EXTENT[1] * 1, EXTENT[2], EXTENT[3], EXTENT[4], EXTENT[5]),
+                        precision=args.precision, chemistry=args.chem, arith=args.arith, device=local,
+                        profile=profile)
+        s.set_mechanism(mech)
+        s.set_state(sd)
+        return s
+
+    # -- device-resident throughput (value) -------------------------------------------------
+    s = make_solver(profile=False)
+    s.step(args.warmup, dt)
+    barrier(dist, device)
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        stats = s.step(args.steps, dt)
+    torch.cuda.synchronize()
+    barrier(dist, device)
+    ms = reduce_max(dist, stats["device_ms"], device)
+    value = ncell * args.steps * world / (ms / 1e3) / 1e6
+    clocks = clk.summary()
+
+    # -- per-kernel times (same stream, CUDA events around each kernel) -----------------------
+    sp = make_solver(profile=True)
+    sp.step(args.warmup, dt)
+    pst = sp.step(args.steps, dt)
+    phase = pst["phase_ms"]
+    names = ["ghost_fill", "flux_update", "recover_kinetics"]
+    per_kernel = {n: round(phase[q] / args.steps, 4) for q, n in enumerate(names)}
+    sp.close()
+
+    hbm, bf16, peak_kind = measured_peaks()
+    flux_ms = phase[1] / args.steps
+    flux_gbs = FLUX_BYTES[args.precision] * ncell / (flux_ms / 1e3) / 1e9
+    dominant = max(range(3), key=lambda q: phase[q])
+    roofline = {"kernel": "flux_update", "bound": "hbm", "achieved": round(flux_gbs, 1), "peak": hbm,
+                "unit": "GB/s", "frac": round(flux_gbs / hbm, 4), "traffic": None,
+                "algorithmic_bytes_per_cell": FLUX_BYTES[args.precision], "peak_source": f"{peak_kind} hbm_gbs",
+                "dominant_kernel": names[dominant],
+                "dominant_share": round(phase[dominant] / max(sum(phase[:3]), 1e-9), 3)}
+
+    # -- end to end through the public API with host buffers ----------------------------------
+    pinned = {}
+    for k, v in sd.items():
+        t = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = v
+        pinned[k] = t.numpy()
+    se = eu3d.Solver(*grid, EXTENT, precision=args.precision, chemistry=args.chem, arith=args.arith,
+                     device=local)
+    se.set_mechanism(mech)
+    se.set_state(pinned)
+    se.step(args.warmup, dt)
+    barrier(dist, device)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    se.set_state(pinned)
+    for _ in range(args.steps):
+        se.step(1, dt)  # synchronous: reads the step's health counters back
+    cs = se.get("CS")
+    torch.cuda.synchronize()
+    e2e_s = reduce_max(dist, time.perf_counter() - t0, device)
+    e2e_value = ncell * args.steps * world / e2e_s / 1e6
+    state_bytes = sum(v.nbytes for v in pinned.values())
+    h2d = state_bytes / args.steps + 8
+    d2h = cs.nbytes / args.steps + 96
+    se.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(dt)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 3), "unit": "Mcell-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": "3-D reacting shock-bubble, 256x128x128 nodes over 64x32x32 mm, "
+                                       "H2_JA919 (9 species, 19 reactions), Mach 2.83 in N2, seed 3",
+                           "grid": list(grid), "dt": dt, "precision": args.precision, "chemistry": args.chem,
+                           "arith": args.arith, "parallelism": f"replicas x{world}",
+                           "l2": f"inputs larger than L2: {sd['CS'].nbytes * 3 // 2**20} MiB state > 126 MiB"},
+                "roofline": roofline, "kernels_ms_per_step": per_kernel,
+                "max_nchem": stats["max_nchem"], "substeps_per_cell": stats["sum_nchem"] / ncell,
+                "clocks": clocks,
+                "e2e": {"value": round(e2e_value, 3), "unit": "Mcell-steps/s",
+                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+                "gpu_launches": stats["launches"],
+                "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--chem", choices=["stiff", "frozen"], default="stiff")
+    ap.add_argument("--arith", choices=["strict", "fast"], default="fast")
+    ap.add_argument("--grid", type=int, nargs=3, default=list(GRID))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args)
+    return our_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,91 @@
+// eu3d_kernels_impl.cuh — launchers for one arithmetic flavour. Included once
+// by eu3d_kernels_strict.cu (EU_STRICT, --fmad=false) and once by
+// eu3d_kernels_fast.cu, with EU3D_NS naming the namespace.
+#pragma once
+
+#include "eu3d_kernels.cuh"
+#include "eu3d_launch.hpp"
+
+namespace eu3d {
+namespace EU3D_NS {
+
+namespace {
+
+template <int NS, int NR>
+cudaError_t boundary_t(const LaunchArgs &a)
+{
+    const DevGrid &g = a.g;
+    const long long n = 2LL * g.bc * ((long long)g.nj * g.nk + (long long)g.ni * g.nk + (long long)g.ni * g.nj);
+    const int threads = 256;
+    const long long blocks = (n + threads - 1) / threads;
+    k_boundary<NS><<<dim3((unsigned)blocks), threads, 0, a.stream>>>(*a.mech, g, a.st);
+    return cudaGetLastError();
+}
+
+template <int NS, int NR>
+cudaError_t flux_t(const LaunchArgs &a)
+{
+    const DevGrid &g = a.g;
+    const dim3 block(32, 2, 2);
+    const dim3 grid((g.nk + block.x - 1) / block.x, (g.nj + block.y - 1) / block.y,
+                    (g.ni + block.z - 1) / block.z);
+    if (a.precision == 1) {
+        k_flux_update<NS, float><<<grid, block, 0, a.stream>>>(g, a.st, a.st.prim32, a.dt_dev);
+    } else {
+        k_flux_update<NS, double><<<grid, block, 0, a.stream>>>(g, a.st, a.st.prim, a.dt_dev);
+    }
+    return cudaGetLastError();
+}
+
+template <int NS, int NR>
+cudaError_t react_t(const LaunchArgs &a, bool react)
+{
+    const DevGrid &g = a.g;
+    const long long n = (long long)g.ni * g.nj * g.nk;
+    const int threads = 128;
+    const long long blocks = (n + threads - 1) / threads;
+    if (react)
+        k_recover_react<NS, NR, true>
+            <<<dim3((unsigned)blocks), threads, 0, a.stream>>>(*a.mech, g, a.st, a.dt_dev, a.max_substeps);
+    else
+        k_recover_react<NS, NR, false>
+            <<<dim3((unsigned)blocks), threads, 0, a.stream>>>(*a.mech, g, a.st, a.dt_dev, a.max_substeps);
+    return cudaGetLastError();
+}
+
+template <int NS, int NR>
+cudaError_t derived_t(const LaunchArgs &a, int which, double *out)
+{
+    const int threads = 256;
+    const long long blocks = (a.g.n3 + threads - 1) / threads;
+    k_derived<NS><<<dim3((unsigned)blocks), threads, 0, a.stream>>>(*a.mech, a.g, a.st, which, out);
+    return cudaGetLastError();
+}
+
+} // namespace
+
+// Supported (NS, NR): the repository mechanism H2_JA919 (9 species, 19
+// reactions), the one the reference's parser reads.
+#define EU3D_DISPATCH(fn, ...)                                                                     \
+    switch (a.mech->ns * 100 + a.mech->nr) {                                                        \
+    case 919:                                                                                      \
+        return fn<9, 19>(__VA_ARGS__);                                                             \
+    default:                                                                                       \
+        return cudaErrorInvalidValue;                                                              \
+    }
+
+cudaError_t launch_boundary(const LaunchArgs &a) { EU3D_DISPATCH(boundary_t, a) }
+cudaError_t launch_flux_update(const LaunchArgs &a) { EU3D_DISPATCH(flux_t, a) }
+cudaError_t launch_recover_react(const LaunchArgs &a, bool react) { EU3D_DISPATCH(react_t, a, react) }
+cudaError_t launch_derived(const LaunchArgs &a, int which, double *out) { EU3D_DISPATCH(derived_t, a, which, out) }
+
+cudaError_t launch_set_value(double *dst, double v, cudaStream_t s)
+{
+    k_set_value<<<1, 1, 0, s>>>(dst, v);
+    return cudaGetLastError();
+}
+
+#undef EU3D_DISPATCH
+
+} // namespace EU3D_NS
+} // namespace eu3d

@@ -1,0 +1,68 @@
+// eu3d_types.h — plain structs shared by host code and kernels: mechanism
+// tables as the kernels see them, grid geometry and device state pointers.
+#pragma once
+
+#include <cstdint>
+
+namespace eu3d {
+
+constexpr int kMaxS = 16; // include/ReactionCuda.cuh:4
+constexpr int kMaxR = 24; // include/ReactionCuda.cuh:5
+
+constexpr double kRUniv = 8.31434;      // include/Flowfield.hpp:57
+constexpr double kRuCal = 1.987;        // include/Reaction.hpp:67
+constexpr double kP0 = 101325.0;        // include/Reaction.hpp:68
+constexpr double kThermoSwitch = 1000.0; // include/ThermoConstants.hpp:3
+
+// Mechanism + thermo tables, passed to kernels by value (__grid_constant__) so
+// that uniform reads come from the constant bank and handles stay independent.
+struct DevMech {
+    int ns, nr;
+    int nu_int;             // 1 when every stoichiometric coefficient is 0, 1 or 2
+    int pad;
+    double mw[kMaxS];
+    double ri[kMaxS];       // R / Mw (src/Reaction.cpp:426-427)
+    double clo[9][kMaxS];   // Coeff0(k, s)
+    double chi[9][kMaxS];   // Coeff1(k, s)
+    double af[kMaxR], bf[kMaxR], eaf[kMaxR];
+    double xr[kMaxR];       // sum_s (nu_b - nu_f)
+    double sf[kMaxR][kMaxS], sb[kMaxR][kMaxS], tb[kMaxR][kMaxS];
+    int has_tb[kMaxR];
+};
+
+// Grid and field pointers of one handle (all device memory).
+struct DevGrid {
+    int ni, nj, nk, bc, nx, ny, nz;
+    long long n3;
+    const double *x, *y, *z; // node coordinates with ghosts
+};
+
+// Primitive planes the stencils read, in this order (haloed, FP64).
+enum PrimIdx { kP = 0, kD = 1, kU = 2, kV = 3, kW = 4, kH = 5, kG = 6, kY0 = 7 };
+
+struct DevState {
+    double *prim;     // (7 + ns) planes
+    float *prim32;    // (7 + ns) planes, FP32 copy for EU_PREC_MIXED (or null)
+    double *cs;       // ns + 4 planes
+    double *T, *E;    // planes
+    int *nchem;       // plane
+    double *cms;      // ns planes (or null)
+    unsigned long long *counters; // see CounterIdx
+};
+
+// Device counters. The first kCntPerStep are statistics of the latest step
+// (cleared before each step); the rest accumulate over one eu_step call so an
+// error in any step of the call is reported.
+enum CounterIdx {
+    kCntMaxNchem = 0,
+    kCntSumNchem = 1,
+    kCntReacting = 2,
+    kCntLearned = 3,
+    kCntFallback = 4,
+    kCntPerStep = 5,
+    kCntNonfinite = 5,
+    kCntBadNchem = 6,
+    kCntCount = 8
+};
+
+} // namespace eu3d

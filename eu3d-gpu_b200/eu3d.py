@@ -1,0 +1,251 @@
+"""Python binding of libeu3d.so (the C ABI declared in include/eu3d.h).
+
+Thin ctypes layer used by the tests and by bench.py. The compute path is the
+CUDA library; this module never computes a timestep itself and raises if the
+library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libeu3d.so")
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+
+STATUS = {0: "EU_OK", 1: "EU_ERR_INVALID_ARGUMENT", 2: "EU_ERR_CUDA", 3: "EU_ERR_OUT_OF_MEMORY", 4: "EU_ERR_IO",
+          5: "EU_ERR_NONFINITE", 6: "EU_ERR_NCHEM", 7: "EU_ERR_NOT_READY", 8: "EU_ERR_UNSUPPORTED",
+          9: "EU_ERR_TIMEOUT"}
+PRECISION = {"fp64": 0, "mixed": 1}
+CHEMISTRY = {"stiff": 0, "frozen": 1, "learned": 2}
+ARITH = {"strict": 0, "fast": 1}
+
+
+class EU3DError(RuntimeError):
+    def __init__(self, status, message=""):
+        self.status = status
+        self.name = STATUS.get(status, str(status))
+        super().__init__(f"{self.name}: {message}" if message else self.name)
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("total_ni", _I), ("total_nj", _I), ("total_nk", _I),
+                ("xa", _D), ("xb", _D), ("ya", _D), ("yb", _D), ("za", _D), ("zb", _D),
+                ("bc", _I), ("device", _I), ("precision", _I), ("chemistry", _I), ("arith", _I),
+                ("max_substeps", _I), ("record_sources", _I), ("profile", _I)]
+
+
+class MechanismC(ctypes.Structure):
+    _fields_ = [("ns", _I), ("nr", _I)] + [(n, _P) for n in ("mw", "coeff_lo", "coeff_hi", "af", "bf", "eaf",
+                                                            "stoi_f", "stoi_b", "tb")]
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [("steps", _I), ("max_nchem", _I), ("sum_nchem", ctypes.c_longlong),
+                ("reacting", ctypes.c_longlong), ("learned", ctypes.c_longlong), ("fallback", ctypes.c_longlong),
+                ("nonfinite", ctypes.c_longlong), ("device_ms", _D), ("phase_ms", _D * 4), ("launches", _I)]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_}
+        d["phase_ms"] = list(self.phase_ms)
+        return d
+
+
+_lib = None
+
+
+def library():
+    """Load libeu3d.so (built in-tree by `make -C eu3d-gpu_b200`)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is not built; run `make -C eu3d-gpu_b200` (or __graft_entry__.build())")
+        lib = ctypes.CDLL(LIB_PATH)
+        lib.eu_abi_version.restype = _I
+        lib.eu_read_grid.argtypes = [ctypes.c_char_p, ctypes.POINTER(Config)]
+        lib.eu_parse_mechanism.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_I), ctypes.POINTER(_I)] + [_P] * 9
+        lib.eu_initial_state.argtypes = [ctypes.POINTER(MechanismC), _I, _I, _I, _I] + [_P] * 10
+        lib.eu_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(_P)]
+        lib.eu_destroy.argtypes = [_P]
+        lib.eu_last_error.restype = ctypes.c_char_p
+        lib.eu_last_error.argtypes = [_P]
+        lib.eu_load_mechanism.argtypes = [_P, ctypes.c_char_p, ctypes.c_char_p]
+        lib.eu_set_mechanism.argtypes = [_P, ctypes.POINTER(MechanismC)]
+        lib.eu_get_mechanism.argtypes = [_P, ctypes.POINTER(_I), ctypes.POINTER(_I)] + [_P] * 9
+        lib.eu_node_coordinates.argtypes = [_P, _P, _P, _P]
+        lib.eu_set_primitive.argtypes = [_P] * 7
+        lib.eu_set_state.argtypes = [_P] * 12
+        lib.eu_step.argtypes = [_P, _I, _D, ctypes.POINTER(StepStats)]
+        lib.eu_get_field.argtypes = [_P, ctypes.c_char_p, _P]
+        lib.eu_sync.argtypes = [_P]
+        lib.eu_device_info.argtypes = [_P, ctypes.POINTER(_P), ctypes.POINTER(ctypes.c_size_t)]
+        for fn in ("eu_read_grid", "eu_parse_mechanism", "eu_initial_state", "eu_create", "eu_destroy",
+                   "eu_load_mechanism", "eu_set_mechanism", "eu_get_mechanism", "eu_node_coordinates",
+                   "eu_set_primitive", "eu_set_state", "eu_step", "eu_get_field", "eu_sync", "eu_device_info"):
+            getattr(lib, fn).restype = _I
+        _lib = lib
+    return _lib
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def parse_mechanism(mech_path, thermo_path):
+    """Mechanism tables as the library parses them (no device needed)."""
+    lib = library()
+    ns, nr = _I(), _I()
+    st = lib.eu_parse_mechanism(mech_path.encode(), thermo_path.encode(), ctypes.byref(ns), ctypes.byref(nr),
+                                *([None] * 9))
+    if st:
+        raise EU3DError(st, f"parse {mech_path} / {thermo_path}")
+    ns, nr = ns.value, nr.value
+    out = {"mw": np.zeros(ns), "coeff_lo": np.zeros((9, ns)), "coeff_hi": np.zeros((9, ns)), "af": np.zeros(nr),
+           "bf": np.zeros(nr), "eaf": np.zeros(nr), "stoi_f": np.zeros((ns, nr)), "stoi_b": np.zeros((ns, nr)),
+           "tb": np.zeros((ns, nr))}
+    order = ["mw", "coeff_lo", "coeff_hi", "af", "bf", "eaf", "stoi_f", "stoi_b", "tb"]
+    st = lib.eu_parse_mechanism(mech_path.encode(), thermo_path.encode(), None, None,
+                                *[out[k].ctypes.data for k in order])
+    if st:
+        raise EU3DError(st)
+    out["ns"], out["nr"] = ns, nr
+    return out
+
+
+def mechanism_struct(m):
+    """eu_mechanism from an object/dict with the table attributes; returns (struct, keepalive)."""
+    get = (lambda k: m[k]) if isinstance(m, dict) else (lambda k: getattr(m, k))
+    keep = [_c(get(k)) for k in ("mw", "coeff_lo", "coeff_hi", "af", "bf", "eaf", "stoi_f", "stoi_b", "tb")]
+    return MechanismC(int(get("ns")), int(get("nr")), *[a.ctypes.data for a in keep]), keep
+
+
+def initial_state(mech, ni, nj, nk, P, T, U, V, W, Y, bc=2):
+    """Host-only FieldInitial-derived state (no device)."""
+    lib = library()
+    ms, keep = mechanism_struct(mech)
+    ns = ms.ns
+    shape = (ni + 2 * bc, nj + 2 * bc, nk + 2 * bc)
+    n3 = int(np.prod(shape))
+    prim = np.zeros((7 + ns) * n3)
+    cs = np.zeros((ns + 4) * n3)
+    To = np.zeros(n3)
+    Eo = np.zeros(n3)
+    ins = [_c(a) for a in (P, T, U, V, W, Y)]
+    st = lib.eu_initial_state(ctypes.byref(ms), ni, nj, nk, bc, *[a.ctypes.data for a in ins], prim.ctypes.data,
+                              cs.ctypes.data, To.ctypes.data, Eo.ctypes.data)
+    if st:
+        raise EU3DError(st, "eu_initial_state")
+    return (prim.reshape(7 + ns, *shape), cs.reshape(ns + 4, *shape), To.reshape(1, *shape), Eo.reshape(1, *shape))
+
+
+class Solver:
+    """One eu_handle: a haloed node grid, a mechanism and the device state."""
+
+    def __init__(self, total_ni, total_nj, total_nk, extent, precision="fp64", chemistry="stiff", arith="strict",
+                 device=0, max_substeps=0, record_sources=False, profile=False, bc=2):
+        lib = library()
+        self.cfg = Config(int(total_ni), int(total_nj), int(total_nk), *[float(v) for v in extent], int(bc),
+                          int(device), PRECISION[precision], CHEMISTRY[chemistry], ARITH[arith], int(max_substeps),
+                          int(bool(record_sources)), int(bool(profile)))
+        h = _P()
+        st = lib.eu_create(ctypes.byref(self.cfg), ctypes.byref(h))
+        if st:
+            raise EU3DError(st, "eu_create")
+        self.h = h
+        self.ni, self.nj, self.nk, self.bc = int(total_ni), int(total_nj), int(total_nk), int(bc)
+        self.shape = (self.ni + 2 * bc, self.nj + 2 * bc, self.nk + 2 * bc)
+        self.n3 = int(np.prod(self.shape))
+        self.ns = None
+
+    @classmethod
+    def from_grid_file(cls, path, **kw):
+        cfg = Config()
+        st = library().eu_read_grid(path.encode(), ctypes.byref(cfg))
+        if st:
+            raise EU3DError(st, path)
+        return cls(cfg.total_ni, cfg.total_nj, cfg.total_nk, (cfg.xa, cfg.xb, cfg.ya, cfg.yb, cfg.za, cfg.zb),
+                   bc=cfg.bc, **kw)
+
+    def _check(self, st, what=""):
+        if st:
+            msg = library().eu_last_error(self.h).decode() if self.h else ""
+            raise EU3DError(st, f"{what}: {msg}" if what else msg)
+
+    def close(self):
+        if getattr(self, "h", None):
+            library().eu_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load_mechanism(self, mech_path, thermo_path):
+        self._check(library().eu_load_mechanism(self.h, mech_path.encode(), thermo_path.encode()), "load_mechanism")
+        self.ns = self.mechanism()["ns"]
+
+    def set_mechanism(self, m):
+        ms, keep = mechanism_struct(m)
+        self._check(library().eu_set_mechanism(self.h, ctypes.byref(ms)), "set_mechanism")
+        self.ns = ms.ns
+
+    def mechanism(self):
+        lib = library()
+        ns, nr = _I(), _I()
+        self._check(lib.eu_get_mechanism(self.h, ctypes.byref(ns), ctypes.byref(nr), *([None] * 9)))
+        ns, nr = ns.value, nr.value
+        out = {"mw": np.zeros(ns), "coeff_lo": np.zeros((9, ns)), "coeff_hi": np.zeros((9, ns)),
+               "af": np.zeros(nr), "bf": np.zeros(nr), "eaf": np.zeros(nr), "stoi_f": np.zeros((ns, nr)),
+               "stoi_b": np.zeros((ns, nr)), "tb": np.zeros((ns, nr))}
+        order = ["mw", "coeff_lo", "coeff_hi", "af", "bf", "eaf", "stoi_f", "stoi_b", "tb"]
+        self._check(lib.eu_get_mechanism(self.h, None, None, *[out[k].ctypes.data for k in order]))
+        out["ns"], out["nr"] = ns, nr
+        return out
+
+    def nodes(self):
+        x, y, z = (np.zeros(n) for n in self.shape)
+        self._check(library().eu_node_coordinates(self.h, x.ctypes.data, y.ctypes.data, z.ctypes.data))
+        return x, y, z
+
+    def set_primitive(self, P, T, U, V, W, Y):
+        arrs = [_c(a) for a in (P, T, U, V, W, Y)]
+        self._check(library().eu_set_primitive(self.h, *[a.ctypes.data for a in arrs]), "set_primitive")
+
+    def set_state(self, st):
+        order = ["CS", "T", "E", "P", "D", "U", "V", "W", "H", "Gamma", "Yi"]
+        arrs = [_c(st[n]) for n in order]
+        self._check(library().eu_set_state(self.h, *[a.ctypes.data for a in arrs]), "set_state")
+
+    def step(self, nsteps, dt, stats=True):
+        s = StepStats()
+        st = library().eu_step(self.h, int(nsteps), float(dt), ctypes.byref(s) if stats else None)
+        self._check(st, "step")
+        return s.as_dict() if stats else None
+
+    def get(self, name):
+        planes = {"Yi": self.ns, "Di": self.ns, "Mc": self.ns, "CMS": self.ns, "CS": self.ns + 4}.get(name, 1)
+        out = np.empty(planes * self.n3)
+        self._check(library().eu_get_field(self.h, name.encode(), out.ctypes.data), f"get {name}")
+        return out.reshape(planes, *self.shape)
+
+    def sync(self):
+        self._check(library().eu_sync(self.h), "sync")
+
+    def device_info(self):
+        stream = _P()
+        nbytes = ctypes.c_size_t()
+        self._check(library().eu_device_info(self.h, ctypes.byref(stream), ctypes.byref(nbytes)))
+        return stream.value, nbytes.value

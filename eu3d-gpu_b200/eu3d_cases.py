@@ -1,0 +1,182 @@
+"""Initial conditions of the EU3D workloads, as primitive fields over the haloed grid.
+
+* ``rsbi`` — the reference's only wired case (reacting shock / H2 cylinder in
+  air): Flowfield::FieldInitial (src/Flowfield.cpp:193-225) for p, T, u and
+  Reaction::ReactionInitial (src/Reaction.cpp:412-471) for the composition,
+  over every node including ghosts, as the reference fills them.
+* ``shock_bubble`` — the 3-D reacting shock-bubble workload: a planar shock
+  in N2 hitting a sphere of stoichiometric 2H2+O2 with a tanh interface and a
+  seeded spherical-harmonic surface perturbation (l = 1..8, RMS amplitude 2 % of
+  the radius). The reference hard-codes only RSBI, so this initialiser is new;
+  the timestep it feeds is the reference's.
+
+Fields come back as numpy arrays over (nx, ny, nz) = haloed node counts; the
+species array is (ns, nx, ny, nz) in mechanism order.
+"""
+from __future__ import annotations
+
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DATA = os.path.join(HERE, "data")
+MECH_JA919 = os.path.join(DATA, "H2_JA919.txt")
+MECH_JA1119 = os.path.join(DATA, "H2_JA1119.txt")
+THERMO = os.path.join(DATA, "thermo.dat")
+
+# species slots of H2_JA919 (H O H2O OH O2 H2 H2O2 HO2 N2)
+S_O2, S_H2, S_N2 = 4, 5, 8
+
+
+def node_coordinates(n, a, b, bc=2):
+    """src/Mesh.cpp:96-142 for one block (ghosts mirrored about the end nodes)."""
+    d = (b - a) / (n - 1)
+    x = np.zeros(n + 2 * bc)
+    for i in range(bc, n + bc):
+        x[i] = a + (0 * (n - 1) + i - bc) * d
+    for i in range(bc):
+        x[i] = 2 * x[bc] - x[2 * bc - i]
+        x[n + bc + i] = 2 * x[n + bc - 1] - x[n + bc - 1 - i - 1]
+    return x
+
+
+def rsbi(x, y, z, mw, ns, p_pre=101325.0, t_pre=1000.0, m_wave=3.0):
+    """The reference's RSBI initial primitives, formula for formula."""
+    nx, ny, nz = len(x), len(y), len(z)
+    # src/Flowfield.cpp:206-225 (gamma 1.4 and R 287 as the reference writes them)
+    u_post = m_wave * (1 - (2 + 0.40 * m_wave ** 2) / (2.40 * m_wave ** 2)) * math.sqrt(1.40 * 287 * t_pre)
+    p_post = p_pre * (1 + 2 * 1.4 / 2.4 * (m_wave ** 2 - 1.0))
+    t_post = t_pre * (2 + 0.40 * m_wave ** 2) / (2.40 * m_wave ** 2) * p_post / p_pre
+    ahead = (x >= 0.01)[:, None, None] * np.ones((1, ny, nz), bool)
+    P = np.where(ahead, p_pre, p_post)
+    T = np.where(ahead, t_pre, t_post)
+    U = np.where(ahead, 0.0, u_post)
+    V = np.zeros((nx, ny, nz))
+    W = np.zeros((nx, ny, nz))
+    # src/Reaction.cpp:419-470, evaluated with the C library's exp/sqrt
+    cx, cy, ir = 0.038, 0.0, 0.022
+    orad = 1.2 * ir
+    alpha = 5
+    Y = np.zeros((ns, nx, ny, nz))
+    col = np.zeros((ns, nx, ny))
+    for i in range(nx):
+        for j in range(ny):
+            d2 = (x[i] - cx) ** 2 + (y[j] - cy) ** 2
+            if d2 > orad ** 2:
+                mr = np.zeros(ns)
+                mr[S_O2] = 1.0
+                mr[S_N2] = 3.76
+                tot = sum(mr[s] * mw[s] for s in range(ns))
+                col[:, i, j] = [mr[s] * mw[s] / tot for s in range(ns)]
+            elif d2 < ir ** 2:
+                col[S_H2, i, j] = 1.0 * mw[S_H2] / (1.0 * mw[S_H2])
+            else:
+                r = math.sqrt(d2)
+                yh2 = math.exp(-alpha * ((r - ir) / (orad - ir)) ** 2)
+                col[S_H2, i, j] = yh2
+                col[S_O2, i, j] = (1 - yh2) * mw[S_O2] / (mw[S_O2] + 3.76 * mw[S_N2])
+                col[S_N2, i, j] = (1 - yh2) * 3.76 * mw[S_N2] / (mw[S_O2] + 3.76 * mw[S_N2])
+    Y[:] = col[:, :, :, None]
+    return P, T, U, V, W, Y
+
+
+def normal_shock(mach, p1, t1, r_gas, gamma=1.4):
+    """Post-shock (p, T, u) of a shock of Mach `mach` running into gas at rest."""
+    g = gamma
+    u2 = mach * (1 - (2 + (g - 1) * mach ** 2) / ((g + 1) * mach ** 2)) * math.sqrt(g * r_gas * t1)
+    p2 = p1 * (1 + 2 * g / (g + 1) * (mach ** 2 - 1.0))
+    t2 = t1 * (2 + (g - 1) * mach ** 2) / ((g + 1) * mach ** 2) * p2 / p1
+    return p2, t2, u2
+
+
+def _real_sph_harm(lmax, theta, phi):
+    """Orthonormal real spherical harmonics Y_lm(theta, phi), l = 0..lmax, as a
+    list of (l, m, values). Associated Legendre functions by the standard
+    three-term recurrence (Condon-Shortley phase omitted)."""
+    x = np.cos(theta)
+    sx = np.sqrt(np.maximum(0.0, 1 - x * x))
+    out = []
+    pmm = np.ones_like(x)
+    plm = {}
+    for m in range(lmax + 1):
+        if m > 0:
+            pmm = pmm * (2 * m - 1) * sx
+        plm[(m, m)] = pmm
+        if m < lmax:
+            plm[(m + 1, m)] = x * (2 * m + 1) * pmm
+        for l in range(m + 2, lmax + 1):
+            plm[(l, m)] = ((2 * l - 1) * x * plm[(l - 1, m)] - (l + m - 1) * plm[(l - 2, m)]) / (l - m)
+    for l in range(lmax + 1):
+        for m in range(-l, l + 1):
+            am = abs(m)
+            norm = math.sqrt((2 * l + 1) / (4 * math.pi) * math.factorial(l - am) / math.factorial(l + am))
+            if m == 0:
+                v = norm * plm[(l, 0)]
+            elif m > 0:
+                v = math.sqrt(2) * norm * plm[(l, am)] * np.cos(am * phi)
+            else:
+                v = math.sqrt(2) * norm * plm[(l, am)] * np.sin(am * phi)
+            out.append((l, m, v))
+    return out
+
+
+def shock_bubble(x, y, z, mw, ns, mach=2.83, p0=101325.0, t0=300.0, radius=8e-3, shock_x=4e-3,
+                 standoff=16e-3, center_yz=None, lmax=8, amplitude=0.02, seed=3, interface_cells=2.0):
+    """Planar shock in N2 (moving +x) hitting a perturbed 2H2+O2 sphere.
+
+    The sphere's centre sits `standoff` downstream of the shock; its surface is
+    r_s(theta, phi) = radius * (1 + sum_{l=1..lmax} a_lm Y_lm) with a_lm drawn from
+    numpy.random.default_rng(seed) and scaled to an RMS of `amplitude` over the
+    sphere. The composition blends across the surface with
+    f = (1 - tanh((r - r_s) / w)) / 2, w = interface_cells * dx / 2 (a 2-cell
+    thick profile). Pre-shock gas and bubble are at (p0, t0) and rest."""
+    nx, ny, nz = len(x), len(y), len(z)
+    dx = x[3] - x[2]
+    if center_yz is None:
+        center_yz = (0.5 * (y[2] + y[-3]), 0.5 * (z[2] + z[-3]))
+    cx = shock_x + standoff
+    cy, cz = center_yz
+    rng = np.random.default_rng(seed)
+    modes = [(l, m) for l in range(1, lmax + 1) for m in range(-l, l + 1)]
+    a = rng.standard_normal(len(modes))
+    a *= amplitude * math.sqrt(4 * math.pi) / math.sqrt(np.sum(a * a))
+    X, Yc, Z = np.meshgrid(x - cx, y - cy, z - cz, indexing="ij")
+    r = np.sqrt(X * X + Yc * Yc + Z * Z)
+    theta = np.arccos(np.clip(np.divide(Z, r, out=np.zeros_like(r), where=r > 0), -1, 1))
+    phi = np.arctan2(Yc, X)
+    pert = np.zeros_like(r)
+    harm = {(l, m): v for l, m, v in _real_sph_harm(lmax, theta, phi)}
+    for coef, (l, m) in zip(a, modes):
+        pert += coef * harm[(l, m)]
+    rs = radius * (1 + pert)
+    w = 0.5 * interface_cells * dx
+    f = 0.5 * (1 - np.tanh((r - rs) / w))
+    y_h2 = 2 * mw[S_H2] / (2 * mw[S_H2] + mw[S_O2])
+    Y = np.zeros((ns, nx, ny, nz))
+    Y[S_H2] = f * y_h2
+    Y[S_O2] = f * (1 - y_h2)
+    Y[S_N2] = 1 - f
+    r_n2 = 8.31434 * 1000 / mw[S_N2]
+    p2, t2, u2 = normal_shock(mach, p0, t0, r_n2)
+    behind = (x < shock_x)[:, None, None] * np.ones((1, ny, nz), bool)
+    P = np.where(behind, p2, p0)
+    T = np.where(behind, t2, t0)
+    U = np.where(behind, u2, 0.0)
+    V = np.zeros((nx, ny, nz))
+    W = np.zeros((nx, ny, nz))
+    # shocked gas is pure N2 (the sphere sits fully downstream of the shock)
+    Y[:, behind] = 0.0
+    Y[S_N2, behind] = 1.0
+    return P, T, U, V, W, Y
+
+
+def cfl_dt(x, y, P, D, U, V, G, cfl, bc=2):
+    """Flowfield::CFLcondition (src/Flowfield.cpp:272-304): dt from dx, dy only."""
+    dx = x[1] - x[0]
+    dy = y[1] - y[0]
+    s = (slice(bc, -bc),) * 3
+    C = np.sqrt(G[s] * P[s] / D[s])
+    t = np.minimum(dx / (np.abs(U[s]) + C), dy / (np.abs(V[s]) + C))
+    return cfl * float(t.min())

@@ -1,0 +1,635 @@
+// eu3d_api.cpp — the C ABI (include/eu3d.h): handle lifetime, device memory,
+// uploads/downloads and the per-timestep launch sequence.
+#include "eu3d.h"
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../csrc/eu3d_launch.hpp"
+#include "readers.hpp"
+#include "state_init.hpp"
+
+using namespace eu3d;
+
+struct eu_handle {
+    eu_config cfg{};
+    int ni = 0, nj = 0, nk = 0, bc = 0, nx = 0, ny = 0, nz = 0;
+    long long n3 = 0;
+    std::vector<double> x, y, z;
+    MechanismTables mech;
+    DevMech dmech{};
+    bool has_mech = false, has_state = false;
+    DevGrid g{};
+    DevState st{};
+    double *d_xyz = nullptr;
+    double *d_dt = nullptr;
+    double *d_scratch = nullptr;
+    std::vector<void *> allocs;
+    size_t bytes = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t pev[4] = {nullptr, nullptr, nullptr, nullptr}; // phase boundaries (cfg.profile)
+    std::string err;
+};
+
+namespace {
+
+const char *kNoHandle = "null handle";
+
+eu_status fail(eu_handle *h, eu_status s, const char *fmt, ...)
+{
+    if (h) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        std::vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        h->err = buf;
+    }
+    return s;
+}
+
+eu_status cuda_fail(eu_handle *h, cudaError_t e, const char *what)
+{
+    if (e == cudaErrorMemoryAllocation)
+        return fail(h, EU_ERR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
+    return fail(h, EU_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(h, call)                                                                                \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return cuda_fail((h), e_, #call);                                                      \
+    } while (0)
+
+template <typename T>
+eu_status dalloc(eu_handle *h, T **p, size_t count)
+{
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+    if (e != cudaSuccess)
+        return cuda_fail(h, e, "cudaMalloc");
+    h->allocs.push_back(q);
+    h->bytes += count * sizeof(T);
+    *p = static_cast<T *>(q);
+    return EU_OK;
+}
+
+void free_all(eu_handle *h)
+{
+    for (void *p : h->allocs) cudaFree(p);
+    h->allocs.clear();
+    h->bytes = 0;
+}
+
+// DevMech from host tables; rejects sizes the kernels are not built for.
+eu_status install_mechanism(eu_handle *h, const MechanismTables &m)
+{
+    if (m.ns <= 0 || m.nr <= 0 || m.ns > kMaxS || m.nr > kMaxR)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "mechanism sizes ns=%d nr=%d outside 1..%d / 1..%d", m.ns, m.nr,
+                    kMaxS, kMaxR);
+    if (!sizes_supported(m.ns, m.nr))
+        return fail(h, EU_ERR_UNSUPPORTED, "no kernels built for ns=%d nr=%d (built: 9/19)", m.ns, m.nr);
+    if (h->has_mech && m.ns != h->mech.ns)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "species count cannot change on a live handle");
+    DevMech d;
+    std::memset(&d, 0, sizeof d);
+    d.ns = m.ns;
+    d.nr = m.nr;
+    int nu_int = 1;
+    for (int s = 0; s < m.ns; ++s) {
+        if (!(m.mw[s] > 0))
+            return fail(h, EU_ERR_INVALID_ARGUMENT, "molecular weight of species %d not positive", s);
+        d.mw[s] = m.mw[s];
+        d.ri[s] = kRUniv / m.mw[s];
+        for (int k = 0; k < 9; ++k) {
+            d.clo[k][s] = m.coeff_lo[k * m.ns + s];
+            d.chi[k][s] = m.coeff_hi[k * m.ns + s];
+        }
+    }
+    for (int r = 0; r < m.nr; ++r) {
+        d.af[r] = m.af[r];
+        d.bf[r] = m.bf[r];
+        d.eaf[r] = m.eaf[r];
+        double xr = 0;
+        int tb = 0;
+        for (int s = 0; s < m.ns; ++s) {
+            const double f = m.stoi_f[s * m.nr + r], b = m.stoi_b[s * m.nr + r];
+            d.sf[r][s] = f;
+            d.sb[r][s] = b;
+            d.tb[r][s] = m.tb[s * m.nr + r];
+            xr += (b - f);
+            if (m.tb[s * m.nr + r] != 0)
+                tb = 1;
+            for (double v : {f, b})
+                if (!(v == 0.0 || v == 1.0 || v == 2.0))
+                    nu_int = 0;
+        }
+        d.xr[r] = xr;
+        d.has_tb[r] = tb;
+    }
+    d.nu_int = nu_int;
+    const bool first = !h->has_mech;
+    h->mech = m;
+    h->dmech = d;
+    h->has_mech = true;
+    if (!first)
+        return EU_OK;
+
+    // State buffers depend on ns: allocate them with the first mechanism.
+    const long long n3 = h->n3;
+    const int ns = m.ns;
+    eu_status s;
+    if ((s = dalloc(h, &h->st.prim, size_t(7 + ns) * n3)) != EU_OK) return s;
+    if (h->cfg.precision == EU_PREC_MIXED)
+        if ((s = dalloc(h, &h->st.prim32, size_t(7 + ns) * n3)) != EU_OK) return s;
+    if ((s = dalloc(h, &h->st.cs, size_t(ns + 4) * n3)) != EU_OK) return s;
+    if ((s = dalloc(h, &h->st.T, size_t(n3))) != EU_OK) return s;
+    if ((s = dalloc(h, &h->st.E, size_t(n3))) != EU_OK) return s;
+    if ((s = dalloc(h, &h->st.nchem, size_t(n3))) != EU_OK) return s;
+    if (h->cfg.record_sources)
+        if ((s = dalloc(h, &h->st.cms, size_t(ns) * n3)) != EU_OK) return s;
+    if ((s = dalloc(h, &h->st.counters, size_t(kCntCount))) != EU_OK) return s;
+    if ((s = dalloc(h, &h->d_scratch, size_t(n3))) != EU_OK) return s;
+    CK(h, cudaMemsetAsync(h->st.prim, 0, size_t(7 + ns) * n3 * sizeof(double), h->stream));
+    if (h->st.prim32)
+        CK(h, cudaMemsetAsync(h->st.prim32, 0, size_t(7 + ns) * n3 * sizeof(float), h->stream));
+    CK(h, cudaMemsetAsync(h->st.cs, 0, size_t(ns + 4) * n3 * sizeof(double), h->stream));
+    CK(h, cudaMemsetAsync(h->st.T, 0, size_t(n3) * sizeof(double), h->stream));
+    CK(h, cudaMemsetAsync(h->st.E, 0, size_t(n3) * sizeof(double), h->stream));
+    CK(h, cudaMemsetAsync(h->st.nchem, 0, size_t(n3) * sizeof(int), h->stream));
+    if (h->st.cms)
+        CK(h, cudaMemsetAsync(h->st.cms, 0, size_t(ns) * n3 * sizeof(double), h->stream));
+    CK(h, cudaMemsetAsync(h->st.counters, 0, kCntCount * sizeof(unsigned long long), h->stream));
+    return EU_OK;
+}
+
+LaunchArgs launch_args(eu_handle *h)
+{
+    LaunchArgs a;
+    a.mech = &h->dmech;
+    a.g = h->g;
+    a.st = h->st;
+    a.dt_dev = h->d_dt;
+    a.max_substeps = h->cfg.max_substeps > 0 ? h->cfg.max_substeps : (1 << 20);
+    a.precision = h->cfg.precision;
+    a.chemistry = h->cfg.chemistry;
+    a.stream = h->stream;
+    return a;
+}
+
+bool is_strict(const eu_handle *h) { return h->cfg.arith == EU_ARITH_STRICT; }
+
+
+} // namespace
+
+namespace eu3d {
+bool sizes_supported(int ns, int nr) { return ns == 9 && nr == 19; }
+} // namespace eu3d
+
+extern "C" {
+
+int eu_abi_version(void) { return EU3D_ABI_VERSION; }
+
+eu_status eu_read_grid(const char *grid_path, eu_config *cfg)
+{
+    if (!grid_path || !cfg)
+        return EU_ERR_INVALID_ARGUMENT;
+    GridSpec g;
+    std::string err;
+    if (!read_grid(grid_path, g, err))
+        return EU_ERR_IO;
+    cfg->total_ni = g.total_ni;
+    cfg->total_nj = g.total_nj;
+    cfg->total_nk = g.total_nk;
+    cfg->xa = g.xa;
+    cfg->xb = g.xb;
+    cfg->ya = g.ya;
+    cfg->yb = g.yb;
+    cfg->za = g.za;
+    cfg->zb = g.zb;
+    cfg->bc = g.bc;
+    return EU_OK;
+}
+
+namespace {
+MechanismTables tables_from(const eu_mechanism *mm)
+{
+    MechanismTables m;
+    m.ns = mm->ns;
+    m.nr = mm->nr;
+    const int ns = m.ns, nr = m.nr;
+    m.mw.assign(mm->mw, mm->mw + ns);
+    m.coeff_lo.assign(mm->coeff_lo, mm->coeff_lo + 9 * ns);
+    m.coeff_hi.assign(mm->coeff_hi, mm->coeff_hi + 9 * ns);
+    m.af.assign(mm->af, mm->af + nr);
+    m.bf.assign(mm->bf, mm->bf + nr);
+    m.eaf.assign(mm->eaf, mm->eaf + nr);
+    m.stoi_f.assign(mm->stoi_f, mm->stoi_f + ns * nr);
+    m.stoi_b.assign(mm->stoi_b, mm->stoi_b + ns * nr);
+    m.tb.assign(mm->tb, mm->tb + ns * nr);
+    return m;
+}
+
+bool mechanism_complete(const eu_mechanism *mm)
+{
+    return mm && mm->mw && mm->coeff_lo && mm->coeff_hi && mm->af && mm->bf && mm->eaf && mm->stoi_f &&
+           mm->stoi_b && mm->tb && mm->ns > 0 && mm->nr > 0 && mm->ns <= kMaxS && mm->nr <= kMaxR;
+}
+} // namespace
+
+eu_status eu_parse_mechanism(const char *mech_path, const char *thermo_path, int *ns, int *nr, double *mw,
+                             double *coeff_lo, double *coeff_hi, double *af, double *bf, double *eaf,
+                             double *stoi_f, double *stoi_b, double *tb)
+{
+    if (!mech_path || !thermo_path)
+        return EU_ERR_INVALID_ARGUMENT;
+    MechanismTables m;
+    std::string err;
+    if (!read_mechanism(mech_path, thermo_path, m, err))
+        return EU_ERR_IO;
+    if (ns) *ns = m.ns;
+    if (nr) *nr = m.nr;
+    auto cp = [](double *dst, const std::vector<double> &v) {
+        if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(double));
+    };
+    cp(mw, m.mw);
+    cp(coeff_lo, m.coeff_lo);
+    cp(coeff_hi, m.coeff_hi);
+    cp(af, m.af);
+    cp(bf, m.bf);
+    cp(eaf, m.eaf);
+    cp(stoi_f, m.stoi_f);
+    cp(stoi_b, m.stoi_b);
+    cp(tb, m.tb);
+    return EU_OK;
+}
+
+eu_status eu_initial_state(const eu_mechanism *mm, int ni, int nj, int nk, int bc, const double *P, const double *T,
+                           const double *U, const double *V, const double *W, const double *Y, double *prim,
+                           double *cs, double *T_out, double *E_out)
+{
+    if (!mechanism_complete(mm) || !P || !T || !U || !V || !W || !Y || !prim || !cs || !T_out || !E_out || bc < 1 ||
+        ni < 2 || nj < 2 || nk < 2)
+        return EU_ERR_INVALID_ARGUMENT;
+    const MechanismTables m = tables_from(mm);
+    std::vector<double> pv, cv, tv, ev;
+    primitive_to_state(m, ni, nj, nk, bc, P, T, U, V, W, Y, pv, cv, tv, ev);
+    std::memcpy(prim, pv.data(), pv.size() * sizeof(double));
+    std::memcpy(cs, cv.data(), cv.size() * sizeof(double));
+    std::memcpy(T_out, tv.data(), tv.size() * sizeof(double));
+    std::memcpy(E_out, ev.data(), ev.size() * sizeof(double));
+    return EU_OK;
+}
+
+eu_status eu_create(const eu_config *cfg, eu_handle **out)
+{
+    if (!cfg || !out)
+        return EU_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (cfg->bc != 2 || cfg->total_ni < 2 || cfg->total_nj < 2 || cfg->total_nk < 2)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (cfg->precision != EU_PREC_FP64 && cfg->precision != EU_PREC_MIXED)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (cfg->chemistry != EU_CHEM_STIFF && cfg->chemistry != EU_CHEM_FROZEN && cfg->chemistry != EU_CHEM_LEARNED)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (cfg->chemistry == EU_CHEM_LEARNED)
+        return EU_ERR_UNSUPPORTED;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return EU_ERR_CUDA;
+    if (cfg->device < 0 || cfg->device >= ndev)
+        return EU_ERR_INVALID_ARGUMENT;
+    eu_handle *h = new (std::nothrow) eu_handle;
+    if (!h)
+        return EU_ERR_OUT_OF_MEMORY;
+    h->cfg = *cfg;
+    if (cudaSetDevice(cfg->device) != cudaSuccess) {
+        delete h;
+        return EU_ERR_CUDA;
+    }
+    h->ni = cfg->total_ni;
+    h->nj = cfg->total_nj;
+    h->nk = cfg->total_nk;
+    h->bc = cfg->bc;
+    h->nx = h->ni + 2 * h->bc;
+    h->ny = h->nj + 2 * h->bc;
+    h->nz = h->nk + 2 * h->bc;
+    h->n3 = (long long)h->nx * h->ny * h->nz;
+    h->x = node_coordinates(h->ni, cfg->xa, cfg->xb, h->bc);
+    h->y = node_coordinates(h->nj, cfg->ya, cfg->yb, h->bc);
+    h->z = node_coordinates(h->nk, cfg->za, cfg->zb, h->bc);
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+        eu_destroy(h);
+        return EU_ERR_CUDA;
+    }
+    for (auto &e : h->pev)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            eu_destroy(h);
+            return EU_ERR_CUDA;
+        }
+    eu_status s;
+    if ((s = dalloc(h, &h->d_xyz, size_t(h->nx + h->ny + h->nz))) != EU_OK ||
+        (s = dalloc(h, &h->d_dt, size_t(1))) != EU_OK) {
+        eu_destroy(h);
+        return s;
+    }
+    std::vector<double> xyz;
+    xyz.insert(xyz.end(), h->x.begin(), h->x.end());
+    xyz.insert(xyz.end(), h->y.begin(), h->y.end());
+    xyz.insert(xyz.end(), h->z.begin(), h->z.end());
+    if (cudaMemcpy(h->d_xyz, xyz.data(), xyz.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+        eu_destroy(h);
+        return EU_ERR_CUDA;
+    }
+    h->g.ni = h->ni;
+    h->g.nj = h->nj;
+    h->g.nk = h->nk;
+    h->g.bc = h->bc;
+    h->g.nx = h->nx;
+    h->g.ny = h->ny;
+    h->g.nz = h->nz;
+    h->g.n3 = h->n3;
+    h->g.x = h->d_xyz;
+    h->g.y = h->d_xyz + h->nx;
+    h->g.z = h->d_xyz + h->nx + h->ny;
+    *out = h;
+    return EU_OK;
+}
+
+eu_status eu_destroy(eu_handle *h)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(h->cfg.device);
+    if (h->stream)
+        cudaStreamSynchronize(h->stream);
+    free_all(h);
+    for (auto &e : h->pev)
+        if (e) cudaEventDestroy(e);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return EU_OK;
+}
+
+const char *eu_last_error(const eu_handle *h) { return h ? h->err.c_str() : kNoHandle; }
+
+eu_status eu_load_mechanism(eu_handle *h, const char *mech_path, const char *thermo_path)
+{
+    if (!h || !mech_path || !thermo_path)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(h->cfg.device);
+    MechanismTables m;
+    std::string err;
+    if (!read_mechanism(mech_path, thermo_path, m, err))
+        return fail(h, EU_ERR_IO, "%s", err.c_str());
+    return install_mechanism(h, m);
+}
+
+eu_status eu_set_mechanism(eu_handle *h, const eu_mechanism *mm)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!mechanism_complete(mm))
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "null table or sizes out of range");
+    cudaSetDevice(h->cfg.device);
+    return install_mechanism(h, tables_from(mm));
+}
+
+eu_status eu_get_mechanism(const eu_handle *h, int *ns, int *nr, double *mw, double *coeff_lo, double *coeff_hi,
+                           double *af, double *bf, double *eaf, double *stoi_f, double *stoi_b, double *tb)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!h->has_mech)
+        return EU_ERR_NOT_READY;
+    const MechanismTables &m = h->mech;
+    if (ns) *ns = m.ns;
+    if (nr) *nr = m.nr;
+    auto cp = [](double *dst, const std::vector<double> &v) {
+        if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(double));
+    };
+    cp(mw, m.mw);
+    cp(coeff_lo, m.coeff_lo);
+    cp(coeff_hi, m.coeff_hi);
+    cp(af, m.af);
+    cp(bf, m.bf);
+    cp(eaf, m.eaf);
+    cp(stoi_f, m.stoi_f);
+    cp(stoi_b, m.stoi_b);
+    cp(tb, m.tb);
+    return EU_OK;
+}
+
+eu_status eu_node_coordinates(const eu_handle *h, double *x, double *y, double *z)
+{
+    if (!h || !x || !y || !z)
+        return EU_ERR_INVALID_ARGUMENT;
+    std::memcpy(x, h->x.data(), h->x.size() * sizeof(double));
+    std::memcpy(y, h->y.data(), h->y.size() * sizeof(double));
+    std::memcpy(z, h->z.data(), h->z.size() * sizeof(double));
+    return EU_OK;
+}
+
+eu_status eu_set_state(eu_handle *h, const double *cs, const double *T, const double *E, const double *P,
+                       const double *D, const double *U, const double *V, const double *W, const double *H,
+                       const double *G, const double *Y)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!cs || !T || !E || !P || !D || !U || !V || !W || !H || !G || !Y)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "null argument");
+    if (!h->has_mech)
+        return fail(h, EU_ERR_NOT_READY, "load a mechanism first");
+    cudaSetDevice(h->cfg.device);
+    const long long n3 = h->n3;
+    const int ns = h->mech.ns;
+    const size_t b = size_t(n3) * sizeof(double);
+    const double *planes[7] = {P, D, U, V, W, H, G};
+    for (int f = 0; f < 7; ++f) CK(h, cudaMemcpyAsync(h->st.prim + f * n3, planes[f], b, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->st.prim + 7 * n3, Y, ns * b, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->st.cs, cs, (ns + 4) * b, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->st.T, T, b, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->st.E, E, b, cudaMemcpyHostToDevice, h->stream));
+    if (h->st.prim32) {
+        std::vector<float> f32(size_t(7 + ns) * n3);
+        for (int f = 0; f < 7; ++f)
+            for (long long c = 0; c < n3; ++c) f32[f * n3 + c] = float(planes[f][c]);
+        for (long long c = 0; c < ns * n3; ++c) f32[7 * n3 + c] = float(Y[c]);
+        CK(h, cudaMemcpyAsync(h->st.prim32, f32.data(), f32.size() * sizeof(float), cudaMemcpyHostToDevice,
+                              h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+    }
+    CK(h, cudaStreamSynchronize(h->stream));
+    h->has_state = true;
+    return EU_OK;
+}
+
+eu_status eu_set_primitive(eu_handle *h, const double *P, const double *T, const double *U, const double *V,
+                           const double *W, const double *Y)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!P || !T || !U || !V || !W || !Y)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "null argument");
+    if (!h->has_mech)
+        return fail(h, EU_ERR_NOT_READY, "load a mechanism first");
+    std::vector<double> prim, cs, Tv, Ev;
+    primitive_to_state(h->mech, h->ni, h->nj, h->nk, h->bc, P, T, U, V, W, Y, prim, cs, Tv, Ev);
+    const long long n3 = h->n3;
+    return eu_set_state(h, cs.data(), Tv.data(), Ev.data(), &prim[0], &prim[n3], &prim[2 * n3], &prim[3 * n3],
+                        &prim[4 * n3], &prim[5 * n3], &prim[6 * n3], &prim[7 * n3]);
+}
+
+eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (nsteps < 0 || !(dt > 0))
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "nsteps must be >= 0 and dt > 0");
+    if (!h->has_mech || !h->has_state)
+        return fail(h, EU_ERR_NOT_READY, "mechanism and state must be set before stepping");
+    cudaSetDevice(h->cfg.device);
+    const bool prof = h->cfg.profile != 0 && stats != nullptr;
+    const LaunchArgs a = launch_args(h);
+    const bool react = h->cfg.chemistry == EU_CHEM_STIFF;
+    const bool st_ = is_strict(h);
+    double phase[4] = {0, 0, 0, 0};
+    int launches = 0;
+    if (stats)
+        CK(h, cudaEventRecord(h->ev0, h->stream));
+    CK(h, cudaMemsetAsync(h->st.counters, 0, kCntCount * sizeof(unsigned long long), h->stream));
+    CK(h, strict::launch_set_value(h->d_dt, dt, h->stream));
+    ++launches;
+    for (int n = 0; n < nsteps; ++n) {
+        CK(h, cudaMemsetAsync(h->st.counters, 0, kCntPerStep * sizeof(unsigned long long), h->stream));
+        if (prof) CK(h, cudaEventRecord(h->pev[0], h->stream));
+        CK(h, st_ ? strict::launch_boundary(a) : fast::launch_boundary(a));
+        if (prof) CK(h, cudaEventRecord(h->pev[1], h->stream));
+        CK(h, st_ ? strict::launch_flux_update(a) : fast::launch_flux_update(a));
+        if (prof) CK(h, cudaEventRecord(h->pev[2], h->stream));
+        CK(h, st_ ? strict::launch_recover_react(a, react) : fast::launch_recover_react(a, react));
+        if (prof) {
+            CK(h, cudaEventRecord(h->pev[3], h->stream));
+            CK(h, cudaEventSynchronize(h->pev[3]));
+            for (int q = 0; q < 3; ++q) {
+                float ms = 0;
+                CK(h, cudaEventElapsedTime(&ms, h->pev[q], h->pev[q + 1]));
+                phase[q] += ms;
+            }
+        }
+        launches += 3;
+    }
+    if (!stats)
+        return EU_OK;
+    CK(h, cudaEventRecord(h->ev1, h->stream));
+    unsigned long long cnt[kCntCount];
+    CK(h, cudaMemcpyAsync(cnt, h->st.counters, sizeof cnt, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    float ms = 0;
+    CK(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    std::memset(stats, 0, sizeof *stats);
+    stats->steps = nsteps;
+    stats->max_nchem = int(cnt[kCntMaxNchem]);
+    stats->sum_nchem = (long long)cnt[kCntSumNchem];
+    stats->reacting = react ? (long long)h->ni * h->nj * h->nk : 0;
+    stats->nonfinite = (long long)cnt[kCntNonfinite];
+    stats->device_ms = ms;
+    stats->launches = launches;
+    for (int q = 0; q < 4; ++q) stats->phase_ms[q] = phase[q];
+    if (cnt[kCntNonfinite])
+        return fail(h, EU_ERR_NONFINITE, "%llu cells with non-finite density or temperature", cnt[kCntNonfinite]);
+    if (cnt[kCntBadNchem])
+        return fail(h, EU_ERR_NCHEM, "%llu cells predicted Nchem <= 0 or above max_substeps", cnt[kCntBadNchem]);
+    return EU_OK;
+}
+
+eu_status eu_get_field(eu_handle *h, const char *name, double *out)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!name || !out)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "null argument");
+    if (!h->has_mech)
+        return fail(h, EU_ERR_NOT_READY, "no state");
+    cudaSetDevice(h->cfg.device);
+    const long long n3 = h->n3;
+    const int ns = h->mech.ns;
+    const size_t b = size_t(n3) * sizeof(double);
+    const std::string n(name);
+    const char *prim_names[7] = {"P", "D", "U", "V", "W", "H", "Gamma"};
+    for (int f = 0; f < 7; ++f)
+        if (n == prim_names[f]) {
+            CK(h, cudaMemcpyAsync(out, h->st.prim + f * n3, b, cudaMemcpyDeviceToHost, h->stream));
+            CK(h, cudaStreamSynchronize(h->stream));
+            return EU_OK;
+        }
+    const double *src = nullptr;
+    size_t planes = 1;
+    if (n == "T") src = h->st.T;
+    else if (n == "E") src = h->st.E;
+    else if (n == "Yi") { src = h->st.prim + 7 * n3; planes = ns; }
+    else if (n == "CS") { src = h->st.cs; planes = ns + 4; }
+    else if (n == "Di" || n == "Mc") { src = h->st.cs; planes = ns; }
+    else if (n == "CMS") {
+        if (!h->st.cms)
+            return fail(h, EU_ERR_INVALID_ARGUMENT, "CMS needs record_sources in the config");
+        src = h->st.cms;
+        planes = ns;
+    }
+    if (src) {
+        CK(h, cudaMemcpyAsync(out, src, planes * b, cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        if (n == "Mc") // Update_after_CS: Mc = Di / Mw * 1000 (src/Flowfield.cpp:1589)
+            for (int s = 0; s < ns; ++s)
+                for (long long c = 0; c < n3; ++c) out[s * n3 + c] = out[s * n3 + c] / h->mech.mw[s] * 1000;
+        return EU_OK;
+    }
+    if (n == "Nchem") {
+        std::vector<int> v(n3);
+        CK(h, cudaMemcpyAsync(v.data(), h->st.nchem, n3 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        for (long long c = 0; c < n3; ++c) out[c] = v[c];
+        return EU_OK;
+    }
+    const char *derived[5] = {"Wav", "Rgas", "Cp", "C", "Ma"};
+    for (int w = 0; w < 5; ++w)
+        if (n == derived[w]) {
+            const LaunchArgs a = launch_args(h);
+            CK(h, is_strict(h) ? strict::launch_derived(a, w, h->d_scratch) : fast::launch_derived(a, w, h->d_scratch));
+            CK(h, cudaMemcpyAsync(out, h->d_scratch, b, cudaMemcpyDeviceToHost, h->stream));
+            CK(h, cudaStreamSynchronize(h->stream));
+            return EU_OK;
+        }
+    return fail(h, EU_ERR_INVALID_ARGUMENT, "unknown field %s", name);
+}
+
+eu_status eu_sync(eu_handle *h)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(h->cfg.device);
+    CK(h, cudaStreamSynchronize(h->stream));
+    return EU_OK;
+}
+
+eu_status eu_device_info(const eu_handle *h, void **stream, size_t *device_bytes)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (stream) *stream = h->stream;
+    if (device_bytes) *device_bytes = h->bytes;
+    return EU_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,189 @@
+/*
+ * eu3d.h — C ABI of the B200 EU3D reacting-Euler timestep library (libeu3d.so).
+ *
+ * One handle owns one solution (a haloed node grid, a mechanism and every device
+ * buffer) on one GPU and one CUDA stream. Several handles may coexist in one
+ * process; a handle is not thread-safe, distinct handles are.
+ *
+ * Host arrays are structure-of-arrays over the reference's haloed node grid:
+ * nx = total_ni + 2*bc, ny = total_nj + 2*bc, nz = total_nk + 2*bc, node
+ * (i,j,k) at c = (i*ny + j)*nz + k (k fastest, the reference's Array<double,3>
+ * order); species and conserved components are consecutive planes of nx*ny*nz
+ * doubles. Every call returns an eu_status; nothing exits the process.
+ *
+ * The entry points replace the reference's C++-linkage GPU glue:
+ *   eu_step            Euler::Computing loop body (src/Euler.cpp:322-376) with
+ *                      FieldBoundary_3dRSBI, Flowfield::Advection -> muscl_ausm_host
+ *                      (include/FlowfieldCuda.cuh:53-67) + TimeAdv::EE_GPU/launch_ee_cuda
+ *                      (include/TimeAdvCuda.cuh:4-15), Update_after_Adv ->
+ *                      post_advection_state_host / post_advection_from_ee_host
+ *                      (include/ReactionCuda.cuh:266, :282) and Euler::Trapezoid(1) ->
+ *                      reaction_cells_host (include/ReactionCuda.cuh:230-248)
+ *   eu_load_mechanism  Reaction::ReactionRead (src/Reaction.cpp:156-327)
+ *   eu_read_grid       Mesh::MeshProcess (src/Mesh.cpp:36-84)
+ *   eu_set_primitive   Flowfield::FieldInitial (src/Flowfield.cpp:193-264)
+ *   eu_get_field       reaction_packed_output / download_resident_output
+ *                      (include/ReactionCuda.cuh:274, :287) and the host scatter of
+ *                      Flowfield::Update_after_Adv (src/Flowfield.cpp:1432-1450)
+ */
+#ifndef EU3D_H
+#define EU3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EU3D_ABI_VERSION 1
+#define EU3D_MAX_SPECIES 16   /* include/ReactionCuda.cuh:4 */
+#define EU3D_MAX_REACTIONS 24 /* include/ReactionCuda.cuh:5 */
+
+typedef struct eu_handle eu_handle;
+
+typedef enum {
+    EU_OK = 0,
+    EU_ERR_INVALID_ARGUMENT = 1, /* bad pointer, size, name or option */
+    EU_ERR_CUDA = 2,             /* a CUDA runtime call failed; see eu_last_error */
+    EU_ERR_OUT_OF_MEMORY = 3,
+    EU_ERR_IO = 4,               /* an input file is missing or does not parse */
+    EU_ERR_NONFINITE = 5,        /* a density or temperature became non-finite */
+    EU_ERR_NCHEM = 6,            /* a cell predicted Nchem <= 0 (the reference aborts,
+                                    src/Reaction.cpp:936-940) or above max_substeps */
+    EU_ERR_NOT_READY = 7,        /* call order: no mechanism or no state yet */
+    EU_ERR_UNSUPPORTED = 8,      /* configuration outside what this build implements */
+    EU_ERR_TIMEOUT = 9           /* a bounded device wait gave up */
+} eu_status;
+
+typedef enum {
+    EU_PREC_FP64 = 0,  /* every flux, update, recovery and kinetics operation in FP64 */
+    EU_PREC_MIXED = 1  /* MUSCL/AUSM in FP32; conserved update, recovery and kinetics FP64 */
+} eu_precision;
+
+typedef enum {
+    EU_CHEM_STIFF = 0,   /* the reference's adaptive trapezoid kinetics on every cell */
+    EU_CHEM_FROZEN = 1,  /* no kinetics (advection and state recovery only) */
+    EU_CHEM_LEARNED = 2  /* learned-chemistry MLP with trust gate, stiff fallback */
+} eu_chemistry;
+
+typedef enum {
+    EU_ARITH_STRICT = 0, /* no FMA contraction: rounds as the reference's CPU build */
+    EU_ARITH_FAST = 1    /* FMA contraction allowed */
+} eu_arith;
+
+typedef struct {
+    int total_ni, total_nj, total_nk; /* nodes per axis (grid file total_ni, ...) */
+    double xa, xb, ya, yb, za, zb;    /* domain extents (grid file xa, xb, ...) */
+    int bc;                           /* ghost layers per side; must be 2 (MUSCL_2 stencil) */
+    int device;                       /* CUDA device ordinal */
+    int precision;                    /* eu_precision */
+    int chemistry;                    /* eu_chemistry */
+    int arith;                        /* eu_arith */
+    int max_substeps;                 /* Nchem cap; 0 selects 1 << 20 */
+    int record_sources;               /* nonzero: keep per-cell mass sources (CMS) */
+    int profile;                      /* nonzero: time each kernel phase with CUDA events */
+} eu_config;
+
+/* Mechanism and thermo tables in the reference's layouts (src/Reaction.cpp:156-327). */
+typedef struct {
+    int ns, nr;
+    const double *mw;       /* [ns] molecular weights, g/mol */
+    const double *coeff_lo; /* [9*ns] Coeff0 (T < 1000 K), (k, s) row-major: a1..a7, b1, b2 */
+    const double *coeff_hi; /* [9*ns] Coeff1 */
+    const double *af;       /* [nr] pre-exponential factors */
+    const double *bf;       /* [nr] temperature exponents */
+    const double *eaf;      /* [nr] activation energies, cal/mol */
+    const double *stoi_f;   /* [ns*nr] reactant coefficients, (s, r) row-major */
+    const double *stoi_b;   /* [ns*nr] product coefficients */
+    const double *tb;       /* [ns*nr] third-body efficiencies (all 0 for ordinary reactions) */
+} eu_mechanism;
+
+/* Per-call step statistics (device counters read back after the last step). */
+typedef struct {
+    int steps;
+    int max_nchem;          /* largest Nchem of the last step */
+    long long sum_nchem;    /* substeps over all cells, last step */
+    long long reacting;     /* cells given to the kinetics in the last step */
+    long long learned;      /* cells advanced by the learned model (EU_CHEM_LEARNED) */
+    long long fallback;     /* cells the trust gate sent back to the stiff path */
+    long long nonfinite;    /* cells with non-finite density or temperature */
+    double device_ms;       /* device time of the call (CUDA events) */
+    double phase_ms[4];     /* with cfg.profile: ghost fill, flux + update, recovery + kinetics, other */
+    int launches;           /* kernels launched by the call */
+} eu_step_stats;
+
+/* Library version / ABI check. */
+int eu_abi_version(void);
+
+/* Parse a grid file in the reference's format (input/grid-*.txt) into cfg's
+ * grid members; other members are left as they are. */
+eu_status eu_read_grid(const char *grid_path, eu_config *cfg);
+
+/* Parse a mechanism file and thermo.dat (reference formats) without a device.
+ * Replaces Reaction::ReactionRead (src/Reaction.cpp:156-327). Pass NULL arrays
+ * to query ns/nr first; arrays sized as in eu_mechanism. */
+eu_status eu_parse_mechanism(const char *mech_path, const char *thermo_path, int *ns, int *nr, double *mw,
+                             double *coeff_lo, double *coeff_hi, double *af, double *bf, double *eaf,
+                             double *stoi_f, double *stoi_b, double *tb);
+
+/* Host-only initial state (no device): Flowfield::FieldInitial's derived fields
+ * (src/Flowfield.cpp:226-262) from primitives over the haloed grid of
+ * total_ni x total_nj x total_nk nodes with bc ghosts. Outputs: prim (7+ns planes:
+ * P D U V W H Gamma Y...), cs (ns+4 planes), T, E (1 plane each). */
+eu_status eu_initial_state(const eu_mechanism *m, int total_ni, int total_nj, int total_nk, int bc,
+                           const double *P, const double *T, const double *U, const double *V, const double *W,
+                           const double *Y, double *prim, double *cs, double *T_out, double *E_out);
+
+/* Create a handle: allocates every device buffer for cfg's grid on cfg->device. */
+eu_status eu_create(const eu_config *cfg, eu_handle **out);
+eu_status eu_destroy(eu_handle *h);
+
+/* Text of the last error on this handle (never NULL). */
+const char *eu_last_error(const eu_handle *h);
+
+/* Read a mechanism file and thermo.dat in the reference's formats
+ * (input/H2_JA919.txt, input/thermo.dat). */
+eu_status eu_load_mechanism(eu_handle *h, const char *mech_path, const char *thermo_path);
+/* Install mechanism tables directly (copied). */
+eu_status eu_set_mechanism(eu_handle *h, const eu_mechanism *m);
+/* Copy the installed tables out; each pointer of m must have room for the sizes
+ * above (ns, nr are filled first; pass NULL arrays to query sizes only). */
+eu_status eu_get_mechanism(const eu_handle *h, int *ns, int *nr, double *mw, double *coeff_lo,
+                           double *coeff_hi, double *af, double *bf, double *eaf, double *stoi_f,
+                           double *stoi_b, double *tb);
+
+/* Node coordinates with mirrored ghosts (src/Mesh.cpp:96-142), lengths nx, ny, nz. */
+eu_status eu_node_coordinates(const eu_handle *h, double *x, double *y, double *z);
+
+/* Initial condition from primitive fields over the haloed grid (host arrays;
+ * Y has ns planes). Derived fields follow Flowfield::FieldInitial. */
+eu_status eu_set_primitive(eu_handle *h, const double *P, const double *T, const double *U, const double *V,
+                           const double *W, const double *Y);
+
+/* Exact state injection: conserved CS (ns+4 planes), T, E, and the primitives the
+ * stencils read (P, D, U, V, W, H, Gamma, Y) over the haloed grid. */
+eu_status eu_set_state(eu_handle *h, const double *cs, const double *T, const double *E, const double *P,
+                       const double *D, const double *U, const double *V, const double *W, const double *H,
+                       const double *G, const double *Y);
+
+/* Advance nsteps timesteps of fixed dt. Asynchronous on the handle's stream
+ * unless stats is non-NULL (then it synchronises and fills stats). */
+eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats);
+
+/* Copy a named field to host (haloed SoA planes). Names: P D T U V W H E Gamma
+ * C Ma Wav Rgas Cp (1 plane); Yi Di Mc CMS (ns planes); CS (ns+4 planes); Nchem
+ * (1 plane, as doubles). Synchronises the handle's stream. */
+eu_status eu_get_field(eu_handle *h, const char *name, double *host_out);
+
+/* Wait for all work queued on the handle. */
+eu_status eu_sync(eu_handle *h);
+
+/* Device pointers and the stream of a handle, for callers that keep inputs
+ * resident and time kernels themselves. */
+eu_status eu_device_info(const eu_handle *h, void **stream, size_t *device_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EU3D_H */

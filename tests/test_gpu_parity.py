@@ -1,0 +1,122 @@
+"""Parity of the CUDA timestep (libeu3d.so) with the reference, on a B200.
+
+The reference's outputs come from the committed golden fixtures (produced by
+the reference's own CPU code, tests/golden/make_golden.py) and, at sizes the
+fixtures do not cover, from the CPU restatement oracle/eu3d_oracle.c, which is
+pinned value-for-value to the reference (tests/test_oracle_pin.py).
+
+Tolerances:
+  strict arithmetic (no FMA): relative L-inf per field <= 1e-12 after 3 steps,
+    <= 1e-9 per conserved variable after 100 steps (the required bound), Nchem exact;
+  fast arithmetic (FMA): <= 1e-9 per conserved variable after 100 steps;
+  mixed precision (FP32 MUSCL/AUSM): species mass-fraction L1 error <= 1e-3 of
+    the FP64 run, stated, not exact.
+"""
+import numpy as np
+import pytest
+
+import eu3d_cases as cases
+from helpers import golden, golden_mechanism, init_state, interior, n_unequal, rel_linf
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ["CS", "T", "E", "P", "D", "U", "V", "W", "H", "Gamma", "Yi", "Nchem", "CMS", "Mc", "Di", "Wav", "Rgas",
+          "Cp", "C", "Ma"]
+
+
+def solver_from_golden(eu3d, z, arith="strict", precision="fp64"):
+    ext = tuple(float(v) for v in z["extent"])
+    s = eu3d.Solver(int(z["ni"]), int(z["nj"]), int(z["nk"]), ext, arith=arith, precision=precision,
+                    record_sources=True)
+    s.load_mechanism(cases.MECH_JA919, cases.THERMO)
+    if "init_CS" in z:
+        s.set_state(init_state(z))
+    else:
+        s.set_primitive(*[z[f"prim_{k}"] for k in "PTUVWY"])
+    return s
+
+
+def test_nodes_match_reference(gpu):
+    z = golden("rsbi_17x13x4_s3.npz")
+    s = solver_from_golden(gpu, z)
+    for got, want in zip(s.nodes(), (z["x"], z["y"], z["z"])):
+        assert np.array_equal(got, want)
+
+
+def test_strict_three_steps_every_field(gpu):
+    z = golden("rsbi_17x13x4_s3.npz")
+    s = solver_from_golden(gpu, z)
+    st = s.step(int(z["steps"]), float(z["dt"]))
+    assert st["nonfinite"] == 0
+    for f in FIELDS:
+        got = interior(s.get(f))
+        want = z[f"out_{f}"]
+        if f == "Nchem":
+            assert n_unequal(got, want) == 0
+        else:
+            assert rel_linf(got, want).max() <= 1e-12, (f, rel_linf(got, want).max())
+
+
+@pytest.mark.parametrize("arith", ["strict", "fast"])
+def test_hundred_steps_conserved_variables(gpu, arith):
+    """The required bound: relative L-inf <= 1e-9 per conserved variable after 100 steps."""
+    z = golden("rsbi_36x18x3_s100.npz")
+    s = solver_from_golden(gpu, z, arith=arith)
+    st = s.step(int(z["steps"]), float(z["dt"]))
+    assert st["max_nchem"] == int(z["out_Nchem"].max())
+    err = rel_linf(interior(s.get("CS")), z["out_CS"])
+    assert err.max() <= 1e-9, err
+    assert n_unequal(interior(s.get("Nchem")), z["out_Nchem"]) == 0
+    assert rel_linf(interior(s.get("T")), z["out_T"]).max() <= 1e-9
+
+
+@pytest.mark.parametrize("arith", ["strict", "fast"])
+def test_shock_bubble_twenty_steps(gpu, arith):
+    z = golden("bubble_25x13x13_s20.npz")
+    s = solver_from_golden(gpu, z, arith=arith)
+    s.step(int(z["steps"]), float(z["dt"]))
+    err = rel_linf(interior(s.get("CS")), z["out_CS"])
+    assert err.max() <= (1e-11 if arith == "strict" else 1e-9), err
+    assert rel_linf(interior(s.get("CMS")), z["out_CMS"]).max() <= 1e-8
+    assert n_unequal(interior(s.get("Nchem")), z["out_Nchem"]) == 0
+
+
+def test_larger_grid_against_restatement(gpu, port_lib):
+    """A grid the fixtures do not cover, against the pinned C restatement."""
+    ni, nj, nk = 49, 25, 25
+    ext = (0.0, 0.024, 0.0, 0.012, 0.0, 0.012)
+    mech = golden_mechanism()
+    x, y, zc = (cases.node_coordinates(n, a, b) for n, a, b in ((ni, 0, 0.024), (nj, 0, 0.012), (nk, 0, 0.012)))
+    prim = cases.shock_bubble(x, y, zc, mech.mw, 9, radius=4e-3, shock_x=3e-3, standoff=5e-3, seed=3)
+    port = port_lib(ni, nj, nk, x, y, zc, mech)
+    port.set_primitive(*prim)
+    s = gpu.Solver(ni, nj, nk, ext, record_sources=True)
+    s.set_mechanism(mech)
+    s.set_primitive(*prim)
+    port.step(30, 5e-8)
+    s.step(30, 5e-8)
+    assert rel_linf(interior(s.get("CS")), interior(port.get("CS"))).max() <= 1e-10
+    assert n_unequal(interior(s.get("Nchem")), interior(port.get("Nchem"))) == 0
+
+
+def test_mixed_precision_error_is_bounded(gpu):
+    """FP32 reconstruction + AUSM, FP64 update/recovery/kinetics: the species
+    mass fractions stay within L1 1e-3 of the all-FP64 run (error stated)."""
+    z = golden("bubble_25x13x13_s20.npz")
+    a = solver_from_golden(gpu, z)
+    b = solver_from_golden(gpu, z, precision="mixed")
+    a.step(20, float(z["dt"]))
+    b.step(20, float(z["dt"]))
+    ya, yb = interior(a.get("Yi")), interior(b.get("Yi"))
+    l1 = np.abs(ya - yb).sum(axis=0).mean()
+    assert l1 <= 1e-3, l1
+    assert rel_linf(interior(b.get("CS")), interior(a.get("CS"))).max() <= 1e-3
+
+
+def test_deterministic(gpu):
+    z = golden("bubble_25x13x13_s20.npz")
+    a = solver_from_golden(gpu, z, arith="fast")
+    b = solver_from_golden(gpu, z, arith="fast")
+    a.step(10, float(z["dt"]))
+    b.step(10, float(z["dt"]))
+    assert n_unequal(a.get("CS"), b.get("CS")) == 0
