@@ -19,6 +19,29 @@ __device__ __forceinline__ long long cell_index(const DevGrid &g, int i, int j, 
     return ((long long)i * g.ny + j) * g.nz + k;
 }
 
+// Reciprocal of a nonzero, non-denormal double by the hardware approximation
+// (rcp.approx.ftz.f64) refined with two Newton-Raphson steps
+// y <- y + y (1 - a y); relative error near one unit in the last place.
+__device__ __forceinline__ double rcp_nr(double a)
+{
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+    double e = fma(-a, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-a, y, 1.0);
+    return fma(y, e, y);
+}
+
+// q = n / d without an IEEE division: exact division only for d == 0 (the
+// hardware approximation is not valid there).
+__device__ __forceinline__ double div_fast(double n, double d)
+{
+    if (d == 0.0)
+        return n / d;
+    return n * rcp_nr(d);
+}
+__device__ __forceinline__ float div_fast(float n, float d) { return __fdividef(n, d); }
+
 // ------------------------------------------------------------------ thermo
 // NASA 9-coefficient polynomials (src/Reaction.cpp:1165-1220). T powers are
 // formed once per temperature.
@@ -95,6 +118,7 @@ __device__ __forceinline__ double s_species(const DevMech &m, const TPow &p, dou
 // Flowfield::Get_temp (src/Flowfield.cpp:2072-2131): Newton on
 // sum_s Y_s h_s(T) - E*1e-3 - (sum_s Y_s R_s) T = 0, at most 10 iterations,
 // stop when |dT| < 1e-6 K. E is the cell's previous internal energy.
+#ifdef EU_STRICT
 template <int NS>
 __device__ __forceinline__ double newton_temperature(const DevMech &m, double T, double E, const double (&Y)[NS])
 {
@@ -119,6 +143,71 @@ __device__ __forceinline__ double newton_temperature(const DevMech &m, double T,
     }
     return T_temp;
 }
+#else
+// Mixture polynomial of one NASA range: c_k = sum_s Y_s R_s a_k,s, with the
+// enthalpy's divisors folded in (h/R uses a_k T^(k-1)/(k-1) for k >= 3).
+template <int NS>
+struct MixPoly {
+    double a0, a1, a2, a3, a4, a5, a6, a7; // cp form: a0/T^2 + a1/T + a2 + a3 T + ... + a6 T^4
+    double h3, h4, h5, h6;                 // a3/2, a4/3, a5/4, a6/5
+};
+
+template <int NS>
+__device__ __forceinline__ void mix_poly(const DevMech &m, const double (&Y)[NS], bool low, MixPoly<NS> &c)
+{
+    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const double w = Y[s] * m.ri[s];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) a[q] = fma(w, low ? m.clo[q][s] : m.chi[q][s], a[q]);
+    }
+    c.a0 = a[0];
+    c.a1 = a[1];
+    c.a2 = a[2];
+    c.a3 = a[3];
+    c.a4 = a[4];
+    c.a5 = a[5];
+    c.a6 = a[6];
+    c.a7 = a[7];
+    c.h3 = a[3] * 0.5;
+    c.h4 = a[4] * (1.0 / 3.0);
+    c.h5 = a[5] * 0.25;
+    c.h6 = a[6] * 0.2;
+}
+
+template <int NS>
+__device__ __forceinline__ double newton_temperature(const DevMech &m, double T, double E, const double (&Y)[NS])
+{
+    double rsum = 0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) rsum += Y[s] * m.ri[s];
+    const double e_scaled = E * 1e-3;
+    bool low = T < kThermoSwitch;
+    MixPoly<NS> c;
+    mix_poly<NS>(m, Y, low, c);
+    double T_temp = T;
+    for (int count = 0; count < 10; ++count) {
+        const double T0 = T_temp;
+        const bool l = T0 < kThermoSwitch;
+        if (l != low) {
+            low = l;
+            mix_poly<NS>(m, Y, low, c);
+        }
+        const double inv = rcp_nr(T0);
+        const double h = fma(T0, fma(T0, fma(T0, fma(T0, fma(T0, c.h6, c.h5), c.h4), c.h3), c.a2), c.a7) -
+                         c.a0 * inv + c.a1 * log(T0);
+        const double cp = fma(T0, fma(T0, fma(T0, fma(T0, c.a6, c.a5), c.a4), c.a3), c.a2) +
+                          inv * fma(c.a0, inv, c.a1);
+        const double temp1 = (h - e_scaled) - rsum * T0;
+        const double temp2 = cp - rsum;
+        T_temp = T0 - div_fast(temp1, temp2);
+        if (fabs(T_temp - T0) < 1e-6)
+            break;
+    }
+    return T_temp;
+}
+#endif
 
 // Per-cell flow state kept in registers by the recovery / kinetics kernel.
 template <int NS>
@@ -159,10 +248,18 @@ __device__ __forceinline__ void finish_primitives(const DevMech &m, const CellSt
     const double Rgas = kRUniv * 1000 / Wav;
     P = c.T * c.D * Rgas;
     H = P / c.D + c.E;
+#ifdef EU_STRICT
     const TPow p = make_tpow(c.T, false);
     double cp = 0;
 #pragma unroll
     for (int s = 0; s < NS; ++s) cp += cp_species<NS>(m, p, m.ri[s], s) * c.Y[s];
+#else
+    MixPoly<NS> mp;
+    mix_poly<NS>(m, c.Y, c.T < kThermoSwitch, mp);
+    const double T0 = c.T, inv = rcp_nr(T0);
+    const double cp = fma(T0, fma(T0, fma(T0, fma(T0, mp.a6, mp.a5), mp.a4), mp.a3), mp.a2) +
+                      inv * fma(mp.a0, inv, mp.a1);
+#endif
     const double Cp = cp * 1000;
     G = Cp / (Cp - kRUniv * inv_w * 1000);
 }
@@ -188,18 +285,21 @@ __device__ __forceinline__ double pow_int_or_real(double x, double e)
     return pow(x, e);
 }
 
-// Net rates of one cell at temperature T and concentrations mc (scaled 1e-6):
-// src/Reaction.cpp:597-623 (also :873-903 in TrapezoidPrediction). Outputs per
-// reaction the forward and backward products kf*[X]^nu_f, kb*[X]^nu_b, the
-// third-body factor and the species mass rates Wi (:720-727).
-template <int NS, int NR>
-struct Rates {
-    double fwd[NR], bwd[NR], rtb[NR];
-    double wi[NS];
+// Per-species production/loss sums of one cell, accumulated reaction by
+// reaction (src/Reaction.cpp:597-623 rates, :720-727 mass rates Wi, :786-797
+// trapezoid P and Q). Summation order over reactions is the reference's for
+// every species; terms whose stoichiometric coefficients vanish are exact zeros
+// in the reference and are skipped here. P and Q do not depend on the substep
+// length, so the prediction's evaluation serves the first substep too.
+template <int NS>
+struct SpeciesRates {
+    double P[NS], Q[NS], W[NS]; // W = Wi (mass rate, g/cm^3/s)
 };
 
+#ifdef EU_STRICT
+// Strict form: the reference's expressions (pow, exp of each Kp, divisions).
 template <int NS, int NR>
-__device__ __forceinline__ void eval_rates(const DevMech &m, double T, const double (&mc)[NS], Rates<NS, NR> &k)
+__device__ __forceinline__ void eval_rates(const DevMech &m, double T, const double (&mc)[NS], SpeciesRates<NS> &k)
 {
     double Gi[NS];
     {
@@ -216,7 +316,11 @@ __device__ __forceinline__ void eval_rates(const DevMech &m, double T, const dou
     const double RuT = kRuCal * T;
     const double p0 = kP0 * 1e-6;
 #pragma unroll
-    for (int s = 0; s < NS; ++s) k.wi[s] = 0.0;
+    for (int s = 0; s < NS; ++s) {
+        k.P[s] = 0.0;
+        k.Q[s] = 0.0;
+        k.W[s] = 0.0;
+    }
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
         double delta_g = 0.0, rrf = 1.0, rrb = 1.0, rtb = 0.0;
@@ -237,54 +341,103 @@ __device__ __forceinline__ void eval_rates(const DevMech &m, double T, const dou
         if (rtb == 0.0)
             rtb = 1.0;
         const double fwd = kf * rrf, bwd = kb * rrb;
-        k.fwd[r] = fwd;
-        k.bwd[r] = bwd;
-        k.rtb[r] = rtb;
         const double rr = fwd - bwd;
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            const double d = m.sb[r][s] - m.sf[r][s];
-            if (d != 0.0)
-                k.wi[s] += d * rtb * rr;
-        }
-    }
-#pragma unroll
-    for (int s = 0; s < NS; ++s) k.wi[s] = m.mw[s] * k.wi[s];
-}
-
-// One linearised trapezoid substep (src/Reaction.cpp:786-805) followed by
-// Flowfield::Explicit(step,i,j,k) (src/Flowfield.cpp:1521-1536) and the state
-// recovery. mc/di hold the scaled concentrations/densities the rates used.
-template <int NS, int NR>
-__device__ __forceinline__ void trapezoid_substep(const DevMech &m, const Rates<NS, NR> &k, double dts,
-                                                  const double (&mc)[NS], const double (&di)[NS],
-                                                  CellState<NS> &c)
-{
-    double P[NS], Q[NS];
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-        P[s] = 0.0;
-        Q[s] = 0.0;
-    }
-#pragma unroll
-    for (int r = 0; r < NR; ++r) {
-        const double fwd = k.fwd[r], bwd = k.bwd[r], rtb = k.rtb[r];
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
             const double b = m.sb[r][s], f = m.sf[r][s];
             if (b != 0.0 || f != 0.0) {
-                Q[s] += (b * fwd + f * bwd) * rtb;
-                P[s] += (b * bwd + f * fwd) * rtb;
+                k.W[s] += (b - f) * rtb * rr;
+                k.Q[s] += (b * fwd + f * bwd) * rtb;
+                k.P[s] += (b * bwd + f * fwd) * rtb;
             }
         }
     }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) k.W[s] = m.mw[s] * k.W[s];
+}
+#else
+// Fast form, algebraically the reference's:
+//   Kc_r = exp(-sum_s nu_rs g_s) (p0/RT)^Xr with g_s = G_s/(R T) per species, so
+//   kb_r = kf_r * prod_s exp(g_s)^nu_rs * (RT/p0)^Xr  (one exp per species);
+//   kf_r = A_r exp(b_r ln T - E_r/(Ru T))            (one exp per reaction).
+template <int NS, int NR>
+__device__ __forceinline__ void eval_rates(const DevMech &m, double T, const double (&mc)[NS], SpeciesRates<NS> &k)
+{
+    double eg[NS], ieg[NS];
+    const TPow p = make_tpow(T, true);
+    const double invRT = 1.0 / (kRUniv * T);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const double g = (h_species<NS>(m, p, kRUniv, s) - s_species<NS>(m, p, kRUniv, s) * T) * invRT;
+        eg[s] = exp(g);
+        ieg[s] = rcp_nr(eg[s]);
+    }
+    const double invRuT = 1.0 / (kRuCal * T);
+    const double rt_p0 = (kRUniv * T) / (kP0 * 1e-6);
+    const double p0_rt = rcp_nr(rt_p0);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        k.P[s] = 0.0;
+        k.Q[s] = 0.0;
+        k.W[s] = 0.0;
+    }
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        double rrf = 1.0, rrb = 1.0, rtb = 0.0, kc_inv = 1.0;
+        const double b = m.bf[r];
+        double kf;
+        if (m.eaf[r] == 0.0 && (b == 0.0 || b == 1.0 || b == -1.0 || b == -2.0))
+            kf = m.af[r] * (b == 0.0 ? 1.0 : b == 1.0 ? T : b == -1.0 ? p.inv : p.inv2);
+        else
+            kf = m.af[r] * exp(b * p.lnT - m.eaf[r] * invRuT);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const double f = m.sf[r][s], bb = m.sb[r][s];
+            rrf *= (f == 0.0 ? 1.0 : (f == 1.0 ? mc[s] : mc[s] * mc[s]));
+            rrb *= (bb == 0.0 ? 1.0 : (bb == 1.0 ? mc[s] : mc[s] * mc[s]));
+            const double d = bb - f;
+            kc_inv *= (d == 0.0 ? 1.0 : d == 1.0 ? eg[s] : d == -1.0 ? ieg[s] : d == 2.0 ? eg[s] * eg[s]
+                                                                                  : ieg[s] * ieg[s]);
+            rtb += mc[s] * m.tb[r][s];
+        }
+        const double Xr = m.xr[r];
+        kc_inv *= (Xr == 0.0 ? 1.0 : Xr == 1.0 ? rt_p0 : p0_rt);
+        const double kb = kf * kc_inv;
+        if (rtb == 0.0)
+            rtb = 1.0;
+        const double fwd = kf * rrf, bwd = kb * rrb;
+        const double rr = fwd - bwd;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const double bb = m.sb[r][s], f = m.sf[r][s];
+            if (bb != 0.0 || f != 0.0) {
+                k.W[s] += (bb - f) * rtb * rr;
+                k.Q[s] += (bb * fwd + f * bwd) * rtb;
+                k.P[s] += (bb * bwd + f * fwd) * rtb;
+            }
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) k.W[s] = m.mw[s] * k.W[s];
+}
+#endif
+
+// One linearised trapezoid substep (src/Reaction.cpp:786-805) followed by
+// Flowfield::Explicit(step,i,j,k) (src/Flowfield.cpp:1521-1536) and the state
+// recovery. mc holds the scaled concentrations the rates used; the scaled
+// densities are cs * 1e-3.
+template <int NS>
+__device__ __forceinline__ void trapezoid_substep(const DevMech &m, const SpeciesRates<NS> &k, double dts,
+                                                  const double (&mc)[NS], CellState<NS> &c)
+{
     const double half = dts / 2.0;
     double D = 0.0;
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-        const double q = m.mw[s] * Q[s];
-        const double p = (mc[s] == 0) ? 0.0 : P[s] / mc[s];
-        const double nd = ((1.0 - half * p) * di[s] + dts * q) / (1.0 + half * p) * 1e3;
+        const double di = c.cs[s] * 1e-3;
+        const double q = m.mw[s] * k.Q[s];
+        const double p = (mc[s] == 0) ? 0.0 : k.P[s] / mc[s];
+        const double nd = ((1.0 - half * p) * di + dts * q) / (1.0 + half * p) * 1e3;
         c.cs[s] = nd;
         D += nd;
     }
@@ -295,15 +448,13 @@ __device__ __forceinline__ void trapezoid_substep(const DevMech &m, const Rates<
     recover_state<NS>(m, c);
 }
 
+// Concentrations scaled to mol/cm^3 as the kinetics reads them: Mc = Di/Mw*1000
+// (src/Flowfield.cpp:1589) times 1e-6 (src/Reaction.cpp:580).
 template <int NS>
-__device__ __forceinline__ void scaled_species(const DevMech &m, const CellState<NS> &c, double (&mc)[NS],
-                                               double (&di)[NS])
+__device__ __forceinline__ void scaled_concentrations(const DevMech &m, const CellState<NS> &c, double (&mc)[NS])
 {
 #pragma unroll
-    for (int s = 0; s < NS; ++s) {
-        di[s] = c.cs[s] * 1e-3;
-        mc[s] = (c.cs[s] / m.mw[s] * 1000) * 1e-6;
-    }
+    for (int s = 0; s < NS; ++s) mc[s] = (c.cs[s] / m.mw[s] * 1000) * 1e-6;
 }
 
 // ----------------------------------------------------------------- fluxes
@@ -317,33 +468,59 @@ __device__ __forceinline__ R minmod(R r)
 
 // MUSCL_2, kappa = 1/3, minmod (include/Differ.hpp:149-238) for the face
 // between m and m+1: fm1, f0, f1, f2 are values at m-1, m, m+1, m+2.
-template <typename R>
+//
+// Strict form: the reference's expression, with its divisions
+//   L = A1/(A0+1e-12), R = A1/(A2+1e-12), limiter values minmod(L), minmod(1/L).
+// Fast form: the same limiter written without the reciprocal ratios. For
+// L > 0 the reference's slope term 0.25((1-k) min(L,1) + (1+k) min(1/L,1) L) A0
+// equals 0.5 min(L,1) A0 (k = 1/3); for L <= 0 it is 0. L is formed with a
+// Newton-refined reciprocal. Results agree to a few units in the last place.
+template <typename R, bool kStrict>
 __device__ __forceinline__ void muscl(R fm1, R f0, R f1, R f2, R &left, R &right)
 {
-    const R kk = R(1.0) / R(3.0);
     const R A0 = f0 - fm1;
     const R A1 = f1 - f0;
     const R A2 = f2 - f1;
-    const R L = A1 / (A0 + R(1e-12));
-    const R Rr = A1 / (A2 + R(1e-12));
-    const R L1 = minmod(L), L2 = minmod(R(1.0) / L), R1 = minmod(Rr), R2 = minmod(R(1.0) / Rr);
-    left = f0 + R(0.25) * ((R(1.0) - kk) * L1 + (R(1) + kk) * L2 * L) * A0;
-    right = f1 - R(0.25) * ((R(1.0) - kk) * R1 + (R(1) + kk) * R2 * Rr) * A2;
+    if (kStrict) {
+        const R kk = R(1.0) / R(3.0);
+        const R L = A1 / (A0 + R(1e-12));
+        const R Rr = A1 / (A2 + R(1e-12));
+        const R L1 = minmod(L), L2 = minmod(R(1.0) / L), R1 = minmod(Rr), R2 = minmod(R(1.0) / Rr);
+        left = f0 + R(0.25) * ((R(1.0) - kk) * L1 + (R(1) + kk) * L2 * L) * A0;
+        right = f1 - R(0.25) * ((R(1.0) - kk) * R1 + (R(1) + kk) * R2 * Rr) * A2;
+    } else {
+        const R L = div_fast(A1, A0 + R(1e-12));
+        const R Rr = div_fast(A1, A2 + R(1e-12));
+        left = f0 + (L > R(0) ? R(0.5) * A0 * fmin(L, R(1)) : R(0));
+        right = f1 - (Rr > R(0) ? R(0.5) * A2 * fmin(Rr, R(1)) : R(0));
+    }
 }
 
 // AUSM+ flux of one face (src/Flowfield.cpp:1811-1930) for direction DIR
 // (0: x, 1: y, 2: z). lr holds the reconstructed left/right primitives
 // {P, D, U, V, W, H, Gamma} and species. Output F[NS+4] in FP64.
-template <int NS, int DIR, typename R>
+template <int NS, int DIR, typename R, bool kStrict, typename FOut>
 __device__ __forceinline__ void ausm(const R (&L)[7], const R (&Rt)[7], const R (&YL)[NS], const R (&YR)[NS],
-                                     double (&F)[NS + 4])
+                                     FOut (&F)[NS + 4])
 {
     const R PL = L[kP], PR = Rt[kP], DL = L[kD], DR = Rt[kD];
-    const R CL = sqrt(L[kG] * PL / DL);
-    const R CR = sqrt(Rt[kG] * PR / DR);
-    const R CI = R(0.5) * (CL + CR);
-    const R MaL = L[kU + DIR] / CI;
-    const R MaR = Rt[kU + DIR] / CI;
+    R CL, CR, CI, MaL, MaR;
+    if (kStrict) {
+        CL = sqrt(L[kG] * PL / DL);
+        CR = sqrt(Rt[kG] * PR / DR);
+        CI = R(0.5) * (CL + CR);
+        MaL = L[kU + DIR] / CI;
+        MaR = Rt[kU + DIR] / CI;
+    } else {
+        // c = sqrt(g p / rho) = (g p) / sqrt(g p rho)
+        const R gpL = L[kG] * PL, gpR = Rt[kG] * PR;
+        CL = gpL * rsqrt(gpL * DL);
+        CR = gpR * rsqrt(gpR * DR);
+        CI = R(0.5) * (CL + CR);
+        const R inv = div_fast(R(1), CI);
+        MaL = L[kU + DIR] * inv;
+        MaR = Rt[kU + DIR] * inv;
+    }
     R B1, G1, B2, G2;
     if (fabs(MaL) < R(1.0)) {
         const R a = MaL + R(1.0), t = MaL * MaL - R(1.0);
@@ -368,13 +545,13 @@ __device__ __forceinline__ void ausm(const R (&L)[7], const R (&Rt)[7], const R 
             Hu = up ? L[kH] : Rt[kH];
     const R m = VI * Du;
 #pragma unroll
-    for (int s = 0; s < NS; ++s) F[s] = double(m * (up ? YL[s] : YR[s]));
+    for (int s = 0; s < NS; ++s) F[s] = FOut(m * (up ? YL[s] : YR[s]));
     R mom[3] = {m * Uu, m * Vu, m * Wu};
     mom[DIR] = mom[DIR] + G1 * PL + G2 * PR;
-    F[NS + 0] = double(mom[0]);
-    F[NS + 1] = double(mom[1]);
-    F[NS + 2] = double(mom[2]);
-    F[NS + 3] = double(VI * (Du * Hu + R(0.5) * Du * (Uu * Uu + Vu * Vu + Wu * Wu)));
+    F[NS + 0] = FOut(mom[0]);
+    F[NS + 1] = FOut(mom[1]);
+    F[NS + 2] = FOut(mom[2]);
+    F[NS + 3] = FOut(VI * (Du * Hu + R(0.5) * Du * (Uu * Uu + Vu * Vu + Wu * Wu)));
 }
 
 } // namespace eu3d

@@ -109,69 +109,112 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
 
 // Face flux between cell c and c + stride along DIR, from the primitive planes
 // (FP64 or FP32 copies): MUSCL_2 on every primitive, then AUSM+.
-template <int NS, int DIR, typename R>
+template <int NS, int DIR, typename R, bool kStrict>
 __device__ __forceinline__ void face_flux(const R *__restrict__ prim, long long n3, long long c, long long stride,
-                                          double (&F)[NS + 4])
+                                          R (&F)[NS + 4])
 {
     R L[7], Rt[7], YL[NS], YR[NS];
 #pragma unroll
     for (int f = 0; f < 7; ++f) {
         const R *a = prim + f * n3 + c;
-        muscl<R>(a[-stride], a[0], a[stride], a[2 * stride], L[f], Rt[f]);
+        muscl<R, kStrict>(__ldg(a - stride), __ldg(a), __ldg(a + stride), __ldg(a + 2 * stride), L[f], Rt[f]);
     }
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
         const R *a = prim + (kY0 + s) * n3 + c;
-        muscl<R>(a[-stride], a[0], a[stride], a[2 * stride], YL[s], YR[s]);
+        muscl<R, kStrict>(__ldg(a - stride), __ldg(a), __ldg(a + stride), __ldg(a + 2 * stride), YL[s], YR[s]);
     }
-    ausm<NS, DIR, R>(L, Rt, YL, YR, F);
+    ausm<NS, DIR, R, kStrict, R>(L, Rt, YL, YR, F);
 }
 
-// Flux divergence and the Euler-explicit update of one interior node:
-// TimeAdv::EE (src/TimeAdv.cpp:42-56) + CS += RHS (src/Flowfield.cpp:1350-1354).
-// One thread per interior node; each thread forms the six face fluxes of its
-// node. dt is read from device memory so a captured graph can follow a
-// device-computed step.
+// Flux divergence and the Euler-explicit update (TimeAdv::EE, src/TimeAdv.cpp:42-56,
+// then CS += RHS, src/Flowfield.cpp:1350-1354) with every face flux formed once.
+//
+// A block owns a kFluxTJ x kFluxTK tile of (j, k) columns and marches along x
+// over kFluxCI nodes. The x-face flux at i-1/2 stays in registers from the
+// previous node; the y- and z-face fluxes of the current plane go through
+// shared memory (row 0 / column 0 hold the faces below the tile, computed by
+// warp 0 and by eight lanes of warp 1). RHS keeps the reference's order
+// -dt/dx (F+ - F-) - dt/dy (G+ - G-) - dt/dz (Q+ - Q-), accumulated in FP64.
+constexpr int kFluxTK = 32, kFluxTJ = 8, kFluxCI = 16;
+
 template <int NS, typename R>
-__global__ void __launch_bounds__(128) k_flux_update(const DevGrid g, const DevState st, const R *__restrict__ prim,
-                                                     const double *__restrict__ dt_dev)
+constexpr size_t flux_smem_bytes()
 {
-    const int k = g.bc + blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = g.bc + blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = g.bc + blockIdx.z * blockDim.z + threadIdx.z;
-    if (k >= g.nk + g.bc || j >= g.nj + g.bc || i >= g.ni + g.bc)
-        return;
-    const long long n3 = g.n3;
-    const long long c = cell_index(g, i, j, k);
-    const long long sx = (long long)g.ny * g.nz, sy = g.nz;
+    return sizeof(R) * (NS + 4) * ((kFluxTJ + 1) * kFluxTK + kFluxTJ * (kFluxTK + 1));
+}
+
+template <int NS, typename R, bool kStrict>
+__global__ void __launch_bounds__(kFluxTK *kFluxTJ, 1)
+    k_flux_update(const DevGrid g, const DevState st, const R *__restrict__ prim, const double *__restrict__ dt_dev)
+{
+    constexpr int NV = NS + 4;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R(*sG)[kFluxTJ + 1][kFluxTK] = reinterpret_cast<R(*)[kFluxTJ + 1][kFluxTK]>(smem_raw);
+    R(*sQ)[kFluxTJ][kFluxTK + 1] =
+        reinterpret_cast<R(*)[kFluxTJ][kFluxTK + 1]>(smem_raw + sizeof(R) * NV * (kFluxTJ + 1) * kFluxTK);
+
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int k0 = blockIdx.x * kFluxTK, j0 = blockIdx.y * kFluxTJ;
+    const int k = g.bc + k0 + tx, j = g.bc + j0 + ty;
+    const bool valid = (k0 + tx < g.nk) && (j0 + ty < g.nj);
+    const int i_begin = g.bc + blockIdx.z * kFluxCI;
+    const int i_end = min(i_begin + kFluxCI, g.bc + g.ni);
+    const long long n3 = g.n3, sx = (long long)g.ny * g.nz, sy = g.nz;
     const double dt = *dt_dev;
-    const double cx = -dt / (g.x[i] - g.x[i - 1]);
-    const double cy = dt / (g.y[j] - g.y[j - 1]);
-    const double cz = dt / (g.z[k] - g.z[k - 1]);
-    double rhs[NS + 4];
-    {
-        double Fp[NS + 4], Fm[NS + 4];
-        face_flux<NS, 0, R>(prim, n3, c, sx, Fp);
-        face_flux<NS, 0, R>(prim, n3, c - sx, sx, Fm);
+    const double cy = valid ? dt / (g.y[j] - g.y[j - 1]) : 0.0;
+    const double cz = valid ? dt / (g.z[k] - g.z[k - 1]) : 0.0;
+    // lanes of warp 1 that form the z faces below the tile, one per row
+    const int zrow = tx;
+    const bool zlow = (ty == 1) && (tx < kFluxTJ) && (j0 + zrow < g.nj) && (k0 < g.nk);
+
+    R Fm[NV];
+    if (valid)
+        face_flux<NS, 0, R, kStrict>(prim, n3, cell_index(g, i_begin - 1, j, k), sx, Fm);
+    for (int i = i_begin; i < i_end; ++i) {
+        const long long c = cell_index(g, i, j, k);
+        R Fp[NV];
+        if (valid) {
+            face_flux<NS, 0, R, kStrict>(prim, n3, c, sx, Fp);
+            {
+                R G[NV];
+                face_flux<NS, 1, R, kStrict>(prim, n3, c, sy, G);
 #pragma unroll
-        for (int q = 0; q < NS + 4; ++q) rhs[q] = cx * (Fp[q] - Fm[q]);
+                for (int q = 0; q < NV; ++q) sG[q][ty + 1][tx] = G[q];
+            }
+            {
+                R Q[NV];
+                face_flux<NS, 2, R, kStrict>(prim, n3, c, 1, Q);
+#pragma unroll
+                for (int q = 0; q < NV; ++q) sQ[q][ty][tx + 1] = Q[q];
+            }
+            if (ty == 0) {
+                R G[NV];
+                face_flux<NS, 1, R, kStrict>(prim, n3, c - sy, sy, G);
+#pragma unroll
+                for (int q = 0; q < NV; ++q) sG[q][0][tx] = G[q];
+            }
+        }
+        if (zlow) {
+            R Q[NV];
+            face_flux<NS, 2, R, kStrict>(prim, n3, cell_index(g, i, g.bc + j0 + zrow, g.bc + k0 - 1), 1, Q);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) sQ[q][zrow][0] = Q[q];
+        }
+        __syncthreads();
+        if (valid) {
+            const double cx = -dt / (g.x[i] - g.x[i - 1]);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
+                const double rhs = cx * (double(Fp[q]) - double(Fm[q])) -
+                                   cy * (double(sG[q][ty + 1][tx]) - double(sG[q][ty][tx])) -
+                                   cz * (double(sQ[q][ty][tx + 1]) - double(sQ[q][ty][tx]));
+                st.cs[q * n3 + c] = st.cs[q * n3 + c] + rhs;
+                Fm[q] = Fp[q];
+            }
+        }
+        __syncthreads();
     }
-    {
-        double Fp[NS + 4], Fm[NS + 4];
-        face_flux<NS, 1, R>(prim, n3, c, sy, Fp);
-        face_flux<NS, 1, R>(prim, n3, c - sy, sy, Fm);
-#pragma unroll
-        for (int q = 0; q < NS + 4; ++q) rhs[q] = rhs[q] - cy * (Fp[q] - Fm[q]);
-    }
-    {
-        double Fp[NS + 4], Fm[NS + 4];
-        face_flux<NS, 2, R>(prim, n3, c, 1, Fp);
-        face_flux<NS, 2, R>(prim, n3, c - 1, 1, Fm);
-#pragma unroll
-        for (int q = 0; q < NS + 4; ++q) rhs[q] = rhs[q] - cz * (Fp[q] - Fm[q]);
-    }
-#pragma unroll
-    for (int q = 0; q < NS + 4; ++q) st.cs[q * n3 + c] = st.cs[q * n3 + c] + rhs[q];
 }
 
 // ------------------------------------------------- recovery + kinetics
@@ -231,15 +274,15 @@ __global__ void __launch_bounds__(128) k_recover_react(const __grid_constant__ D
 
     if (kReact) {
         const double dtm = *dt_dev;
-        double mc[NS], di[NS];
-        scaled_species<NS>(m, cell, mc, di);
-        Rates<NS, NR> rates;
+        double mc[NS];
+        scaled_concentrations<NS>(m, cell, mc);
+        SpeciesRates<NS> rates;
         eval_rates<NS, NR>(m, cell.T, mc, rates);
         double dt = dtm;
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
-            if (cell.Y[s] >= 1e-6 && rates.wi[s] != 0) {
-                const double dt_temp = fabs(-di[s] / rates.wi[s]);
+            if (cell.Y[s] >= 1e-6 && rates.W[s] != 0) {
+                const double dt_temp = fabs(-(cell.cs[s] * 1e-3) / rates.W[s]);
                 if (dt_temp < dt)
                     dt = dt_temp;
             }
@@ -260,14 +303,14 @@ __global__ void __launch_bounds__(128) k_recover_react(const __grid_constant__ D
         const double dts = dtm / nchem;
         for (int step = 0; step < nchem; ++step) {
             if (step > 0) {
-                scaled_species<NS>(m, cell, mc, di);
+                scaled_concentrations<NS>(m, cell, mc);
                 eval_rates<NS, NR>(m, cell.T, mc, rates);
             }
             if (st.cms) {
 #pragma unroll
-                for (int s = 0; s < NS; ++s) st.cms[s * n3 + c] = rates.wi[s] * 1e3;
+                for (int s = 0; s < NS; ++s) st.cms[s * n3 + c] = rates.W[s] * 1e3;
             }
-            trapezoid_substep<NS, NR>(m, rates, dts, mc, di, cell);
+            trapezoid_substep<NS>(m, rates, dts, mc, cell);
         }
     }
     store_cell<NS>(m, st, n3, c, cell);

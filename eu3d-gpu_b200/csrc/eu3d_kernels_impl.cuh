@@ -22,19 +22,39 @@ cudaError_t boundary_t(const LaunchArgs &a)
     return cudaGetLastError();
 }
 
+#ifdef EU_STRICT
+constexpr bool kStrictFlux = true;
+#else
+constexpr bool kStrictFlux = false;
+#endif
+
+template <int NS, typename R, bool kStrict>
+cudaError_t flux_launch(const LaunchArgs &a, const R *prim)
+{
+    const DevGrid &g = a.g;
+    const size_t smem = flux_smem_bytes<NS, R>();
+    static bool configured = false; // per instantiation, once per process
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_flux_update<NS, R, kStrict>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess)
+            return e;
+        configured = true;
+    }
+    const dim3 block(kFluxTK, kFluxTJ);
+    const dim3 grid((g.nk + kFluxTK - 1) / kFluxTK, (g.nj + kFluxTJ - 1) / kFluxTJ,
+                    (g.ni + kFluxCI - 1) / kFluxCI);
+    k_flux_update<NS, R, kStrict><<<grid, block, smem, a.stream>>>(g, a.st, prim, a.dt_dev);
+    return cudaGetLastError();
+}
+
 template <int NS, int NR>
 cudaError_t flux_t(const LaunchArgs &a)
 {
-    const DevGrid &g = a.g;
-    const dim3 block(32, 2, 2);
-    const dim3 grid((g.nk + block.x - 1) / block.x, (g.nj + block.y - 1) / block.y,
-                    (g.ni + block.z - 1) / block.z);
-    if (a.precision == 1) {
-        k_flux_update<NS, float><<<grid, block, 0, a.stream>>>(g, a.st, a.st.prim32, a.dt_dev);
-    } else {
-        k_flux_update<NS, double><<<grid, block, 0, a.stream>>>(g, a.st, a.st.prim, a.dt_dev);
-    }
-    return cudaGetLastError();
+    // mixed precision: FP32 reconstruction and AUSM (always the division-light forms)
+    if (a.precision == 1)
+        return flux_launch<NS, float, false>(a, a.st.prim32);
+    return flux_launch<NS, double, kStrictFlux>(a, a.st.prim);
 }
 
 template <int NS, int NR>

@@ -135,6 +135,8 @@ eu_status install_mechanism(eu_handle *h, const MechanismTables &m)
         d.xr[r] = xr;
         d.has_tb[r] = tb;
     }
+    if (!nu_int)
+        return fail(h, EU_ERR_UNSUPPORTED, "stoichiometric coefficients other than 0, 1, 2 are not supported");
     d.nu_int = nu_int;
     const bool first = !h->has_mech;
     h->mech = m;
