@@ -4,6 +4,7 @@
 #pragma once
 
 #include "eu3d_device.cuh"
+#include "eu3d_mech_JA919.cuh"
 
 #ifndef EU3D_NS
 #error "define EU3D_NS (the arithmetic flavour's namespace) before including eu3d_kernels.cuh"
@@ -251,7 +252,17 @@ __device__ __forceinline__ void store_cell(const DevMech &m, const DevState &st,
 // src/Reaction.cpp:562-805, src/Flowfield.cpp:1521-1536). The prediction's
 // rate evaluation is reused by the first substep: both evaluate the same
 // expression on the same state. One thread per interior node.
-template <int NS, int NR, bool kReact>
+// Rate evaluation from the runtime tables (any mechanism of these sizes).
+template <int NS_, int NR_>
+struct TableRates {
+    static constexpr int NS = NS_, NR = NR_;
+    __device__ __forceinline__ static void rates(const DevMech &m, double T, const double (&mc)[NS], SpeciesRates<NS> &k)
+    {
+        eval_rates<NS, NR>(m, T, mc, k);
+    }
+};
+
+template <int NS, int NR, bool kReact, class Rt>
 __global__ void __launch_bounds__(128) k_recover_react(const __grid_constant__ DevMech m, const DevGrid g,
                                                        const DevState st, const double *__restrict__ dt_dev,
                                                        int max_substeps)
@@ -277,7 +288,7 @@ __global__ void __launch_bounds__(128) k_recover_react(const __grid_constant__ D
         double mc[NS];
         scaled_concentrations<NS>(m, cell, mc);
         SpeciesRates<NS> rates;
-        eval_rates<NS, NR>(m, cell.T, mc, rates);
+        Rt::rates(m, cell.T, mc, rates);
         double dt = dtm;
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
@@ -304,7 +315,7 @@ __global__ void __launch_bounds__(128) k_recover_react(const __grid_constant__ D
         for (int step = 0; step < nchem; ++step) {
             if (step > 0) {
                 scaled_concentrations<NS>(m, cell, mc);
-                eval_rates<NS, NR>(m, cell.T, mc, rates);
+                Rt::rates(m, cell.T, mc, rates);
             }
             if (st.cms) {
 #pragma unroll

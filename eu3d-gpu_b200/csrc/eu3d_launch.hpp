@@ -17,6 +17,7 @@ struct LaunchArgs {
     int max_substeps;
     int precision; // eu_precision
     int chemistry; // eu_chemistry
+    int spec;      // 1: tables are bitwise H2_JA919, use the generated rate code
     cudaStream_t stream;
 };
 

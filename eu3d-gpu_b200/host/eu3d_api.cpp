@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include "../csrc/eu3d_launch.hpp"
+#include "eu3d_mech_JA919_tables.h"
 #include "readers.hpp"
 #include "state_init.hpp"
 
@@ -24,6 +25,7 @@ struct eu_handle {
     std::vector<double> x, y, z;
     MechanismTables mech;
     DevMech dmech{};
+    int spec = 0; // 1 when the tables are the generated H2_JA919 ones
     bool has_mech = false, has_state = false;
     DevGrid g{};
     DevState st{};
@@ -139,6 +141,10 @@ eu_status install_mechanism(eu_handle *h, const MechanismTables &m)
         return fail(h, EU_ERR_UNSUPPORTED, "stoichiometric coefficients other than 0, 1, 2 are not supported");
     d.nu_int = nu_int;
     const bool first = !h->has_mech;
+    h->spec = matches_JA919(m.ns, m.nr, m.mw.data(), m.coeff_lo.data(), m.coeff_hi.data(), m.af.data(), m.bf.data(),
+                            m.eaf.data(), m.stoi_f.data(), m.stoi_b.data(), m.tb.data())
+                  ? 1
+                  : 0;
     h->mech = m;
     h->dmech = d;
     h->has_mech = true;
@@ -183,6 +189,7 @@ LaunchArgs launch_args(eu_handle *h)
     a.max_substeps = h->cfg.max_substeps > 0 ? h->cfg.max_substeps : (1 << 20);
     a.precision = h->cfg.precision;
     a.chemistry = h->cfg.chemistry;
+    a.spec = h->spec;
     a.stream = h->stream;
     return a;
 }
