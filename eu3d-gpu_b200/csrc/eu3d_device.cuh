@@ -1,10 +1,11 @@
 // eu3d_device.cuh — device-side types and per-cell / per-face arithmetic of the
 // EU3D reacting-Euler timestep for sm_100a.
 //
-// Included by the kernel translation units. EU_STRICT selects the variants that
-// round exactly as the reference's CPU build (no FMA: those units are compiled
-// with --fmad=false; divisions and operand order as in the reference); without
-// it, FMA contraction and algebraically equivalent fast forms are used.
+// Included by the kernel translation units. EU_EXACT_CHEM selects thermo,
+// temperature-inversion and rate expressions with the reference's operand
+// order and divisions (compiled with --fmad=false they round exactly as the
+// reference's CPU build); without it, algebraically equivalent fast forms are
+// used. The flux reconstruction has its own switch (EU_EXACT_FLUX).
 #pragma once
 
 #include <cstdint>
@@ -88,7 +89,7 @@ __device__ __forceinline__ double h_species(const DevMech &m, const TPow &p, dou
     const double a0 = coeff<NS>(m, p, 0, s), a1 = coeff<NS>(m, p, 1, s), a2 = coeff<NS>(m, p, 2, s),
                  a3 = coeff<NS>(m, p, 3, s), a4 = coeff<NS>(m, p, 4, s), a5 = coeff<NS>(m, p, 5, s),
                  a6 = coeff<NS>(m, p, 6, s), a7 = coeff<NS>(m, p, 7, s);
-#ifdef EU_STRICT
+#ifdef EU_EXACT_CHEM
     return R * (-a0 * p.inv + a1 * p.lnT + a2 * p.T + a3 * p.t2 / 2 + a4 * p.t3 / 3 + a5 * p.t4 / 4 +
                 a6 * p.t5 / 5 + a7);
 #else
@@ -104,7 +105,7 @@ __device__ __forceinline__ double s_species(const DevMech &m, const TPow &p, dou
     const double a0 = coeff<NS>(m, p, 0, s), a1 = coeff<NS>(m, p, 1, s), a2 = coeff<NS>(m, p, 2, s),
                  a3 = coeff<NS>(m, p, 3, s), a4 = coeff<NS>(m, p, 4, s), a5 = coeff<NS>(m, p, 5, s),
                  a6 = coeff<NS>(m, p, 6, s), a8 = coeff<NS>(m, p, 8, s);
-#ifdef EU_STRICT
+#ifdef EU_EXACT_CHEM
     return R * (-a0 * p.inv2 / 2 - a1 * p.inv + a2 * p.lnT + a3 * p.T + a4 * p.t2 / 2 + a5 * p.t3 / 3 +
                 a6 * p.t4 / 4 + a8);
 #else
@@ -118,7 +119,7 @@ __device__ __forceinline__ double s_species(const DevMech &m, const TPow &p, dou
 // Flowfield::Get_temp (src/Flowfield.cpp:2072-2131): Newton on
 // sum_s Y_s h_s(T) - E*1e-3 - (sum_s Y_s R_s) T = 0, at most 10 iterations,
 // stop when |dT| < 1e-6 K. E is the cell's previous internal energy.
-#ifdef EU_STRICT
+#ifdef EU_EXACT_CHEM
 template <int NS>
 __device__ __forceinline__ double newton_temperature(const DevMech &m, double T, double E, const double (&Y)[NS])
 {
@@ -248,7 +249,7 @@ __device__ __forceinline__ void finish_primitives(const DevMech &m, const CellSt
     const double Rgas = kRUniv * 1000 / Wav;
     P = c.T * c.D * Rgas;
     H = P / c.D + c.E;
-#ifdef EU_STRICT
+#ifdef EU_EXACT_CHEM
     const TPow p = make_tpow(c.T, false);
     double cp = 0;
 #pragma unroll
@@ -296,7 +297,7 @@ struct SpeciesRates {
     double P[NS], Q[NS], W[NS]; // W = Wi (mass rate, g/cm^3/s)
 };
 
-#ifdef EU_STRICT
+#ifdef EU_EXACT_CHEM
 // Strict form: the reference's expressions (pow, exp of each Kp, divisions).
 template <int NS, int NR>
 __device__ __forceinline__ void eval_rates(const DevMech &m, double T, const double (&mc)[NS], SpeciesRates<NS> &k)

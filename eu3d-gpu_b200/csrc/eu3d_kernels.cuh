@@ -1,6 +1,6 @@
 // eu3d_kernels.cuh — the timestep kernels, templated on the species and
 // reaction counts. Instantiated twice: eu3d_kernels_strict.cu (--fmad=false,
-// EU_STRICT: rounds as the reference's CPU build) and eu3d_kernels_fast.cu.
+// EU_EXACT_CHEM/EU_EXACT_FLUX) and eu3d_kernels_fast.cu.
 #pragma once
 
 #include "eu3d_device.cuh"

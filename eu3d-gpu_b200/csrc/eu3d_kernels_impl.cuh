@@ -1,5 +1,5 @@
 // eu3d_kernels_impl.cuh — launchers for one arithmetic flavour. Included once
-// by eu3d_kernels_strict.cu (EU_STRICT, --fmad=false) and once by
+// by eu3d_kernels_strict.cu (--fmad=false, exact forms) and once by
 // eu3d_kernels_fast.cu, with EU3D_NS naming the namespace.
 #pragma once
 
@@ -22,11 +22,9 @@ cudaError_t boundary_t(const LaunchArgs &a)
     return cudaGetLastError();
 }
 
-// FP64 reconstruction keeps the reference's divisions in both arithmetic
-// flavours: the limiter ratios feed back into the solution, and with the
-// division-light form the 100-step difference from the reference reached the
-// 1e-9 bound on transverse momentum. The fast flavour only adds FMA contraction.
-constexpr bool kStrictFlux = true;
+// FP64 reconstruction: the reference's divisions (EU_EXACT_FLUX=1) or the
+// division-light limiter form.
+constexpr bool kStrictFlux = EU_EXACT_FLUX != 0;
 
 template <int NS, typename R, bool kStrict>
 cudaError_t flux_launch(const LaunchArgs &a, const R *prim)

@@ -84,6 +84,13 @@ def library():
         lib.eu_get_field.argtypes = [_P, ctypes.c_char_p, _P]
         lib.eu_sync.argtypes = [_P]
         lib.eu_device_info.argtypes = [_P, ctypes.POINTER(_P), ctypes.POINTER(ctypes.c_size_t)]
+        lib.eu_mlp_create.argtypes = [_I, ctypes.POINTER(_P)]
+        lib.eu_mlp_destroy.argtypes = [_P]
+        lib.eu_mlp_last_error.restype = ctypes.c_char_p
+        lib.eu_mlp_last_error.argtypes = [_P]
+        lib.eu_mlp_gemm.argtypes = [_P, _P, _I, _P, _I, _I, _I, _I, _P, _I, _P, _P, _P, _I, _P]
+        for fn in ("eu_mlp_create", "eu_mlp_destroy", "eu_mlp_gemm"):
+            getattr(lib, fn).restype = _I
         for fn in ("eu_read_grid", "eu_parse_mechanism", "eu_initial_state", "eu_create", "eu_destroy",
                    "eu_load_mechanism", "eu_set_mechanism", "eu_get_mechanism", "eu_node_coordinates",
                    "eu_set_primitive", "eu_set_state", "eu_step", "eu_get_field", "eu_sync", "eu_device_info"):
@@ -249,3 +256,42 @@ class Solver:
         nbytes = ctypes.c_size_t()
         self._check(library().eu_device_info(self.h, ctypes.byref(stream), ctypes.byref(nbytes)))
         return stream.value, nbytes.value
+
+
+class Mlp:
+    """eu_mlp: the learned-chemistry model and its tensor-core kernels."""
+
+    def __init__(self, device=0):
+        h = _P()
+        st = library().eu_mlp_create(int(device), ctypes.byref(h))
+        if st:
+            raise EU3DError(st, "eu_mlp_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            library().eu_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, what):
+        if st:
+            raise EU3DError(st, f"{what}: {library().eu_mlp_last_error(self.h).decode()}")
+
+    def gemm(self, A, B, bias=None, act=0, Cf=None, Cb=None, Cpre=None, stream=None):
+        """C = act(A @ B.T + bias) on torch CUDA tensors (A, B bf16, row-major)."""
+        M, K = A.shape
+        N = B.shape[0]
+        ldc = N
+        for c in (Cf, Cb, Cpre):
+            if c is not None:
+                ldc = c.stride(0)
+        ptr = lambda t: None if t is None else t.data_ptr()
+        st = library().eu_mlp_gemm(self.h, A.data_ptr(), A.stride(0), B.data_ptr(), B.stride(0), M, N, K,
+                                   ptr(bias), int(act), ptr(Cf), ptr(Cb), ptr(Cpre), ldc, stream)
+        self._check(st, "gemm")

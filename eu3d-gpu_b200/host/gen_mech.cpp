@@ -269,7 +269,7 @@ int main(int argc, char **argv)
           << "// Rates of mechanism " << name << " (" << m.ns << " species, " << m.nr << " reactions).\n"
           << "struct Mech_" << name << " {\n    static constexpr int NS = " << m.ns << ", NR = " << m.nr << ";\n"
           << "    __device__ __forceinline__ static void rates(const DevMech &m, double T, const double (&mc)[" << m.ns
-          << "], SpeciesRates<" << m.ns << "> &k)\n    {\n#ifdef EU_STRICT\n";
+          << "], SpeciesRates<" << m.ns << "> &k)\n    {\n#ifdef EU_EXACT_CHEM\n";
         emit_strict(o, m);
         o << "#else\n";
         emit_fast(o, m);

@@ -183,6 +183,24 @@ eu_status eu_sync(eu_handle *h);
  * resident and time kernels themselves. */
 eu_status eu_device_info(const eu_handle *h, void **stream, size_t *device_bytes);
 
+/* ---------------------------------------------------------------------------
+ * Learned chemistry (no counterpart in the reference, which has no learned
+ * model): a small MLP evaluated and trained with BF16 tensor-core kernels.
+ * ------------------------------------------------------------------------- */
+typedef struct eu_mlp eu_mlp;
+
+eu_status eu_mlp_create(int device, eu_mlp **out);
+eu_status eu_mlp_destroy(eu_mlp *m);
+const char *eu_mlp_last_error(const eu_mlp *m);
+
+/* Tensor-core building block on device pointers: C = act(A * B^T + bias) with
+ * A (M x K) and B (N x K) row-major bf16, fp32 accumulation; K % 16 == 0,
+ * lda and ldb multiples of 8, 16-byte aligned operands. act: 0 none, 1 SiLU.
+ * Outputs (each optional, ldc): Cf fp32, Cb bf16, Cpre fp32 pre-activation.
+ * Runs on `stream` (a cudaStream_t, NULL: the model's stream) and waits for it. */
+eu_status eu_mlp_gemm(eu_mlp *m, const void *A, int lda, const void *B, int ldb, int M, int N, int K,
+                      const float *bias, int act, float *Cf, void *Cb, float *Cpre, int ldc, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
