@@ -21,9 +21,17 @@ namespace eu3d {
 
 constexpr int kGemmBM = 128, kGemmBK = 64, kGemmThreads = 128;
 
-enum GemmAct { kActNone = 0, kActSilu = 1 };
+// Epilogue modes: 0 none, 1 SiLU, 2 multiply by SiLU'(Z) (backward through an
+// activation whose pre-activation Z is given), 3 accumulate into Cf with
+// atomics (split-K partial sums; no bias).
+enum GemmAct { kActNone = 0, kActSilu = 1, kActSiluGrad = 2, kActAccumulate = 3 };
 
 __device__ __forceinline__ float silu(float x) { return x / (1.0f + __expf(-x)); }
+__device__ __forceinline__ float silu_grad(float z)
+{
+    const float s = 1.0f / (1.0f + __expf(-z));
+    return s * (1.0f + z * (1.0f - s));
+}
 
 template <int BN>
 constexpr size_t gemm_smem_bytes()
@@ -52,7 +60,7 @@ template <int BN>
 __global__ void __launch_bounds__(kGemmThreads, 1)
     k_gemm_bf16(const __nv_bfloat16 *__restrict__ A, int lda, const __nv_bfloat16 *__restrict__ B, int ldb, int M,
                 int N, int K, const float *__restrict__ bias, int act, float *Cf, __nv_bfloat16 *Cb, float *Cpre,
-                int ldc, int *err)
+                int ldc, const float *__restrict__ Z, int k_split, int *err)
 {
     static_assert(BN % 32 == 0 && BN >= 32 && BN <= 256, "BN");
     constexpr int BM = kGemmBM, BK = kGemmBK;
@@ -65,7 +73,12 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-    const int KT = (K + BK - 1) / BK;
+    // split-K: CTA z handles K slabs [kt0, kt1)
+    const int KT_all = (K + BK - 1) / BK;
+    const int per = (KT_all + k_split - 1) / k_split;
+    const int kt0 = blockIdx.z * per;
+    const int KT = max(0, min(KT_all, kt0 + per) - kt0);
+    const int kbase = kt0 * BK;
 
     if (warp == 0) {
         tc::tmem_alloc(tslot, BN);
@@ -82,8 +95,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     const uint32_t tmem = *tslot;
     bool ok = true;
 
-    stage_slab<BM>(sa[0], A, lda, m0, M, 0, K);
-    stage_slab<BN>(sb[0], B, ldb, n0, N, 0, K);
+    if (KT > 0) {
+        stage_slab<BM>(sa[0], A, lda, m0, M, kbase, K);
+        stage_slab<BN>(sb[0], B, ldb, n0, N, kbase, K);
+    }
     tc::cp_async_commit();
 
     constexpr uint32_t idesc = tc::idesc_bf16_f32(BM, BN);
@@ -102,8 +117,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                     break;
                 }
             }
-            stage_slab<BM>(sa[s1], A, lda, m0, M, (kt + 1) * BK, K);
-            stage_slab<BN>(sb[s1], B, ldb, n0, N, (kt + 1) * BK, K);
+            stage_slab<BM>(sa[s1], A, lda, m0, M, kbase + (kt + 1) * BK, K);
+            stage_slab<BN>(sb[s1], B, ldb, n0, N, kbase + (kt + 1) * BK, K);
             tc::cp_async_commit();
             tc::cp_async_wait<1>();
         } else {
@@ -132,7 +147,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     }
     tc::tc_fence_after();
 
-    if (ok) {
+    if (ok && KT > 0) {
         const int row = m0 + warp * 32 + lane;
 #pragma unroll 1
         for (int c0 = 0; c0 < BN; c0 += 32) {
@@ -143,15 +158,22 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                 for (int q = 0; q < 32; ++q) {
                     const int n = n0 + c0 + q;
                     if (n < N) {
+                        const size_t o = (size_t)row * ldc + n;
+                        if (act == kActAccumulate) {
+                            atomicAdd(&Cf[o], v[q]);
+                            continue;
+                        }
                         float x = v[q] + (bias ? bias[n] : 0.0f);
                         if (Cpre)
-                            Cpre[(size_t)row * ldc + n] = x;
+                            Cpre[o] = x;
                         if (act == kActSilu)
                             x = silu(x);
+                        else if (act == kActSiluGrad)
+                            x *= silu_grad(Z[o]);
                         if (Cf)
-                            Cf[(size_t)row * ldc + n] = x;
+                            Cf[o] = x;
                         if (Cb)
-                            Cb[(size_t)row * ldc + n] = __float2bfloat16_rn(x);
+                            Cb[o] = __float2bfloat16_rn(x);
                     }
                 }
             }

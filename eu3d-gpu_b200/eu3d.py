@@ -89,7 +89,17 @@ def library():
         lib.eu_mlp_last_error.restype = ctypes.c_char_p
         lib.eu_mlp_last_error.argtypes = [_P]
         lib.eu_mlp_gemm.argtypes = [_P, _P, _I, _P, _I, _I, _I, _I, _P, _I, _P, _P, _P, _I, _P]
-        for fn in ("eu_mlp_create", "eu_mlp_destroy", "eu_mlp_gemm"):
+        lib.eu_mlp_init.argtypes = [_P, _I, _I, _I, _I, _I, _I, ctypes.c_uint]
+        lib.eu_mlp_set_scaling.argtypes = [_P, _P, _P, _P, _P]
+        lib.eu_mlp_num_params.restype = ctypes.c_longlong
+        lib.eu_mlp_num_params.argtypes = [_P]
+        lib.eu_mlp_get_params.argtypes = [_P, _P]
+        lib.eu_mlp_set_params.argtypes = [_P, _P]
+        lib.eu_mlp_loss_grad.argtypes = [_P, _I, _P, _P, _I, _P, _P]
+        lib.eu_mlp_train.argtypes = [_P, _P, _P, ctypes.c_longlong, _I, _I, ctypes.c_float, ctypes.c_uint, _P]
+        lib.eu_mlp_predict.argtypes = [_P, _P, ctypes.c_longlong, _P]
+        for fn in ("eu_mlp_create", "eu_mlp_destroy", "eu_mlp_gemm", "eu_mlp_init", "eu_mlp_set_scaling",
+                   "eu_mlp_get_params", "eu_mlp_set_params", "eu_mlp_loss_grad", "eu_mlp_train", "eu_mlp_predict"):
             getattr(lib, fn).restype = _I
         for fn in ("eu_read_grid", "eu_parse_mechanism", "eu_initial_state", "eu_create", "eu_destroy",
                    "eu_load_mechanism", "eu_set_mechanism", "eu_get_mechanism", "eu_node_coordinates",
@@ -282,6 +292,45 @@ class Mlp:
     def _check(self, st, what):
         if st:
             raise EU3DError(st, f"{what}: {library().eu_mlp_last_error(self.h).decode()}")
+
+    def init(self, n_in, width, hidden, n_out, members, max_batch=8192, seed=1):
+        self.shape = (n_in, width, hidden, n_out, members)
+        self._check(library().eu_mlp_init(self.h, n_in, width, hidden, n_out, members, max_batch, seed), "init")
+
+    def set_scaling(self, in_shift, in_scale, out_shift, out_scale):
+        a = [np.ascontiguousarray(v, dtype=np.float32) for v in (in_shift, in_scale, out_shift, out_scale)]
+        self._check(library().eu_mlp_set_scaling(self.h, *[v.ctypes.data for v in a]), "set_scaling")
+
+    def num_params(self):
+        return int(library().eu_mlp_num_params(self.h))
+
+    def get_params(self):
+        out = np.zeros(self.num_params(), np.float32)
+        self._check(library().eu_mlp_get_params(self.h, out.ctypes.data), "get_params")
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.num_params()
+        self._check(library().eu_mlp_set_params(self.h, p.ctypes.data), "set_params")
+
+    def loss_grad(self, member, X, T):
+        """X, T: torch CUDA fp32 tensors (n x n_in, n x n_out)."""
+        loss = ctypes.c_float()
+        g = np.zeros(self.num_params() // self.shape[4], np.float32)
+        self._check(library().eu_mlp_loss_grad(self.h, member, X.data_ptr(), T.data_ptr(), X.shape[0],
+                                               ctypes.byref(loss), g.ctypes.data), "loss_grad")
+        return loss.value, g
+
+    def train(self, X, T, batch, steps, lr, seed=1):
+        losses = np.zeros(self.shape[4], np.float32)
+        self._check(library().eu_mlp_train(self.h, X.data_ptr(), T.data_ptr(), X.shape[0], batch, steps, lr, seed,
+                                           losses.ctypes.data), "train")
+        return losses
+
+    def predict(self, X, out):
+        """out: torch CUDA fp32 tensor (members x n x n_out)."""
+        self._check(library().eu_mlp_predict(self.h, X.data_ptr(), X.shape[0], out.data_ptr()), "predict")
 
     def gemm(self, A, B, bias=None, act=0, Cf=None, Cb=None, Cpre=None, stream=None):
         """C = act(A @ B.T + bias) on torch CUDA tensors (A, B bf16, row-major)."""

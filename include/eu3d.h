@@ -201,6 +201,32 @@ const char *eu_mlp_last_error(const eu_mlp *m);
 eu_status eu_mlp_gemm(eu_mlp *m, const void *A, int lda, const void *B, int ldb, int M, int N, int K,
                       const float *bias, int act, float *Cf, void *Cb, float *Cpre, int ldc, void *stream);
 
+/* Build an ensemble of `members` MLPs n_in -> width (x hidden_layers, SiLU) ->
+ * n_out with He-uniform weights from `seed`; max_batch (multiple of 16) sizes
+ * the device scratch. BF16 weights/activations, fp32 master weights. */
+eu_status eu_mlp_init(eu_mlp *m, int n_in, int width, int hidden_layers, int n_out, int members, int max_batch,
+                      unsigned seed);
+/* Affine normalisation: network input = (x - in_shift) * in_scale, physical
+ * output = y / out_scale + out_shift (host arrays of n_in / n_out floats). */
+eu_status eu_mlp_set_scaling(eu_mlp *m, const float *in_shift, const float *in_scale, const float *out_shift,
+                             const float *out_scale);
+/* Parameters flattened per member, per layer: W (out x in, row-major) then b. */
+long long eu_mlp_num_params(const eu_mlp *m);
+eu_status eu_mlp_get_params(eu_mlp *m, float *out);
+eu_status eu_mlp_set_params(eu_mlp *m, const float *in);
+/* Mean-squared-error loss (normalised outputs) and its gradient for one member
+ * on n rows (device fp32 X [n x n_in], T [n x n_out]; n % 16 == 0); gradients
+ * to host in the parameter order above (NULL to skip). */
+eu_status eu_mlp_loss_grad(eu_mlp *m, int member, const float *X, const float *T, int n, float *loss,
+                           float *grads);
+/* `steps` Adam steps per member on random batches drawn on the device from
+ * n training rows (device fp32 X, T); mean_loss receives each member's last
+ * batch loss. */
+eu_status eu_mlp_train(eu_mlp *m, const float *X, const float *T, long long n, int batch, int steps, float lr,
+                       unsigned seed, float *mean_loss);
+/* Physical outputs of every member: out[member][row][n_out] (device fp32). */
+eu_status eu_mlp_predict(eu_mlp *m, const float *X, long long n, float *out);
+
 #ifdef __cplusplus
 }
 #endif
