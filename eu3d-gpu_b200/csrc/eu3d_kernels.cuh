@@ -262,6 +262,86 @@ struct TableRates {
     }
 };
 
+// Nchem prediction (Reaction::TrapezoidPrediction, src/Reaction.cpp:865-942)
+// and the Nchem trapezoid substeps with state recovery after each
+// (src/Euler.cpp:462-493, src/Reaction.cpp:562-805, src/Flowfield.cpp:1521-1536)
+// on a recovered cell state. The prediction's rate evaluation is reused by
+// the first substep: both evaluate the same expression on the same state.
+// Returns Nchem; a prediction <= 0 or above max_substeps is counted as an error.
+template <int NS, class Rt>
+__device__ __forceinline__ int react_cell(const DevMech &m, CellState<NS> &cell, double dtm, int max_substeps,
+                                          unsigned long long *counters, double *cms, long long cms_stride)
+{
+    double mc[NS];
+    scaled_concentrations<NS>(m, cell, mc);
+    SpeciesRates<NS> rates;
+    Rt::rates(m, cell.T, mc, rates);
+    double dt = dtm;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        if (cell.Y[s] >= 1e-6 && rates.W[s] != 0) {
+            const double dt_temp = fabs(-(cell.cs[s] * 1e-3) / rates.W[s]);
+            if (dt_temp < dt)
+                dt = dt_temp;
+        }
+    }
+    const double ratio = ceil(dtm / dt);
+    int nchem;
+    if (!(ratio >= 1.0) || ratio > double(max_substeps)) {
+        atomicAdd(&counters[kCntBadNchem], 1ULL);
+        nchem = (ratio > double(max_substeps)) ? max_substeps : 0;
+    } else {
+        nchem = int(ratio);
+    }
+    if (nchem > 0) {
+        atomicMax(&counters[kCntMaxNchem], (unsigned long long)nchem);
+        atomicAdd(&counters[kCntSumNchem], (unsigned long long)nchem);
+    }
+    const double dts = dtm / nchem;
+    for (int step = 0; step < nchem; ++step) {
+        if (step > 0) {
+            scaled_concentrations<NS>(m, cell, mc);
+            Rt::rates(m, cell.T, mc, rates);
+        }
+        if (cms) {
+#pragma unroll
+            for (int s = 0; s < NS; ++s) cms[s * cms_stride] = rates.W[s] * 1e3;
+        }
+        trapezoid_substep<NS>(m, rates, dts, mc, cell);
+    }
+    return nchem;
+}
+
+template <int NS>
+__device__ __forceinline__ void load_cell(const DevState &st, long long n3, long long c, CellState<NS> &cell)
+{
+#pragma unroll
+    for (int q = 0; q < NS + 4; ++q) cell.cs[q] = st.cs[q * n3 + c];
+    cell.T = st.T[c];
+    cell.E = st.E[c];
+}
+
+// The recovered state of a cell whose recovery already ran and was stored:
+// D, Y, u, v, w are re-formed from CS with the expressions of recover_state
+// (same values), T and E are the stored ones.
+template <int NS>
+__device__ __forceinline__ void load_recovered(const DevState &st, long long n3, long long c, CellState<NS> &cell)
+{
+    load_cell<NS>(st, n3, c, cell);
+    double D = 0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) D += cell.cs[s];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) cell.Y[s] = cell.cs[s] / D;
+    cell.D = D;
+    cell.U = cell.cs[NS + 0] / D;
+    cell.V = cell.cs[NS + 1] / D;
+    cell.W = cell.cs[NS + 2] / D;
+}
+
+// Post-advection state recovery (Flowfield::Update_after_Adv ->
+// Update_after_CS, src/Flowfield.cpp:1579-1617) followed, in the stiff modes,
+// by the kinetics of react_cell. One thread per interior node.
 template <int NS, int NR, bool kReact, class Rt>
 __global__ void __launch_bounds__(128) k_recover_react(const __grid_constant__ DevMech m, const DevGrid g,
                                                        const DevState st, const double *__restrict__ dt_dev,
@@ -277,54 +357,238 @@ __global__ void __launch_bounds__(128) k_recover_react(const __grid_constant__ D
     const long long n3 = g.n3;
     const long long c = cell_index(g, i, j, k);
     CellState<NS> cell;
-#pragma unroll
-    for (int q = 0; q < NS + 4; ++q) cell.cs[q] = st.cs[q * n3 + c];
-    cell.T = st.T[c];
-    cell.E = st.E[c];
+    load_cell<NS>(st, n3, c, cell);
     recover_state<NS>(m, cell);
+    if (kReact)
+        st.nchem[c] = react_cell<NS, Rt>(m, cell, *dt_dev, max_substeps, st.counters, st.cms ? st.cms + c : nullptr,
+                                         n3);
+    store_cell<NS>(m, st, n3, c, cell);
+}
 
-    if (kReact) {
-        const double dtm = *dt_dev;
-        double mc[NS];
-        scaled_concentrations<NS>(m, cell, mc);
-        SpeciesRates<NS> rates;
-        Rt::rates(m, cell.T, mc, rates);
-        double dt = dtm;
+// ------------------------------------------------- learned chemistry
+
+// Post-advection recovery of every cell; cells with chemistry to do are
+// appended to the learned queue (warp-aggregated atomics), the others are
+// final. Every cell's recovered state is stored.
+template <int NS>
+__global__ void __launch_bounds__(128) k_recover_classify(const __grid_constant__ DevMech m, const DevGrid g,
+                                                          const DevState st, LearnedParams lp)
+{
+    const long long ncell = (long long)g.ni * g.nj * g.nk;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool active = false;
+    long long c = 0;
+    if (t < ncell) {
+        const int k = g.bc + int(t % g.nk);
+        const int j = g.bc + int((t / g.nk) % g.nj);
+        const int i = g.bc + int(t / ((long long)g.nk * g.nj));
+        const long long n3 = g.n3;
+        c = cell_index(g, i, j, k);
+        CellState<NS> cell;
+        load_cell<NS>(st, n3, c, cell);
+        recover_state<NS>(m, cell);
+        store_cell<NS>(m, st, n3, c, cell);
+        double reactive = 0;
 #pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            if (cell.Y[s] >= 1e-6 && rates.W[s] != 0) {
-                const double dt_temp = fabs(-(cell.cs[s] * 1e-3) / rates.W[s]);
-                if (dt_temp < dt)
-                    dt = dt_temp;
+        for (int s = 0; s < NS; ++s)
+            if (!lp.inert[s])
+                reactive += cell.Y[s];
+        active = reactive >= lp.frozen_y && cell.T >= lp.frozen_T;
+        st.nchem[c] = 0;
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, active);
+    if (mask) {
+        const int lane = threadIdx.x & 31;
+        int base = 0;
+        if (lane == __ffs(mask) - 1)
+            base = atomicAdd(&lp.counts[0], __popc(mask));
+        base = __shfl_sync(0xffffffffu, base, __ffs(mask) - 1);
+        if (active)
+            lp.queue[base + __popc(mask & ((1u << lane) - 1))] = int(c);
+    }
+}
+
+// Model inputs of the queued cells: T, log10 p, Y_0..Y_{NS-1}, log10 dt, with
+// p = rho R T and R = 8314.34 / Wav (Update_after_CS, src/Flowfield.cpp:1606-1608).
+template <int NS>
+__global__ void k_learned_features(const __grid_constant__ DevMech m, const DevGrid g, const DevState st,
+                                   LearnedParams lp, const double *__restrict__ dt_dev)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= lp.counts[0])
+        return;
+    const long long n3 = g.n3, c = lp.queue[q];
+    CellState<NS> cell;
+    load_recovered<NS>(st, n3, c, cell);
+    float *f = lp.feat + (long long)q * (NS + 3);
+    double inv_w = 0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) inv_w += cell.Y[s] / m.mw[s];
+    f[0] = float(cell.T);
+    f[1] = float(log10(cell.T * cell.D * (kRUniv * 1000 * inv_w)));
+#pragma unroll
+    for (int s = 0; s < NS; ++s) f[2 + s] = float(cell.Y[s]);
+    f[NS + 2] = float(log10(*dt_dev));
+}
+
+// Apply the ensemble's prediction to each queued cell, or send it to the stiff
+// fallback queue. Accepted when every input lies in the trained box and the
+// members' spread (largest per-output standard deviation, in output-scale
+// units) is below tau. The mean species change is projected onto element
+// conservation (which implies sum Y = 1), clipped at zero and renormalised;
+// density, momentum and internal energy are held (the reference's chemistry
+// changes only the species densities); T is re-solved by the Newton inversion
+// from the predicted T.
+template <int NS>
+__global__ void __launch_bounds__(128) k_learned_apply(const __grid_constant__ DevMech m, const DevGrid g,
+                                                       const DevState st, LearnedParams lp)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nq = lp.counts[0];
+    bool fallback = false;
+    int c = 0;
+    if (q < nq) {
+        const long long n3 = g.n3;
+        c = lp.queue[q];
+        const float *f = lp.feat + (long long)q * (NS + 3);
+        bool ok = true;
+#pragma unroll
+        for (int a = 0; a < NS + 3; ++a) ok = ok && f[a] >= float(lp.box_lo[a]) && f[a] <= float(lp.box_hi[a]);
+        double mean[NS + 1], spread = 0;
+#pragma unroll
+        for (int o = 0; o < NS + 1; ++o) {
+            double s1 = 0, s2 = 0;
+            for (int e = 0; e < lp.members; ++e) {
+                const double v = lp.pred[((long long)e * nq + q) * (NS + 1) + o];
+                s1 += v;
+                s2 += v * v;
             }
+            const double mu = s1 / lp.members;
+            const double var = fmax(s2 / lp.members - mu * mu, 0.0);
+            mean[o] = mu;
+            spread = fmax(spread, sqrt(var) * lp.out_scale[o]);
         }
-        const double ratio = ceil(dtm / dt);
-        int nchem;
-        if (!(ratio >= 1.0) || ratio > double(max_substeps)) {
-            atomicAdd(&st.counters[kCntBadNchem], 1ULL);
-            nchem = (ratio > double(max_substeps)) ? max_substeps : 0;
+        ok = ok && spread <= lp.tau && isfinite(spread);
+        if (ok) {
+            CellState<NS> cell;
+            load_recovered<NS>(st, n3, c, cell);
+            double dY[NS], Y[NS], sum = 0;
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                double d = 0;
+#pragma unroll
+                for (int r = 0; r < NS; ++r) d += lp.proj[s][r] * mean[r];
+                dY[s] = d;
+            }
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                Y[s] = fmax(cell.Y[s] + dY[s], 0.0);
+                sum += Y[s];
+            }
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                cell.Y[s] = Y[s] / sum;
+                cell.cs[s] = cell.D * cell.Y[s];
+            }
+            cell.T = newton_temperature<NS>(m, cell.T + mean[NS], cell.E, cell.Y);
+            store_cell<NS>(m, st, n3, c, cell);
+            atomicAdd(&st.counters[kCntLearned], 1ULL);
         } else {
-            nchem = int(ratio);
-        }
-        st.nchem[c] = nchem;
-        if (nchem > 0) {
-            atomicMax(&st.counters[kCntMaxNchem], (unsigned long long)nchem);
-            atomicAdd(&st.counters[kCntSumNchem], (unsigned long long)nchem);
-        }
-        const double dts = dtm / nchem;
-        for (int step = 0; step < nchem; ++step) {
-            if (step > 0) {
-                scaled_concentrations<NS>(m, cell, mc);
-                Rt::rates(m, cell.T, mc, rates);
-            }
-            if (st.cms) {
-#pragma unroll
-                for (int s = 0; s < NS; ++s) st.cms[s * n3 + c] = rates.W[s] * 1e3;
-            }
-            trapezoid_substep<NS>(m, rates, dts, mc, cell);
+            fallback = true;
         }
     }
+    const unsigned mask = __ballot_sync(0xffffffffu, fallback);
+    if (mask) {
+        const int lane = threadIdx.x & 31;
+        int base = 0;
+        if (lane == __ffs(mask) - 1)
+            base = atomicAdd(&lp.counts[1], __popc(mask));
+        base = __shfl_sync(0xffffffffu, base, __ffs(mask) - 1);
+        if (fallback)
+            lp.fallback[base + __popc(mask & ((1u << lane) - 1))] = c;
+    }
+}
+
+// The stiff kinetics on a queue of cells whose recovered state is stored.
+template <int NS, class Rt>
+__global__ void __launch_bounds__(128) k_react_queue(const __grid_constant__ DevMech m, const DevGrid g,
+                                                     const DevState st, const int *__restrict__ queue,
+                                                     const int *__restrict__ count, const double *__restrict__ dt_dev,
+                                                     int max_substeps, int counter)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= *count)
+        return;
+    const long long n3 = g.n3, c = queue[q];
+    CellState<NS> cell;
+    load_recovered<NS>(st, n3, c, cell);
+    st.nchem[c] = react_cell<NS, Rt>(m, cell, *dt_dev, max_substeps, st.counters, st.cms ? st.cms + c : nullptr, n3);
     store_cell<NS>(m, st, n3, c, cell);
+    atomicAdd(&st.counters[counter], 1ULL);
+}
+
+// ------------------------------------------------- independent cell samples
+// (training data for the learned model: the stiff chemistry on a batch of
+// constant-volume, constant-energy cells, each with its own dt)
+
+// Conserved state of cells at rest from (T, p, Y): FieldInitial's formulas
+// (src/Flowfield.cpp:226-262). cs: NS + 4 planes of n; Y: NS planes of n.
+template <int NS>
+__global__ void k_state_from_tpy(const __grid_constant__ DevMech m, long long n, const double *__restrict__ T,
+                                 const double *__restrict__ p, const double *__restrict__ Y, double *cs, double *E)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    double y[NS], inv_w = 0, e = 0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) y[s] = Y[s * n + i];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) inv_w += y[s] / m.mw[s];
+    const double Tc = T[i];
+    const double D = p[i] / (kRUniv * 1000 * inv_w * Tc);
+    const TPow pw = make_tpow(Tc, true);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) e += y[s] * (h_species<NS>(m, pw, m.ri[s], s) - m.ri[s] * Tc);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) cs[s * n + i] = D * y[s];
+    cs[(NS + 0) * n + i] = 0;
+    cs[(NS + 1) * n + i] = 0;
+    cs[(NS + 2) * n + i] = 0;
+    cs[(NS + 3) * n + i] = D * e * 1000;
+    E[i] = e * 1000;
+}
+
+// One chemistry step (react_cell) of each sample with its own dt, in place.
+template <int NS, class Rt>
+__global__ void __launch_bounds__(128) k_chem_samples(const __grid_constant__ DevMech m, long long n, double *cs,
+                                                      double *T, double *E, const double *__restrict__ dt,
+                                                      int *nchem, int max_substeps, unsigned long long *counters)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    CellState<NS> cell;
+#pragma unroll
+    for (int q = 0; q < NS + 4; ++q) cell.cs[q] = cs[q * n + i];
+    cell.T = T[i];
+    cell.E = E[i];
+    double D = 0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) D += cell.cs[s];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) cell.Y[s] = cell.cs[s] / D;
+    cell.D = D;
+    cell.U = cell.cs[NS] / D;
+    cell.V = cell.cs[NS + 1] / D;
+    cell.W = cell.cs[NS + 2] / D;
+    const int nc = react_cell<NS, Rt>(m, cell, dt[i], max_substeps, counters, nullptr, 0);
+    if (nchem)
+        nchem[i] = nc;
+#pragma unroll
+    for (int q = 0; q < NS + 4; ++q) cs[q * n + i] = cell.cs[q];
+    T[i] = cell.T;
+    E[i] = cell.E;
 }
 
 // Derived output fields of Update_after_CS that the timestep does not keep

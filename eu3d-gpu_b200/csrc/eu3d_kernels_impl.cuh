@@ -84,6 +84,73 @@ cudaError_t derived_t(const LaunchArgs &a, int which, double *out)
     return cudaGetLastError();
 }
 
+template <int NS, int NR>
+cudaError_t classify_t(const LaunchArgs &a, const LearnedParams &lp)
+{
+    const long long n = (long long)a.g.ni * a.g.nj * a.g.nk;
+    k_recover_classify<NS><<<dim3(unsigned((n + 127) / 128)), 128, 0, a.stream>>>(*a.mech, a.g, a.st, lp);
+    return cudaGetLastError();
+}
+
+template <int NS, int NR>
+cudaError_t features_t(const LaunchArgs &a, const LearnedParams &lp, int nq)
+{
+    if (nq <= 0)
+        return cudaSuccess;
+    k_learned_features<NS><<<dim3(unsigned((nq + 127) / 128)), 128, 0, a.stream>>>(*a.mech, a.g, a.st, lp, a.dt_dev);
+    return cudaGetLastError();
+}
+
+template <int NS, int NR>
+cudaError_t apply_t(const LaunchArgs &a, const LearnedParams &lp, int nq)
+{
+    if (nq <= 0)
+        return cudaSuccess;
+    k_learned_apply<NS><<<dim3(unsigned((nq + 127) / 128)), 128, 0, a.stream>>>(*a.mech, a.g, a.st, lp);
+    return cudaGetLastError();
+}
+
+template <int NS, int NR>
+cudaError_t react_queue_t(const LaunchArgs &a, const int *queue, const int *count, int nq, int counter)
+{
+    if (nq <= 0)
+        return cudaSuccess;
+    const dim3 grid(unsigned((nq + 127) / 128));
+    if (a.spec == 1 && NS == Mech_JA919::NS && NR == Mech_JA919::NR)
+        k_react_queue<NS, Mech_JA919><<<grid, 128, 0, a.stream>>>(*a.mech, a.g, a.st, queue, count, a.dt_dev,
+                                                                  a.max_substeps, counter);
+    else
+        k_react_queue<NS, TableRates<NS, NR>><<<grid, 128, 0, a.stream>>>(*a.mech, a.g, a.st, queue, count,
+                                                                          a.dt_dev, a.max_substeps, counter);
+    return cudaGetLastError();
+}
+
+template <int NS, int NR>
+cudaError_t state_from_tpy_t(const LaunchArgs &a, long long n, const double *T, const double *p, const double *Y,
+                             double *cs, double *E)
+{
+    if (n <= 0)
+        return cudaSuccess;
+    k_state_from_tpy<NS><<<dim3(unsigned((n + 127) / 128)), 128, 0, a.stream>>>(*a.mech, n, T, p, Y, cs, E);
+    return cudaGetLastError();
+}
+
+template <int NS, int NR>
+cudaError_t chem_samples_t(const LaunchArgs &a, long long n, double *cs, double *T, double *E, const double *dt,
+                           int *nchem)
+{
+    if (n <= 0)
+        return cudaSuccess;
+    const dim3 grid(unsigned((n + 127) / 128));
+    if (a.spec == 1 && NS == Mech_JA919::NS && NR == Mech_JA919::NR)
+        k_chem_samples<NS, Mech_JA919><<<grid, 128, 0, a.stream>>>(*a.mech, n, cs, T, E, dt, nchem, a.max_substeps,
+                                                                   a.st.counters);
+    else
+        k_chem_samples<NS, TableRates<NS, NR>><<<grid, 128, 0, a.stream>>>(*a.mech, n, cs, T, E, dt, nchem,
+                                                                           a.max_substeps, a.st.counters);
+    return cudaGetLastError();
+}
+
 } // namespace
 
 // Supported (NS, NR): the repository mechanism H2_JA919 (9 species, 19
@@ -100,6 +167,27 @@ cudaError_t launch_boundary(const LaunchArgs &a) { EU3D_DISPATCH(boundary_t, a) 
 cudaError_t launch_flux_update(const LaunchArgs &a) { EU3D_DISPATCH(flux_t, a) }
 cudaError_t launch_recover_react(const LaunchArgs &a, bool react) { EU3D_DISPATCH(react_t, a, react) }
 cudaError_t launch_derived(const LaunchArgs &a, int which, double *out) { EU3D_DISPATCH(derived_t, a, which, out) }
+
+cudaError_t launch_recover_classify(const LaunchArgs &a, const LearnedParams &lp) { EU3D_DISPATCH(classify_t, a, lp) }
+cudaError_t launch_learned_features(const LaunchArgs &a, const LearnedParams &lp, int nq)
+{
+    EU3D_DISPATCH(features_t, a, lp, nq)
+}
+cudaError_t launch_learned_apply(const LaunchArgs &a, const LearnedParams &lp, int nq) { EU3D_DISPATCH(apply_t, a, lp, nq) }
+cudaError_t launch_react_queue(const LaunchArgs &a, const int *queue, const int *count, int nq, int counter)
+{
+    EU3D_DISPATCH(react_queue_t, a, queue, count, nq, counter)
+}
+cudaError_t launch_state_from_tpy(const LaunchArgs &a, long long n, const double *T, const double *p, const double *Y,
+                                  double *cs, double *E)
+{
+    EU3D_DISPATCH(state_from_tpy_t, a, n, T, p, Y, cs, E)
+}
+cudaError_t launch_chem_samples(const LaunchArgs &a, long long n, double *cs, double *T, double *E, const double *dt,
+                                int *nchem)
+{
+    EU3D_DISPATCH(chem_samples_t, a, n, cs, T, E, dt, nchem)
+}
 
 cudaError_t launch_set_value(double *dst, double v, cudaStream_t s)
 {

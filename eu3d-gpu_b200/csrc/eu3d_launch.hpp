@@ -30,6 +30,15 @@ bool sizes_supported(int ns, int nr);
     cudaError_t launch_recover_react(const LaunchArgs &a, bool react);                             \
     cudaError_t launch_derived(const LaunchArgs &a, int which, double *out);                       \
     cudaError_t launch_set_value(double *dst, double v, cudaStream_t s);                           \
+    cudaError_t launch_recover_classify(const LaunchArgs &a, const LearnedParams &lp);             \
+    cudaError_t launch_learned_features(const LaunchArgs &a, const LearnedParams &lp, int nq);     \
+    cudaError_t launch_learned_apply(const LaunchArgs &a, const LearnedParams &lp, int nq);        \
+    cudaError_t launch_react_queue(const LaunchArgs &a, const int *queue, const int *count, int nq, \
+                                   int counter);                                                   \
+    cudaError_t launch_state_from_tpy(const LaunchArgs &a, long long n, const double *T,           \
+                                      const double *p, const double *Y, double *cs, double *E);    \
+    cudaError_t launch_chem_samples(const LaunchArgs &a, long long n, double *cs, double *T,       \
+                                    double *E, const double *dt, int *nchem);                      \
     }
 
 EU3D_DECLARE_LAUNCHERS(strict)

@@ -65,4 +65,20 @@ enum CounterIdx {
     kCntCount = 8
 };
 
+// Parameters and buffers of the learned-chemistry step (set by eu_set_learned).
+struct LearnedParams {
+    float *feat;           // [queue capacity x (3 + NS)] fp32 model inputs
+    float *pred;           // [members x queue length x (NS + 1)] fp32 physical outputs
+    int *queue, *fallback; // cell indices
+    int *counts;           // [0] learned queue length, [1] fallback queue length
+    int members;
+    double frozen_y;       // a cell whose non-inert mass fraction is below this is frozen
+    double frozen_T;       // a cell colder than this is frozen (0 disables)
+    double tau;            // largest accepted ensemble spread, in output-scale units
+    double box_lo[kMaxS + 3], box_hi[kMaxS + 3]; // accepted input ranges
+    double out_scale[kMaxS + 1];
+    double proj[kMaxS][kMaxS]; // element-conservation projector
+    int inert[kMaxS];
+};
+
 } // namespace eu3d

@@ -45,6 +45,11 @@ class MechanismC(ctypes.Structure):
                                                             "stoi_f", "stoi_b", "tb")]
 
 
+class LearnedConfig(ctypes.Structure):
+    _fields_ = [("tau", _D), ("frozen_y", _D), ("frozen_T", _D), ("box_lo", _P), ("box_hi", _P),
+                ("out_scale", _P)]
+
+
 class StepStats(ctypes.Structure):
     _fields_ = [("steps", _I), ("max_nchem", _I), ("sum_nchem", ctypes.c_longlong),
                 ("reacting", ctypes.c_longlong), ("learned", ctypes.c_longlong), ("fallback", ctypes.c_longlong),
@@ -84,6 +89,11 @@ def library():
         lib.eu_get_field.argtypes = [_P, ctypes.c_char_p, _P]
         lib.eu_sync.argtypes = [_P]
         lib.eu_device_info.argtypes = [_P, ctypes.POINTER(_P), ctypes.POINTER(ctypes.c_size_t)]
+        lib.eu_chem_states.argtypes = [_P, ctypes.c_longlong, _P, _P, _P, _P, _P]
+        lib.eu_chem_advance.argtypes = [_P, ctypes.c_longlong, _P, _P, _P, _P, _P]
+        lib.eu_set_learned.argtypes = [_P, _P, ctypes.POINTER(LearnedConfig)]
+        for fn in ("eu_chem_states", "eu_chem_advance", "eu_set_learned"):
+            getattr(lib, fn).restype = _I
         lib.eu_mlp_create.argtypes = [_I, ctypes.POINTER(_P)]
         lib.eu_mlp_destroy.argtypes = [_P]
         lib.eu_mlp_last_error.restype = ctypes.c_char_p
@@ -260,6 +270,24 @@ class Solver:
 
     def sync(self):
         self._check(library().eu_sync(self.h), "sync")
+
+    def chem_states(self, T, p, Y, cs, E):
+        """Torch CUDA float64 tensors: T, p (n), Y (ns x n) -> cs (ns+4 x n), E (n)."""
+        n = T.shape[0]
+        self._check(library().eu_chem_states(self.h, n, T.data_ptr(), p.data_ptr(), Y.data_ptr(), cs.data_ptr(),
+                                             E.data_ptr()), "chem_states")
+
+    def chem_advance(self, cs, T, E, dt, nchem=None):
+        n = T.shape[0]
+        self._check(library().eu_chem_advance(self.h, n, cs.data_ptr(), T.data_ptr(), E.data_ptr(), dt.data_ptr(),
+                                              None if nchem is None else nchem.data_ptr()), "chem_advance")
+
+    def set_learned(self, model, tau, box_lo, box_hi, out_scale, frozen_y=1e-9, frozen_T=0.0):
+        self._learned_keep = [np.ascontiguousarray(v, dtype=np.float64) for v in (box_lo, box_hi, out_scale)]
+        cfg = LearnedConfig(float(tau), float(frozen_y), float(frozen_T),
+                            *[v.ctypes.data for v in self._learned_keep])
+        self._model = model
+        self._check(library().eu_set_learned(self.h, model.h, ctypes.byref(cfg)), "set_learned")
 
     def device_info(self):
         stream = _P()

@@ -2,6 +2,9 @@
 // uploads/downloads and the per-timestep launch sequence.
 #include "eu3d.h"
 
+#include <array>
+#include <cctype>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -13,6 +16,7 @@
 
 #include "../csrc/eu3d_launch.hpp"
 #include "eu3d_mech_JA919_tables.h"
+#include "mlp_internal.hpp"
 #include "readers.hpp"
 #include "state_init.hpp"
 
@@ -37,6 +41,11 @@ struct eu_handle {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t pev[4] = {nullptr, nullptr, nullptr, nullptr}; // phase boundaries (cfg.profile)
+    // learned chemistry
+    eu_mlp *model = nullptr;
+    LearnedParams lp{};
+    long long lp_capacity = 0;
+    int *h_counts = nullptr; // pinned [2]
     std::string err;
 };
 
@@ -309,8 +318,6 @@ eu_status eu_create(const eu_config *cfg, eu_handle **out)
         return EU_ERR_INVALID_ARGUMENT;
     if (cfg->chemistry != EU_CHEM_STIFF && cfg->chemistry != EU_CHEM_FROZEN && cfg->chemistry != EU_CHEM_LEARNED)
         return EU_ERR_INVALID_ARGUMENT;
-    if (cfg->chemistry == EU_CHEM_LEARNED)
-        return EU_ERR_UNSUPPORTED;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return EU_ERR_CUDA;
@@ -382,6 +389,8 @@ eu_status eu_destroy(eu_handle *h)
     if (h->stream)
         cudaStreamSynchronize(h->stream);
     free_all(h);
+    if (h->h_counts)
+        cudaFreeHost(h->h_counts);
     for (auto &e : h->pev)
         if (e) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -500,6 +509,209 @@ eu_status eu_set_primitive(eu_handle *h, const double *P, const double *T, const
                         &prim[4 * n3], &prim[5 * n3], &prim[6 * n3], &prim[7 * n3]);
 }
 
+namespace {
+
+// Atoms of each element in a species name such as "H2O2" or "AR".
+bool element_counts(const std::string &name, double (&cnt)[6])
+{
+    static const char *sym[6] = {"H", "O", "N", "C", "AR", "HE"};
+    for (double &c : cnt) c = 0;
+    size_t i = 0;
+    std::string up;
+    for (char ch : name) up += char(std::toupper((unsigned char)ch));
+    while (i < up.size()) {
+        int e = -1;
+        if (up.compare(i, 2, "AR") == 0) e = 4;
+        else if (up.compare(i, 2, "HE") == 0) e = 5;
+        else if (up[i] == 'H') e = 0;
+        else if (up[i] == 'O') e = 1;
+        else if (up[i] == 'N') e = 2;
+        else if (up[i] == 'C') e = 3;
+        if (e < 0)
+            return false;
+        i += std::strlen(sym[e]);
+        int n = 0;
+        while (i < up.size() && std::isdigit((unsigned char)up[i])) n = n * 10 + (up[i++] - '0');
+        cnt[e] += n ? n : 1;
+    }
+    return true;
+}
+
+// P = I - A^T (A A^T)^-1 A with A[e][s] the mass fraction of element e in
+// species s: the closest change (in the Euclidean sense) that conserves every
+// element's mass, which also conserves sum Y. Without species names the
+// projector only removes the mean (sum Y conserved).
+void element_projector(const MechanismTables &m, double (&P)[kMaxS][kMaxS])
+{
+    static const double aw[6] = {1.00794, 15.9994, 14.0067, 12.011, 39.948, 4.002602};
+    const int ns = m.ns;
+    std::vector<std::vector<double>> A;
+    bool named = (int)m.species.size() >= ns;
+    std::vector<std::array<double, 6>> cnt(ns);
+    for (int s = 0; named && s < ns; ++s) {
+        double c[6];
+        named = element_counts(m.species[s], c);
+        for (int e = 0; e < 6; ++e) cnt[s][e] = c[e];
+    }
+    if (named) {
+        for (int e = 0; e < 6; ++e) {
+            std::vector<double> row(ns, 0.0);
+            bool any = false;
+            for (int s = 0; s < ns; ++s) {
+                row[s] = cnt[s][e] * aw[e] / m.mw[s];
+                any |= row[s] != 0;
+            }
+            if (any)
+                A.push_back(row);
+        }
+    } else {
+        A.push_back(std::vector<double>(ns, 1.0));
+    }
+    const int ne = (int)A.size();
+    // G = A A^T, solve G X = A for X (ne x ns), P = I - A^T X
+    std::vector<std::vector<double>> G(ne, std::vector<double>(ne, 0.0)), X = A;
+    for (int a = 0; a < ne; ++a)
+        for (int b = 0; b < ne; ++b)
+            for (int s = 0; s < ns; ++s) G[a][b] += A[a][s] * A[b][s];
+    for (int c = 0; c < ne; ++c) { // Gauss-Jordan with partial pivoting
+        int piv = c;
+        for (int r = c + 1; r < ne; ++r)
+            if (std::fabs(G[r][c]) > std::fabs(G[piv][c])) piv = r;
+        std::swap(G[c], G[piv]);
+        std::swap(X[c], X[piv]);
+        const double d = G[c][c];
+        for (int k = 0; k < ne; ++k) G[c][k] /= d;
+        for (int s = 0; s < ns; ++s) X[c][s] /= d;
+        for (int r = 0; r < ne; ++r)
+            if (r != c) {
+                const double f = G[r][c];
+                for (int k = 0; k < ne; ++k) G[r][k] -= f * G[c][k];
+                for (int s = 0; s < ns; ++s) X[r][s] -= f * X[c][s];
+            }
+    }
+    for (int i = 0; i < kMaxS; ++i)
+        for (int j = 0; j < kMaxS; ++j) P[i][j] = 0.0;
+    for (int i = 0; i < ns; ++i)
+        for (int j = 0; j < ns; ++j) {
+            double v = (i == j) ? 1.0 : 0.0;
+            for (int e = 0; e < ne; ++e) v -= A[e][i] * X[e][j];
+            P[i][j] = v;
+        }
+}
+
+// One learned-chemistry phase of a step: recover + classify every cell,
+// features of the queued cells, the ensemble, gate + apply, stiff fallback.
+eu_status learned_chemistry(eu_handle *h, const LaunchArgs &a, bool strict_, long long *reacting)
+{
+    LearnedParams &lp = h->lp;
+    CK(h, cudaMemsetAsync(lp.counts, 0, 2 * sizeof(int), h->stream));
+    CK(h, strict_ ? strict::launch_recover_classify(a, lp) : fast::launch_recover_classify(a, lp));
+    CK(h, cudaMemcpyAsync(h->h_counts, lp.counts, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    const int nq = h->h_counts[0];
+    *reacting = nq;
+    if (nq == 0)
+        return EU_OK;
+    CK(h, strict_ ? strict::launch_learned_features(a, lp, nq) : fast::launch_learned_features(a, lp, nq));
+    eu_status s = mlp_predict_stream(h->model, lp.feat, nq, lp.pred, h->stream);
+    if (s != EU_OK)
+        return fail(h, s, "learned model: %s", eu_mlp_last_error(h->model));
+    CK(h, strict_ ? strict::launch_learned_apply(a, lp, nq) : fast::launch_learned_apply(a, lp, nq));
+    CK(h, cudaMemcpyAsync(h->h_counts + 1, lp.counts + 1, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    const int nf = h->h_counts[1];
+    if (nf > 0)
+        CK(h, strict_ ? strict::launch_react_queue(a, lp.fallback, lp.counts + 1, nf, kCntFallback)
+                      : fast::launch_react_queue(a, lp.fallback, lp.counts + 1, nf, kCntFallback));
+    return EU_OK;
+}
+
+} // namespace
+
+eu_status eu_chem_states(eu_handle *h, long long n, const double *T, const double *p, const double *Y, double *cs,
+                         double *E)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!T || !p || !Y || !cs || !E || n < 0)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "null argument");
+    if (!h->has_mech)
+        return fail(h, EU_ERR_NOT_READY, "load a mechanism first");
+    cudaSetDevice(h->cfg.device);
+    LaunchArgs a = launch_args(h);
+    CK(h, strict::launch_state_from_tpy(a, n, T, p, Y, cs, E));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return EU_OK;
+}
+
+eu_status eu_chem_advance(eu_handle *h, long long n, double *cs, double *T, double *E, const double *dt, int *nchem)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!cs || !T || !E || !dt || n < 0)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "null argument");
+    if (!h->has_mech)
+        return fail(h, EU_ERR_NOT_READY, "load a mechanism first");
+    cudaSetDevice(h->cfg.device);
+    LaunchArgs a = launch_args(h);
+    CK(h, cudaMemsetAsync(h->st.counters, 0, kCntCount * sizeof(unsigned long long), h->stream));
+    CK(h, strict::launch_chem_samples(a, n, cs, T, E, dt, nchem));
+    unsigned long long cnt[kCntCount];
+    CK(h, cudaMemcpyAsync(cnt, h->st.counters, sizeof cnt, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (cnt[kCntBadNchem])
+        return fail(h, EU_ERR_NCHEM, "%llu samples predicted Nchem <= 0 or above max_substeps", cnt[kCntBadNchem]);
+    return EU_OK;
+}
+
+eu_status eu_set_learned(eu_handle *h, eu_mlp *model, const eu_learned_config *lc)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!model || !lc || !lc->box_lo || !lc->box_hi || !lc->out_scale)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "null argument");
+    if (!h->has_mech)
+        return fail(h, EU_ERR_NOT_READY, "load a mechanism first");
+    int n_in = 0, n_out = 0, members = 0;
+    if (!mlp_shape(model, &n_in, &n_out, &members))
+        return fail(h, EU_ERR_NOT_READY, "the model is not initialised");
+    const int ns = h->mech.ns;
+    if (n_in != ns + 3 || n_out != ns + 1)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "model must map %d inputs to %d outputs", ns + 3, ns + 1);
+    cudaSetDevice(h->cfg.device);
+    const long long cap = (long long)h->ni * h->nj * h->nk;
+    LearnedParams &lp = h->lp;
+    if (h->lp_capacity < cap || lp.members != members) {
+        eu_status s;
+        if ((s = dalloc(h, &lp.feat, size_t(cap) * (ns + 3))) != EU_OK) return s;
+        if ((s = dalloc(h, &lp.pred, size_t(cap) * members * (ns + 1))) != EU_OK) return s;
+        if ((s = dalloc(h, &lp.queue, size_t(cap))) != EU_OK) return s;
+        if ((s = dalloc(h, &lp.fallback, size_t(cap))) != EU_OK) return s;
+        if ((s = dalloc(h, &lp.counts, size_t(2))) != EU_OK) return s;
+        h->lp_capacity = cap;
+    }
+    if (!h->h_counts)
+        CK(h, cudaMallocHost(&h->h_counts, 2 * sizeof(int)));
+    lp.members = members;
+    lp.tau = lc->tau;
+    lp.frozen_y = lc->frozen_y;
+    lp.frozen_T = lc->frozen_T;
+    for (int a = 0; a < ns + 3; ++a) {
+        lp.box_lo[a] = lc->box_lo[a];
+        lp.box_hi[a] = lc->box_hi[a];
+    }
+    for (int o = 0; o < ns + 1; ++o) lp.out_scale[o] = lc->out_scale[o];
+    element_projector(h->mech, lp.proj);
+    for (int s = 0; s < ns; ++s) {
+        bool used = false;
+        for (int r = 0; r < h->mech.nr; ++r)
+            used |= h->mech.stoi_f[s * h->mech.nr + r] != 0 || h->mech.stoi_b[s * h->mech.nr + r] != 0;
+        lp.inert[s] = used ? 0 : 1;
+    }
+    h->model = model;
+    return EU_OK;
+}
+
 eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
 {
     if (!h)
@@ -512,6 +724,10 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
     const bool prof = h->cfg.profile != 0 && stats != nullptr;
     const LaunchArgs a = launch_args(h);
     const bool react = h->cfg.chemistry == EU_CHEM_STIFF;
+    const bool learned = h->cfg.chemistry == EU_CHEM_LEARNED;
+    if (learned && !h->model)
+        return fail(h, EU_ERR_NOT_READY, "learned chemistry needs eu_set_learned first");
+    long long reacting = 0;
     const bool st_ = is_strict(h);
     double phase[4] = {0, 0, 0, 0};
     int launches = 0;
@@ -527,7 +743,14 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
         if (prof) CK(h, cudaEventRecord(h->pev[1], h->stream));
         CK(h, st_ ? strict::launch_flux_update(a) : fast::launch_flux_update(a));
         if (prof) CK(h, cudaEventRecord(h->pev[2], h->stream));
-        CK(h, st_ ? strict::launch_recover_react(a, react) : fast::launch_recover_react(a, react));
+        if (learned) {
+            eu_status ls = learned_chemistry(h, a, st_, &reacting);
+            if (ls != EU_OK)
+                return ls;
+            launches += 4;
+        } else {
+            CK(h, st_ ? strict::launch_recover_react(a, react) : fast::launch_recover_react(a, react));
+        }
         if (prof) {
             CK(h, cudaEventRecord(h->pev[3], h->stream));
             CK(h, cudaEventSynchronize(h->pev[3]));
@@ -551,7 +774,9 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
     stats->steps = nsteps;
     stats->max_nchem = int(cnt[kCntMaxNchem]);
     stats->sum_nchem = (long long)cnt[kCntSumNchem];
-    stats->reacting = react ? (long long)h->ni * h->nj * h->nk : 0;
+    stats->reacting = react ? (long long)h->ni * h->nj * h->nk : reacting;
+    stats->learned = (long long)cnt[kCntLearned];
+    stats->fallback = (long long)cnt[kCntFallback];
     stats->nonfinite = (long long)cnt[kCntNonfinite];
     stats->device_ms = ms;
     stats->launches = launches;

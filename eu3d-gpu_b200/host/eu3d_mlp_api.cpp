@@ -16,6 +16,7 @@
 
 #include "eu3d.h"
 #include "eu3d_mlp_kernels.hpp"
+#include "mlp_internal.hpp"
 
 namespace {
 
@@ -107,20 +108,23 @@ long long params_per_member(const eu_mlp *m)
     return n;
 }
 
-// forward of member e over n packed rows in m->X
-eu_status forward(eu_mlp *m, int e, int n)
+// forward of member e over n packed rows in m->X (on stream s; training keeps
+// the pre-activations)
+eu_status forward(eu_mlp *m, int e, int n, cudaStream_t s = nullptr, bool keep_pre = true)
 {
+    if (!s)
+        s = m->stream;
     auto &net = m->net[e];
     for (int l = 0; l < m->hidden; ++l) {
         const void *A = l == 0 ? m->X : m->H[l - 1];
         const int lda = l == 0 ? m->in_pad : m->width;
         const Layer &L = net[l];
-        MCK(m, eu3d::gemm_bf16(A, lda, L.Wb, L.in_pad, n, L.out_pad, L.in_pad, L.b, 1, nullptr, m->H[l], m->Z[l],
-                               m->width, nullptr, 1, m->d_err, m->stream));
+        MCK(m, eu3d::gemm_bf16(A, lda, L.Wb, L.in_pad, n, L.out_pad, L.in_pad, L.b, 1, nullptr, m->H[l],
+                               keep_pre ? m->Z[l] : nullptr, m->width, nullptr, 1, m->d_err, s));
     }
     const Layer &L = net[m->hidden];
     MCK(m, eu3d::gemm_bf16(m->H[m->hidden - 1], m->width, L.Wb, L.in_pad, n, L.out_pad, L.in_pad, L.b, 0, m->Y, nullptr,
-                           nullptr, m->out_pad, nullptr, 1, m->d_err, m->stream));
+                           nullptr, m->out_pad, nullptr, 1, m->d_err, s));
     return EU_OK;
 }
 
@@ -186,6 +190,35 @@ eu_status check_err(eu_mlp *m)
 }
 
 } // namespace
+
+namespace eu3d {
+bool mlp_shape(const eu_mlp *m, int *n_in, int *n_out, int *members)
+{
+    if (!m || !m->ready)
+        return false;
+    *n_in = m->n_in;
+    *n_out = m->n_out;
+    *members = m->members;
+    return true;
+}
+
+eu_status mlp_predict_stream(eu_mlp *m, const float *X, long long n, float *out, cudaStream_t s)
+{
+    for (long long r0 = 0; r0 < n; r0 += m->max_batch) {
+        const int nb = int(n - r0 < m->max_batch ? n - r0 : m->max_batch);
+        MCK(m, eu3d::pack_features(X + r0 * m->n_in, nb, m->n_in, nullptr, m->in_shift, m->in_scale, m->X, m->in_pad,
+                                   s));
+        for (int e = 0; e < m->members; ++e) {
+            eu_status st = forward(m, e, nb, s, false);
+            if (st != EU_OK)
+                return st;
+            MCK(m, eu3d::unscale_outputs(m->Y, nb, m->out_pad, m->n_out, m->out_shift, m->out_scale,
+                                         out + ((long long)e * n + r0) * m->n_out, s));
+        }
+    }
+    return EU_OK;
+}
+} // namespace eu3d
 
 extern "C" {
 

@@ -1,0 +1,153 @@
+"""Learned chemistry for the EU3D timestep: training data from the stiff
+integrator, training with the library's tensor-core kernels, calibration of the
+trust gate, and checkpoints.
+
+The model maps (T, log10 p, Y_0..Y_{ns-1}, log10 dt) of a cell after advection
+to the change (dY_0..dY_{ns-1}, dT) that the stiff kinetics (Nchem adaptive
+trapezoid substeps at fixed density and internal energy) produces over dt.
+
+Training states come from the library's own stiff integrator (eu_chem_advance)
+run along constant-volume, constant-energy trajectories. Each trajectory
+starts from a mixture of stoichiometric 2H2+O2 or H2-air (Y_H2 0.0285, Y_O2
+0.2264, Y_N2 0.7451) with N2, at T ~ U[300, 3500] K and p ~ logU[0.05, 5] MPa,
+and each step draws dt ~ logU[1e-9, 3e-7] s. All tensors stay on the GPU
+(torch provides the buffers; every computation is a libeu3d kernel).
+"""
+from __future__ import annotations
+
+import math
+import os
+
+import numpy as np
+
+import eu3d
+import eu3d_cases as cases
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CHECKPOINT = os.path.join(HERE, "data", "chem_mlp_ja919.npz")
+
+N_SPECIES = 9
+N_IN, N_OUT = N_SPECIES + 3, N_SPECIES + 1
+WIDTH, HIDDEN, MEMBERS = 256, 3, 3
+S_O2, S_H2, S_N2 = cases.S_O2, cases.S_H2, cases.S_N2
+
+
+def _initial_compositions(rng, n, mw):
+    """Mixtures of a reactive gas (2H2+O2 or H2-air) with N2."""
+    y_h2 = 2 * mw[S_H2] / (2 * mw[S_H2] + mw[S_O2])
+    bubble = np.zeros(N_SPECIES)
+    bubble[S_H2], bubble[S_O2] = y_h2, 1 - y_h2
+    air = np.zeros(N_SPECIES)
+    air[S_H2], air[S_O2], air[S_N2] = 0.0285, 0.2264, 0.7451
+    n2 = np.zeros(N_SPECIES)
+    n2[S_N2] = 1.0
+    f = rng.uniform(0, 1, n)
+    which = rng.uniform(0, 1, n) < 0.7
+    fuel = np.where(which[:, None], bubble[None, :], air[None, :])
+    Y = f[:, None] * fuel + (1 - f[:, None]) * n2[None, :]
+    return Y / Y.sum(axis=1, keepdims=True)
+
+
+def generate(solver, n_traj, n_steps, seed=11, t_range=(300.0, 3500.0), p_range=(5e4, 5e6), dt_range=(1e-9, 3e-7)):
+    """(inputs, targets) as torch CUDA fp32 tensors, n_traj * n_steps rows."""
+    import torch
+    rng = np.random.default_rng(seed)
+    mech = solver.mechanism()
+    ns = mech["ns"]
+    dev = "cuda"
+    T0 = rng.uniform(*t_range, n_traj)
+    p0 = np.exp(rng.uniform(math.log(p_range[0]), math.log(p_range[1]), n_traj))
+    Y0 = _initial_compositions(rng, n_traj, mech["mw"])
+    T = torch.tensor(T0, device=dev, dtype=torch.float64)
+    p = torch.tensor(p0, device=dev, dtype=torch.float64)
+    Yp = torch.tensor(np.ascontiguousarray(Y0.T), device=dev, dtype=torch.float64)
+    cs = torch.zeros(ns + 4, n_traj, device=dev, dtype=torch.float64)
+    E = torch.zeros(n_traj, device=dev, dtype=torch.float64)
+    solver.chem_states(T, p, Yp, cs, E)
+    mw = torch.tensor(mech["mw"], device=dev, dtype=torch.float64)
+    X = torch.empty(n_traj * n_steps, ns + 3, device=dev, dtype=torch.float32)
+    Tg = torch.empty(n_traj * n_steps, ns + 1, device=dev, dtype=torch.float32)
+    for k in range(n_steps):
+        dt = torch.exp(torch.empty(n_traj, device=dev, dtype=torch.float64).uniform_(
+            math.log(dt_range[0]), math.log(dt_range[1])))
+        D = cs[:ns].sum(0)
+        Y = cs[:ns] / D
+        P = T * D * (8.31434 * 1000 * (Y / mw[:, None]).sum(0))
+        rows = slice(k * n_traj, (k + 1) * n_traj)
+        X[rows, 0] = T.float()
+        X[rows, 1] = torch.log10(P).float()
+        X[rows, 2:2 + ns] = Y.T.float()
+        X[rows, ns + 2] = torch.log10(dt).float()
+        T_before, Y_before = T.clone(), Y.clone()
+        solver.chem_advance(cs, T, E, dt)
+        Y_after = cs[:ns] / cs[:ns].sum(0)
+        Tg[rows, :ns] = (Y_after - Y_before).T.float()
+        Tg[rows, ns] = (T - T_before).float()
+    return X, Tg
+
+
+def fit(X, T, steps=4000, batch=4096, lr=1e-3, seed=5, members=MEMBERS, log=None):
+    """Train an ensemble on device tensors; returns (model, scaling dict)."""
+    m = eu3d.Mlp()
+    m.init(N_IN, WIDTH, HIDDEN, N_OUT, members, max_batch=max(batch, 65536), seed=seed)
+    xm, xs = X.mean(0), X.std(0).clamp_min(1e-12)
+    tm, ts = T.mean(0), T.std(0).clamp_min(1e-12)
+    scaling = {"in_shift": xm.cpu().numpy(), "in_scale": (1 / xs).cpu().numpy(), "out_shift": tm.cpu().numpy(),
+               "out_scale": (1 / ts).cpu().numpy()}
+    m.set_scaling(scaling["in_shift"], scaling["in_scale"], scaling["out_shift"], scaling["out_scale"])
+    done = 0
+    chunk = 500
+    while done < steps:
+        k = min(chunk, steps - done)
+        # step decay of the learning rate over the run
+        frac = done / max(steps, 1)
+        cur = lr * (1.0 if frac < 0.5 else (0.3 if frac < 0.8 else 0.1))
+        losses = m.train(X, T, batch=batch, steps=k, lr=cur, seed=seed + done)
+        done += k
+        if log:
+            log(f"step {done}: batch loss per member {np.round(losses, 5).tolist()}")
+    return m, scaling
+
+
+def predict(model, X, members=MEMBERS):
+    import torch
+    out = torch.empty(members, X.shape[0], N_OUT, device="cuda")
+    model.predict(X, out)
+    return out
+
+
+def calibrate(model, scaling, X, T, target=2e-4, members=MEMBERS):
+    """Input box (trained range) and the spread threshold tau: the largest
+    spread whose accepted rows keep the mean species L1 error below target."""
+    import torch
+    out = predict(model, X, members)
+    mean = out.mean(0)
+    spread = (out.std(0, unbiased=False) * torch.tensor(scaling["out_scale"], device="cuda")).max(1).values
+    err = (mean[:, :N_SPECIES] - T[:, :N_SPECIES]).abs().sum(1)
+    order = torch.argsort(spread)
+    cum = torch.cumsum(err[order], 0) / torch.arange(1, err.numel() + 1, device="cuda")
+    ok = (cum <= target).nonzero()
+    idx = int(ok[-1]) if ok.numel() else 0
+    tau = float(spread[order[idx]])
+    accepted = float((spread <= tau).float().mean())
+    return {"tau": tau, "accepted_fraction": accepted, "box_lo": X.min(0).values.double().cpu().numpy(),
+            "box_hi": X.max(0).values.double().cpu().numpy(),
+            "l1_accepted": float(err[spread <= tau].mean()) if accepted > 0 else float("nan"),
+            "l1_all": float(err.mean())}
+
+
+def save(path, model, scaling, gate, meta=None):
+    np.savez(path, params=model.get_params(), shape=np.array([N_IN, WIDTH, HIDDEN, N_OUT, MEMBERS]),
+             **scaling, tau=gate["tau"], box_lo=gate["box_lo"], box_hi=gate["box_hi"],
+             meta=np.array(repr(meta or {})))
+
+
+def load(path=CHECKPOINT, device=0):
+    z = np.load(path)
+    n_in, width, hidden, n_out, members = (int(v) for v in z["shape"])
+    m = eu3d.Mlp(device)
+    m.init(n_in, width, hidden, n_out, members, max_batch=65536, seed=1)
+    m.set_scaling(z["in_shift"], z["in_scale"], z["out_shift"], z["out_scale"])
+    m.set_params(z["params"])
+    gate = {"tau": float(z["tau"]), "box_lo": z["box_lo"], "box_hi": z["box_hi"], "out_scale": z["out_scale"]}
+    return m, gate

@@ -179,6 +179,17 @@ eu_status eu_get_field(eu_handle *h, const char *name, double *host_out);
 /* Wait for all work queued on the handle. */
 eu_status eu_sync(eu_handle *h);
 
+/* The stiff chemistry of the timestep on independent cells at rest (no
+ * counterpart call in the reference; it runs the same kinetics as
+ * Euler::Trapezoid(1), src/Euler.cpp:462-493, cell by cell). All pointers are
+ * device memory; fields are planes of n values (cs: ns + 4 planes, Y: ns).
+ * eu_chem_states forms cs and E from (T, p, Y) as FieldInitial does;
+ * eu_chem_advance advances every cell by its own dt in place (nchem optional).
+ * Used to generate the learned model's training data. */
+eu_status eu_chem_states(eu_handle *h, long long n, const double *T, const double *p, const double *Y, double *cs,
+                         double *E);
+eu_status eu_chem_advance(eu_handle *h, long long n, double *cs, double *T, double *E, const double *dt, int *nchem);
+
 /* Device pointers and the stream of a handle, for callers that keep inputs
  * resident and time kernels themselves. */
 eu_status eu_device_info(const eu_handle *h, void **stream, size_t *device_bytes);
@@ -226,6 +237,24 @@ eu_status eu_mlp_train(eu_mlp *m, const float *X, const float *T, long long n, i
                        unsigned seed, float *mean_loss);
 /* Physical outputs of every member: out[member][row][n_out] (device fp32). */
 eu_status eu_mlp_predict(eu_mlp *m, const float *X, long long n, float *out);
+
+/* Learned chemistry in the timestep (cfg.chemistry == EU_CHEM_LEARNED). The
+ * model maps (T, log10 p, Y_0..Y_{ns-1}, log10 dt) to (dY_0..dY_{ns-1}, dT) and
+ * must have ns + 3 inputs and ns + 1 outputs. A cell is advanced by the
+ * ensemble mean when every input lies in [box_lo, box_hi] and the members'
+ * largest per-output standard deviation times out_scale is at most tau;
+ * otherwise the stiff kinetics advances it. Cells whose non-inert mass
+ * fraction is below frozen_y, or colder than frozen_T (> 0), skip chemistry. */
+typedef struct {
+    double tau;
+    double frozen_y;
+    double frozen_T;
+    const double *box_lo;    /* [ns + 3] */
+    const double *box_hi;    /* [ns + 3] */
+    const double *out_scale; /* [ns + 1] */
+} eu_learned_config;
+
+eu_status eu_set_learned(eu_handle *h, eu_mlp *model, const eu_learned_config *cfg);
 
 #ifdef __cplusplus
 }
