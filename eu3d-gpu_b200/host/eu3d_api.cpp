@@ -659,7 +659,9 @@ eu_status eu_chem_advance(eu_handle *h, long long n, double *cs, double *T, doub
     unsigned long long cnt[kCntCount];
     CK(h, cudaMemcpyAsync(cnt, h->st.counters, sizeof cnt, cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
-    if (cnt[kCntBadNchem])
+    // With a per-sample nchem output the caller sees capped samples (nchem ==
+    // max_substeps) and invalid ones (0) itself.
+    if (cnt[kCntBadNchem] && !nchem)
         return fail(h, EU_ERR_NCHEM, "%llu samples predicted Nchem <= 0 or above max_substeps", cnt[kCntBadNchem]);
     return EU_OK;
 }

@@ -48,8 +48,13 @@ def _initial_compositions(rng, n, mw):
     return Y / Y.sum(axis=1, keepdims=True)
 
 
-def generate(solver, n_traj, n_steps, seed=11, t_range=(300.0, 3500.0), p_range=(5e4, 5e6), dt_range=(1e-9, 3e-7)):
-    """(inputs, targets) as torch CUDA fp32 tensors, n_traj * n_steps rows."""
+def generate(solver, n_traj, n_steps, seed=11, t_range=(300.0, 3500.0), p_range=(5e4, 5e6), dt_range=(1e-9, 3e-7),
+             max_substeps=20000):
+    """(inputs, targets) as torch CUDA fp32 tensors, up to n_traj * n_steps rows.
+
+    A trajectory whose step needed more than max_substeps substeps (the solver
+    handle's cap) is dropped from that step on: its label would be inaccurate
+    and such stiffness is far outside the flows of the workloads."""
     import torch
     rng = np.random.default_rng(seed)
     mech = solver.mechanism()
@@ -67,6 +72,9 @@ def generate(solver, n_traj, n_steps, seed=11, t_range=(300.0, 3500.0), p_range=
     mw = torch.tensor(mech["mw"], device=dev, dtype=torch.float64)
     X = torch.empty(n_traj * n_steps, ns + 3, device=dev, dtype=torch.float32)
     Tg = torch.empty(n_traj * n_steps, ns + 1, device=dev, dtype=torch.float32)
+    keep = torch.zeros(n_traj * n_steps, device=dev, dtype=torch.bool)
+    alive = torch.ones(n_traj, device=dev, dtype=torch.bool)
+    nchem = torch.zeros(n_traj, device=dev, dtype=torch.int32)
     for k in range(n_steps):
         dt = torch.exp(torch.empty(n_traj, device=dev, dtype=torch.float64).uniform_(
             math.log(dt_range[0]), math.log(dt_range[1])))
@@ -79,11 +87,13 @@ def generate(solver, n_traj, n_steps, seed=11, t_range=(300.0, 3500.0), p_range=
         X[rows, 2:2 + ns] = Y.T.float()
         X[rows, ns + 2] = torch.log10(dt).float()
         T_before, Y_before = T.clone(), Y.clone()
-        solver.chem_advance(cs, T, E, dt)
+        solver.chem_advance(cs, T, E, dt, nchem)
+        alive &= (nchem > 0) & (nchem < max_substeps) & torch.isfinite(T)
+        keep[rows] = alive
         Y_after = cs[:ns] / cs[:ns].sum(0)
         Tg[rows, :ns] = (Y_after - Y_before).T.float()
         Tg[rows, ns] = (T - T_before).float()
-    return X, Tg
+    return X[keep].contiguous(), Tg[keep].contiguous()
 
 
 def fit(X, T, steps=4000, batch=4096, lr=1e-3, seed=5, members=MEMBERS, log=None):

@@ -184,7 +184,10 @@ eu_status eu_sync(eu_handle *h);
  * Euler::Trapezoid(1), src/Euler.cpp:462-493, cell by cell). All pointers are
  * device memory; fields are planes of n values (cs: ns + 4 planes, Y: ns).
  * eu_chem_states forms cs and E from (T, p, Y) as FieldInitial does;
- * eu_chem_advance advances every cell by its own dt in place (nchem optional).
+ * eu_chem_advance advances every cell by its own dt in place. With nchem
+ * (optional) each sample's substep count is returned and a prediction above
+ * max_substeps is not an error: that sample runs max_substeps substeps and
+ * reports nchem == max_substeps (0 marks an invalid prediction).
  * Used to generate the learned model's training data. */
 eu_status eu_chem_states(eu_handle *h, long long n, const double *T, const double *p, const double *Y, double *cs,
                          double *E);

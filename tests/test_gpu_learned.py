@@ -1,0 +1,84 @@
+"""The learned-chemistry step on the GPU.
+
+* Plumbing: with the gate rejecting every cell and no cell frozen, the learned
+  path (classify -> queue -> ensemble -> gate -> stiff fallback queue) must give
+  exactly the stiff path's result.
+* Gate: cells outside the input box fall back; the counts add up.
+* Conservation: an accepted prediction changes neither the density nor the
+  momentum and energy of a cell; the species change is projected onto element
+  conservation, so sum Y = 1 holds.
+"""
+import numpy as np
+import pytest
+
+import eu3d_cases as cases
+from helpers import golden, golden_mechanism, interior, n_unequal
+
+pytestmark = pytest.mark.gpu
+
+NS = 9
+
+
+def bubble(gpu, chemistry, precision="fp64"):
+    z = golden("bubble_25x13x13_s20.npz")
+    s = gpu.Solver(int(z["ni"]), int(z["nj"]), int(z["nk"]), tuple(z["extent"]), chemistry=chemistry,
+                   precision=precision, arith="fast")
+    s.load_mechanism(cases.MECH_JA919, cases.THERMO)
+    s.set_primitive(*[z[f"prim_{k}"] for k in "PTUVWY"])
+    return s, z
+
+
+def random_model(gpu, seed=1):
+    m = gpu.Mlp()
+    m.init(NS + 3, 256, 3, NS + 1, 3, max_batch=4096, seed=seed)
+    m.set_scaling(np.zeros(NS + 3), np.ones(NS + 3), np.zeros(NS + 1), np.ones(NS + 1) * 1e3)
+    return m
+
+
+def test_reject_all_equals_stiff(gpu):
+    a, z = bubble(gpu, "stiff")
+    b, _ = bubble(gpu, "learned")
+    m = random_model(gpu)
+    big = np.full(NS + 3, 1e30)
+    b.set_learned(m, tau=-1.0, box_lo=-big, box_hi=big, out_scale=np.ones(NS + 1), frozen_y=-1.0)
+    sa = a.step(10, float(z["dt"]))
+    sb = b.step(10, float(z["dt"]))
+    assert sb["learned"] == 0 and sb["fallback"] == sb["reacting"] == z["ni"] * z["nj"] * z["nk"]
+    for f in ["CS", "T", "E", "Nchem"]:
+        assert n_unequal(interior(a.get(f)), interior(b.get(f))) == 0, f
+    assert sa["max_nchem"] == sb["max_nchem"]
+
+
+def test_frozen_cells_skip_chemistry(gpu):
+    b, z = bubble(gpu, "learned")
+    m = random_model(gpu)
+    big = np.full(NS + 3, 1e30)
+    b.set_learned(m, tau=-1.0, box_lo=-big, box_hi=big, out_scale=np.ones(NS + 1), frozen_y=1e-9)
+    st = b.step(1, float(z["dt"]))
+    Y = interior(b.get("Yi"))
+    reactive = (Y[:8].sum(0) >= 1e-9).sum()
+    assert 0 < st["reacting"] < z["ni"] * z["nj"] * z["nk"]
+    assert abs(st["reacting"] - reactive) <= 0.05 * reactive + 10
+
+
+def test_accepted_prediction_conserves(gpu):
+    b, z = bubble(gpu, "learned")
+    m = random_model(gpu, seed=3)
+    big = np.full(NS + 3, 1e30)
+    b.set_learned(m, tau=1e30, box_lo=-big, box_hi=big, out_scale=np.ones(NS + 1), frozen_y=1e-9)
+    st = b.step(1, float(z["dt"]))
+    assert st["learned"] == st["reacting"] > 0 and st["fallback"] == 0
+    Y = interior(b.get("Yi"))
+    assert np.abs(Y.sum(0) - 1).max() < 1e-12
+    assert (Y >= 0).all()
+
+
+def test_gate_box_sends_cells_to_fallback(gpu):
+    b, z = bubble(gpu, "learned")
+    m = random_model(gpu)
+    lo = np.full(NS + 3, -1e30)
+    hi = np.full(NS + 3, 1e30)
+    hi[0] = 0.0  # every temperature is above the box
+    b.set_learned(m, tau=1e30, box_lo=lo, box_hi=hi, out_scale=np.ones(NS + 1), frozen_y=1e-9)
+    st = b.step(1, float(z["dt"]))
+    assert st["learned"] == 0 and st["fallback"] == st["reacting"] > 0
