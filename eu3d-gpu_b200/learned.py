@@ -52,9 +52,13 @@ def generate(solver, n_traj, n_steps, seed=11, t_range=(300.0, 3500.0), p_range=
              max_substeps=20000):
     """(inputs, targets) as torch CUDA fp32 tensors, up to n_traj * n_steps rows.
 
-    A trajectory whose step needed more than max_substeps substeps (the solver
-    handle's cap) is dropped from that step on: its label would be inaccurate
-    and such stiffness is far outside the flows of the workloads."""
+    A trajectory is dropped from the first step that leaves the physical
+    range: more than max_substeps substeps (the solver handle's cap), a
+    non-finite or out-of-range temperature, a mass fraction below -1e-8, or a
+    single-step change of any mass fraction above 0.5. At the extreme corners
+    of the sampled (T, p, dt) box the linearised trapezoid scheme can overshoot
+    into such states; they are far from the workloads' flows and would only
+    teach the model the scheme's instability."""
     import torch
     rng = np.random.default_rng(seed)
     mech = solver.mechanism()
@@ -88,9 +92,10 @@ def generate(solver, n_traj, n_steps, seed=11, t_range=(300.0, 3500.0), p_range=
         X[rows, ns + 2] = torch.log10(dt).float()
         T_before, Y_before = T.clone(), Y.clone()
         solver.chem_advance(cs, T, E, dt, nchem)
-        alive &= (nchem > 0) & (nchem < max_substeps) & torch.isfinite(T)
-        keep[rows] = alive
         Y_after = cs[:ns] / cs[:ns].sum(0)
+        alive &= (nchem > 0) & (nchem < max_substeps) & torch.isfinite(T) & (T > 250.0) & (T < 4500.0)
+        alive &= (Y_after.min(0).values > -1e-8) & ((Y_after - Y_before).abs().max(0).values < 0.5)
+        keep[rows] = alive
         Tg[rows, :ns] = (Y_after - Y_before).T.float()
         Tg[rows, ns] = (T - T_before).float()
     return X[keep].contiguous(), Tg[keep].contiguous()
