@@ -257,6 +257,16 @@ def cpu_baseline(dt):
                       f"workload at its node spacing, {steps} steps after 1 warm-up, single thread ({secs:.1f} s)"}
 
 
+def species_error(a, b, bc=2):
+    """Mean over cells of sum_s |Y_a - Y_b| (all cells; and cells holding any
+    reactive species)."""
+    ya = a[:, bc:-bc, bc:-bc, bc:-bc]
+    yb = b[:, bc:-bc, bc:-bc, bc:-bc]
+    l1 = np.abs(ya - yb).sum(axis=0)
+    reactive = yb[:8].sum(axis=0) > 1e-9
+    return float(l1.mean()), float(l1[reactive].mean()) if reactive.any() else 0.0
+
+
 def our_arm(args):
     import torch
     world, rank, local, dist = dist_setup(args)
@@ -266,17 +276,32 @@ def our_arm(args):
     ncell = grid[0] * grid[1] * grid[2]
     mech, prim, st0, dt = build_workload(grid)
     sd = state_dict(st0)
+    model = gate = None
+    if args.chem == "learned":
+        import learned
+        model, gate = learned.load(device=local)
 
-    def make_solver(profile):
-        s = eu3d.Solver(*grid, (EXTENT[0], EXTENT[1] * 1, EXTENT[2], EXTENT[3], EXTENT[4], EXTENT[5]),
-                        precision=args.precision, chemistry=args.chem, arith=args.arith, device=local,
+    def make_solver(chem, precision, arith, profile=False, state=sd):
+        s = eu3d.Solver(*grid, EXTENT, precision=precision, chemistry=chem, arith=arith, device=local,
                         profile=profile)
         s.set_mechanism(mech)
-        s.set_state(sd)
+        s.set_state(state)
+        if chem == "learned":
+            import learned
+            learned.attach(s, model, gate)
         return s
 
-    # -- device-resident throughput (value) -------------------------------------------------
-    s = make_solver(profile=False)
+    def timed(s):
+        s.step(args.warmup, dt)
+        barrier(dist, device)
+        torch.cuda.synchronize()
+        st = s.step(args.steps, dt)
+        torch.cuda.synchronize()
+        barrier(dist, device)
+        return st, reduce_max(dist, st["device_ms"], device)
+
+    # -- device-resident throughput of the configured path (value) --------------------------
+    s = make_solver(args.chem, args.precision, args.arith)
     s.step(args.warmup, dt)
     barrier(dist, device)
     torch.cuda.synchronize()
@@ -287,13 +312,28 @@ def our_arm(args):
     ms = reduce_max(dist, stats["device_ms"], device)
     value = ncell * args.steps * world / (ms / 1e3) / 1e6
     clocks = clk.summary()
+    y_fast = s.get("Yi")
+    s.close()
 
-    # -- per-kernel times (same stream, CUDA events around each kernel) -----------------------
-    sp = make_solver(profile=True)
+    # -- the plain FP64 stiff step on the same input (the comparison the metric names) -------
+    plain = None
+    if (args.chem, args.precision) != ("stiff", "fp64"):
+        sp_ = make_solver("stiff", "fp64", "fast")
+        pst, pms = timed(sp_)
+        y_ref = sp_.get("Yi")
+        sp_.close()
+        err_all, err_reactive = species_error(y_fast, y_ref)
+        plain = {"value": round(ncell * args.steps * world / (pms / 1e3) / 1e6, 3), "ms_per_step":
+                 round(pms / args.steps, 4), "speedup": round(value / (ncell * args.steps * world / (pms / 1e3) / 1e6), 3),
+                 "species_l1_vs_plain": err_all, "species_l1_vs_plain_reactive_cells": err_reactive,
+                 "after_steps": args.warmup + args.steps}
+
+    # -- per-kernel times (same stream, CUDA events around each kernel phase) -----------------
+    sp = make_solver(args.chem, args.precision, args.arith, profile=True)
     sp.step(args.warmup, dt)
     pst = sp.step(args.steps, dt)
     phase = pst["phase_ms"]
-    names = ["ghost_fill", "flux_update", "recover_kinetics"]
+    names = ["ghost_fill", "flux_update", "recover_kinetics" if args.chem != "learned" else "recover_learned_chem"]
     per_kernel = {n: round(phase[q] / args.steps, 4) for q, n in enumerate(names)}
     sp.close()
 
@@ -313,10 +353,7 @@ def our_arm(args):
         t = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)
         t.numpy()[...] = v
         pinned[k] = t.numpy()
-    se = eu3d.Solver(*grid, EXTENT, precision=args.precision, chemistry=args.chem, arith=args.arith,
-                     device=local)
-    se.set_mechanism(mech)
-    se.set_state(pinned)
+    se = make_solver(args.chem, args.precision, args.arith, state=pinned)
     se.step(args.warmup, dt)
     barrier(dist, device)
     torch.cuda.synchronize()
@@ -347,8 +384,10 @@ def our_arm(args):
                            "grid": list(grid), "dt": dt, "precision": args.precision, "chemistry": args.chem,
                            "arith": args.arith, "parallelism": f"replicas x{world}",
                            "l2": f"inputs larger than L2: {sd['CS'].nbytes * 3 // 2**20} MiB state > 126 MiB"},
+                "plain_fp64": plain,
                 "roofline": roofline, "kernels_ms_per_step": per_kernel,
-                "max_nchem": stats["max_nchem"], "substeps_per_cell": stats["sum_nchem"] / ncell,
+                "max_nchem": stats["max_nchem"], "reacting_cells": stats["reacting"],
+                "learned_cells": stats["learned"], "fallback_cells": stats["fallback"],
                 "clocks": clocks,
                 "e2e": {"value": round(e2e_value, 3), "unit": "Mcell-steps/s",
                         "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
@@ -366,12 +405,18 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
-    ap.add_argument("--chem", choices=["stiff", "frozen"], default="stiff")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--chem", choices=["stiff", "frozen", "learned"], default="learned")
     ap.add_argument("--arith", choices=["strict", "fast"], default="fast")
     ap.add_argument("--grid", type=int, nargs=3, default=list(GRID))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.chem == "learned":
+        sys.path.insert(0, os.path.join(ROOT, "eu3d-gpu_b200"))
+        import learned
+        if not os.path.exists(learned.CHECKPOINT):
+            print("no trained learned-chemistry checkpoint; measuring the stiff kinetics", file=sys.stderr)
+            args.chem = "stiff"
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":

@@ -388,12 +388,15 @@ __global__ void __launch_bounds__(128) k_recover_classify(const __grid_constant_
         load_cell<NS>(st, n3, c, cell);
         recover_state<NS>(m, cell);
         store_cell<NS>(m, st, n3, c, cell);
-        double reactive = 0;
+        double reactive = 0, radical = 0;
 #pragma unroll
-        for (int s = 0; s < NS; ++s)
+        for (int s = 0; s < NS; ++s) {
             if (!lp.inert[s])
                 reactive += cell.Y[s];
-        active = reactive >= lp.frozen_y && cell.T >= lp.frozen_T;
+            if (lp.radical[s])
+                radical += cell.Y[s];
+        }
+        active = reactive >= lp.frozen_y && !(cell.T < lp.frozen_T && radical < lp.frozen_radical);
         st.nchem[c] = 0;
     }
     const unsigned mask = __ballot_sync(0xffffffffu, active);
@@ -465,8 +468,9 @@ __global__ void __launch_bounds__(128) k_learned_apply(const __grid_constant__ D
             }
             const double mu = s1 / lp.members;
             const double var = fmax(s2 / lp.members - mu * mu, 0.0);
-            mean[o] = mu;
+            // spread and mean in the model's output space, the change back in physical units
             spread = fmax(spread, sqrt(var) * lp.out_scale[o]);
+            mean[o] = lp.out_eps[o] > 0 ? lp.out_eps[o] * sinh(mu) : mu;
         }
         ok = ok && spread <= lp.tau && isfinite(spread);
         if (ok) {

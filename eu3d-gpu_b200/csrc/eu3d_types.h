@@ -73,12 +73,15 @@ struct LearnedParams {
     int *counts;           // [0] learned queue length, [1] fallback queue length
     int members;
     double frozen_y;       // a cell whose non-inert mass fraction is below this is frozen
-    double frozen_T;       // a cell colder than this is frozen (0 disables)
+    double frozen_T;       // a cell colder than this whose radical pool is below frozen_radical is frozen
+    double frozen_radical;
     double tau;            // largest accepted ensemble spread, in output-scale units
     double box_lo[kMaxS + 3], box_hi[kMaxS + 3]; // accepted input ranges
     double out_scale[kMaxS + 1];
+    double out_eps[kMaxS + 1]; // model output o is asinh(change / eps) when eps > 0
     double proj[kMaxS][kMaxS]; // element-conservation projector
     int inert[kMaxS];
+    int radical[kMaxS];
 };
 
 } // namespace eu3d

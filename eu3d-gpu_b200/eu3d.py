@@ -46,8 +46,8 @@ class MechanismC(ctypes.Structure):
 
 
 class LearnedConfig(ctypes.Structure):
-    _fields_ = [("tau", _D), ("frozen_y", _D), ("frozen_T", _D), ("box_lo", _P), ("box_hi", _P),
-                ("out_scale", _P)]
+    _fields_ = [("tau", _D), ("frozen_y", _D), ("frozen_T", _D), ("frozen_radical", _D), ("box_lo", _P),
+                ("box_hi", _P), ("out_scale", _P), ("out_eps", _P)]
 
 
 class StepStats(ctypes.Structure):
@@ -282,10 +282,13 @@ class Solver:
         self._check(library().eu_chem_advance(self.h, n, cs.data_ptr(), T.data_ptr(), E.data_ptr(), dt.data_ptr(),
                                               None if nchem is None else nchem.data_ptr()), "chem_advance")
 
-    def set_learned(self, model, tau, box_lo, box_hi, out_scale, frozen_y=1e-9, frozen_T=0.0):
-        self._learned_keep = [np.ascontiguousarray(v, dtype=np.float64) for v in (box_lo, box_hi, out_scale)]
-        cfg = LearnedConfig(float(tau), float(frozen_y), float(frozen_T),
-                            *[v.ctypes.data for v in self._learned_keep])
+    def set_learned(self, model, tau, box_lo, box_hi, out_scale, frozen_y=1e-9, frozen_T=0.0,
+                    frozen_radical=1e-9, out_eps=None):
+        keep = [np.ascontiguousarray(v, dtype=np.float64) for v in (box_lo, box_hi, out_scale)]
+        keep.append(None if out_eps is None else np.ascontiguousarray(out_eps, dtype=np.float64))
+        self._learned_keep = keep
+        cfg = LearnedConfig(float(tau), float(frozen_y), float(frozen_T), float(frozen_radical),
+                            *[None if v is None else v.ctypes.data for v in keep])
         self._model = model
         self._check(library().eu_set_learned(self.h, model.h, ctypes.byref(cfg)), "set_learned")
 

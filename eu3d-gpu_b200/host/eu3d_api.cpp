@@ -698,11 +698,21 @@ eu_status eu_set_learned(eu_handle *h, eu_mlp *model, const eu_learned_config *l
     lp.tau = lc->tau;
     lp.frozen_y = lc->frozen_y;
     lp.frozen_T = lc->frozen_T;
+    lp.frozen_radical = lc->frozen_radical;
     for (int a = 0; a < ns + 3; ++a) {
         lp.box_lo[a] = lc->box_lo[a];
         lp.box_hi[a] = lc->box_hi[a];
     }
-    for (int o = 0; o < ns + 1; ++o) lp.out_scale[o] = lc->out_scale[o];
+    for (int o = 0; o < ns + 1; ++o) {
+        lp.out_scale[o] = lc->out_scale[o];
+        lp.out_eps[o] = lc->out_eps ? lc->out_eps[o] : 0.0;
+    }
+    for (int s = 0; s < ns; ++s) {
+        std::string up;
+        if (s < (int)h->mech.species.size())
+            for (char ch : h->mech.species[s]) up += char(std::toupper((unsigned char)ch));
+        lp.radical[s] = (up == "H" || up == "O" || up == "OH" || up == "HO2" || up == "H2O2") ? 1 : 0;
+    }
     element_projector(h->mech, lp.proj);
     for (int s = 0; s < ns; ++s) {
         bool used = false;

@@ -28,6 +28,13 @@ CHECKPOINT = os.path.join(HERE, "data", "chem_mlp_ja919.npz")
 
 N_SPECIES = 9
 N_IN, N_OUT = N_SPECIES + 3, N_SPECIES + 1
+# The model predicts asinh(change / eps): linear below eps, logarithmic above,
+# so a 1e-9 and a 0.1 change get the same relative precision.
+OUT_EPS = np.array([1e-8] * N_SPECIES + [1e-3])
+# Cells colder than FROZEN_T with a radical pool below FROZEN_RADICAL skip the
+# kinetics: along the stiff integrator's own trajectories the largest one-step
+# change of any mass fraction below 800 K was 1.5e-10 (700-800 K band).
+FROZEN_T, FROZEN_RADICAL, FROZEN_Y = 800.0, 1e-9, 1e-9
 WIDTH, HIDDEN, MEMBERS = 256, 3, 3
 S_O2, S_H2, S_N2 = cases.S_O2, cases.S_H2, cases.S_N2
 
@@ -101,8 +108,20 @@ def generate(solver, n_traj, n_steps, seed=11, t_range=(300.0, 3500.0), p_range=
     return X[keep].contiguous(), Tg[keep].contiguous()
 
 
+def to_model_space(T):
+    import torch
+    eps = torch.tensor(OUT_EPS, device=T.device, dtype=T.dtype)
+    return torch.asinh(T / eps)
+
+
+def from_model_space(Tt):
+    import torch
+    eps = torch.tensor(OUT_EPS, device=Tt.device, dtype=Tt.dtype)
+    return eps * torch.sinh(Tt)
+
+
 def fit(X, T, steps=4000, batch=4096, lr=1e-3, seed=5, members=MEMBERS, log=None):
-    """Train an ensemble on device tensors; returns (model, scaling dict)."""
+    """Train an ensemble on device tensors (T in model space); returns (model, scaling dict)."""
     m = eu3d.Mlp()
     m.init(N_IN, WIDTH, HIDDEN, N_OUT, members, max_batch=max(batch, 65536), seed=seed)
     xm, xs = X.mean(0), X.std(0).clamp_min(1e-12)
@@ -114,9 +133,9 @@ def fit(X, T, steps=4000, batch=4096, lr=1e-3, seed=5, members=MEMBERS, log=None
     chunk = 500
     while done < steps:
         k = min(chunk, steps - done)
-        # step decay of the learning rate over the run
-        frac = done / max(steps, 1)
-        cur = lr * (1.0 if frac < 0.5 else (0.3 if frac < 0.8 else 0.1))
+        # cosine decay of the learning rate over the run (to 2 % of lr)
+        frac = (done + 0.5 * k) / max(steps, 1)
+        cur = lr * (0.02 + 0.98 * 0.5 * (1 + math.cos(math.pi * frac)))
         losses = m.train(X, T, batch=batch, steps=k, lr=cur, seed=seed + done)
         done += k
         if log:
@@ -133,10 +152,12 @@ def predict(model, X, members=MEMBERS):
 
 def calibrate(model, scaling, X, T, target=2e-4, members=MEMBERS):
     """Input box (trained range) and the spread threshold tau: the largest
-    spread whose accepted rows keep the mean species L1 error below target."""
+    spread whose accepted rows keep the mean species L1 error (physical
+    units, T the physical change) below target. The mean and spread are formed
+    as the step kernel forms them: in model space, the mean mapped back."""
     import torch
     out = predict(model, X, members)
-    mean = out.mean(0)
+    mean = from_model_space(out.mean(0))
     spread = (out.std(0, unbiased=False) * torch.tensor(scaling["out_scale"], device="cuda")).max(1).values
     err = (mean[:, :N_SPECIES] - T[:, :N_SPECIES]).abs().sum(1)
     order = torch.argsort(spread)
@@ -153,8 +174,8 @@ def calibrate(model, scaling, X, T, target=2e-4, members=MEMBERS):
 
 def save(path, model, scaling, gate, meta=None):
     np.savez(path, params=model.get_params(), shape=np.array([N_IN, WIDTH, HIDDEN, N_OUT, MEMBERS]),
-             **scaling, tau=gate["tau"], box_lo=gate["box_lo"], box_hi=gate["box_hi"],
-             meta=np.array(repr(meta or {})))
+             **scaling, tau=gate["tau"], box_lo=gate["box_lo"], box_hi=gate["box_hi"], out_eps=OUT_EPS,
+             frozen=np.array([FROZEN_Y, FROZEN_T, FROZEN_RADICAL]), meta=np.array(repr(meta or {})))
 
 
 def load(path=CHECKPOINT, device=0):
@@ -164,5 +185,15 @@ def load(path=CHECKPOINT, device=0):
     m.init(n_in, width, hidden, n_out, members, max_batch=65536, seed=1)
     m.set_scaling(z["in_shift"], z["in_scale"], z["out_shift"], z["out_scale"])
     m.set_params(z["params"])
-    gate = {"tau": float(z["tau"]), "box_lo": z["box_lo"], "box_hi": z["box_hi"], "out_scale": z["out_scale"]}
+    gate = {"tau": float(z["tau"]), "box_lo": z["box_lo"], "box_hi": z["box_hi"], "out_scale": z["out_scale"],
+            "out_eps": z["out_eps"] if "out_eps" in z.files else None}
+    fz = z["frozen"] if "frozen" in z.files else np.array([FROZEN_Y, FROZEN_T, FROZEN_RADICAL])
+    gate.update(frozen_y=float(fz[0]), frozen_T=float(fz[1]), frozen_radical=float(fz[2]))
     return m, gate
+
+
+def attach(solver, model, gate):
+    """Install a loaded model and its gate on a solver handle."""
+    solver.set_learned(model, gate["tau"], gate["box_lo"], gate["box_hi"], gate["out_scale"],
+                       frozen_y=gate["frozen_y"], frozen_T=gate["frozen_T"], frozen_radical=gate["frozen_radical"],
+                       out_eps=gate["out_eps"])

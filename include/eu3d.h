@@ -247,14 +247,18 @@ eu_status eu_mlp_predict(eu_mlp *m, const float *X, long long n, float *out);
  * ensemble mean when every input lies in [box_lo, box_hi] and the members'
  * largest per-output standard deviation times out_scale is at most tau;
  * otherwise the stiff kinetics advances it. Cells whose non-inert mass
- * fraction is below frozen_y, or colder than frozen_T (> 0), skip chemistry. */
+ * fraction is below frozen_y, or that are colder than frozen_T with a radical
+ * pool (H, O, OH, HO2, H2O2 by species name) below frozen_radical, skip
+ * chemistry. When out_eps[o] > 0 the model's output o is asinh(change/out_eps[o]). */
 typedef struct {
     double tau;
     double frozen_y;
     double frozen_T;
+    double frozen_radical;
     const double *box_lo;    /* [ns + 3] */
     const double *box_hi;    /* [ns + 3] */
     const double *out_scale; /* [ns + 1] */
+    const double *out_eps;   /* [ns + 1], NULL: linear outputs */
 } eu_learned_config;
 
 eu_status eu_set_learned(eu_handle *h, eu_mlp *model, const eu_learned_config *cfg);
