@@ -108,6 +108,8 @@ def library():
         lib.eu_mlp_loss_grad.argtypes = [_P, _I, _P, _P, _I, _P, _P]
         lib.eu_mlp_train.argtypes = [_P, _P, _P, ctypes.c_longlong, _I, _I, ctypes.c_float, ctypes.c_uint, _P]
         lib.eu_mlp_predict.argtypes = [_P, _P, ctypes.c_longlong, _P]
+        lib.eu_mlp_predict_noalloc.argtypes = [_P, _P, ctypes.c_longlong, _P]
+        lib.eu_mlp_predict_noalloc.restype = _I
         for fn in ("eu_mlp_create", "eu_mlp_destroy", "eu_mlp_gemm", "eu_mlp_init", "eu_mlp_set_scaling",
                    "eu_mlp_get_params", "eu_mlp_set_params", "eu_mlp_loss_grad", "eu_mlp_train", "eu_mlp_predict"):
             getattr(lib, fn).restype = _I
@@ -362,6 +364,14 @@ class Mlp:
     def predict(self, X, out):
         """out: torch CUDA fp32 tensor (members x n x n_out)."""
         self._check(library().eu_mlp_predict(self.h, X.data_ptr(), X.shape[0], out.data_ptr()), "predict")
+
+    def predict_noalloc(self, X, out):
+        """predict() with its scratch in the library's fixed device array
+        instead of allocated buffers (eu_mlp_predict_noalloc): for callers that
+        cannot allocate device memory while they run. At most ~15k rows for the
+        chemistry model's shape; overlapping calls on one device race."""
+        self._check(library().eu_mlp_predict_noalloc(self.h, X.data_ptr(), X.shape[0], out.data_ptr()),
+                    "predict_noalloc")
 
     def gemm(self, A, B, bias=None, act=0, Cf=None, Cb=None, Cpre=None, stream=None):
         """C = act(A @ B.T + bias) on torch CUDA tensors (A, B bf16, row-major)."""

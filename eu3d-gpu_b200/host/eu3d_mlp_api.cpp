@@ -202,6 +202,26 @@ bool mlp_shape(const eu_mlp *m, int *n_in, int *n_out, int *members)
     return true;
 }
 
+bool mlp_view(const eu_mlp *m, MlpView *v)
+{
+    if (!m || !m->ready || !v)
+        return false;
+    *v = MlpView{m->device, m->n_in,  m->width,    m->hidden,   m->n_out,    m->members,  m->in_pad,
+                 m->out_pad, m->stream, m->in_shift, m->in_scale, m->out_shift, m->out_scale};
+    return true;
+}
+
+bool mlp_layer_view(const eu_mlp *m, int member, int layer, MlpLayerView *v)
+{
+    if (!m || !m->ready || !v || member < 0 || member >= m->members || layer < 0 || layer > m->hidden)
+        return false;
+    const Layer &L = m->net[member][layer];
+    *v = MlpLayerView{L.in_pad, L.out_pad, L.Wb, L.b};
+    return true;
+}
+
+eu_status mlp_fail(eu_mlp *m, eu_status s, const char *msg) { return mfail(m, s, "%s", msg); }
+
 eu_status mlp_predict_stream(eu_mlp *m, const float *X, long long n, float *out, cudaStream_t s)
 {
     for (long long r0 = 0; r0 < n; r0 += m->max_batch) {

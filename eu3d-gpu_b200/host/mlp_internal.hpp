@@ -11,4 +11,21 @@ bool mlp_shape(const eu_mlp *m, int *n_in, int *n_out, int *members);
 // Physical outputs of every member for n fp32 input rows, on `stream`:
 // out[member][row][n_out]. Uses the model's scratch buffers.
 eu_status mlp_predict_stream(eu_mlp *m, const float *X, long long n, float *out, cudaStream_t stream);
+
+// Read-only views of an initialised model, for inference with scratch that
+// the caller of these views provides (eu3d_noalloc.cu).
+struct MlpView {
+    int device, n_in, width, hidden, n_out, members, in_pad, out_pad;
+    cudaStream_t stream;
+    const float *in_shift, *in_scale, *out_shift, *out_scale;
+};
+struct MlpLayerView {
+    int in_pad, out_pad;
+    const void *Wb; // bf16 [out_pad x in_pad]
+    const float *b; // [out_pad]
+};
+bool mlp_view(const eu_mlp *m, MlpView *v);
+bool mlp_layer_view(const eu_mlp *m, int member, int layer, MlpLayerView *v);
+// Records msg as the model's last error and returns s.
+eu_status mlp_fail(eu_mlp *m, eu_status s, const char *msg);
 } // namespace eu3d

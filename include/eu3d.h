@@ -241,6 +241,26 @@ eu_status eu_mlp_train(eu_mlp *m, const float *X, const float *T, long long n, i
 /* Physical outputs of every member: out[member][row][n_out] (device fp32). */
 eu_status eu_mlp_predict(eu_mlp *m, const float *X, long long n, float *out);
 
+/* eu_mlp_predict without any device allocation, for callers that cannot call
+ * cudaMalloc while they run: a solver that gives all free device memory to its
+ * own pool after start-up (where a library's allocation fails or fragments
+ * it), or a time loop that cannot take the device-wide synchronisation of
+ * cudaMalloc/cudaFree. It has no counterpart in the reference.
+ * Same inputs, outputs and results as eu_mlp_predict. The scratch (packed
+ * inputs, hidden activations, outputs before unscaling, an error flag) is one
+ * fixed array of EU_MLP_NOALLOC_SCRATCH_BYTES in the library's device memory,
+ * held on every GPU that loads the library until the process exits; n may be
+ * at most (EU_MLP_NOALLOC_SCRATCH_BYTES - 1024) / (2 in_pad + 4 width + 4
+ * out_pad) rows (in_pad, out_pad: n_in, n_out rounded up to 16), 14978 for
+ * the 12 -> 256 x 3 -> 10 chemistry model; more is EU_ERR_INVALID_ARGUMENT.
+ * The first call on a device looks up the array's device address (once per
+ * device); make that first call before any stream capture. All calls share
+ * the one array: calls that overlap on the GPU (other threads, other streams
+ * of the same device) race and corrupt each other's results. Returns after
+ * the model's stream has finished the work. */
+#define EU_MLP_NOALLOC_SCRATCH_BYTES (16u << 20)
+eu_status eu_mlp_predict_noalloc(eu_mlp *m, const float *X, long long n, float *out);
+
 /* Learned chemistry in the timestep (cfg.chemistry == EU_CHEM_LEARNED). The
  * model maps (T, log10 p, Y_0..Y_{ns-1}, log10 dt) to (dY_0..dY_{ns-1}, dT) and
  * must have ns + 3 inputs and ns + 1 outputs. A cell is advanced by the
