@@ -204,7 +204,9 @@ def reference_sample(nproc, steps, warmup, dt, box=(32, 32, 32)):
 
 
 def reference_arm(args):
-    world, rank, local, dist = dist_setup(args)
+    # Rank 0 alone times the host-side reference; the other ranks exit without
+    # work (no process group: the arm has no collective step).
+    world, rank = env_int("WORLD_SIZE", 1), env_int("RANK", 0)
     if rank != 0:
         return 0
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -265,6 +267,47 @@ def species_error(a, b, bc=2):
     l1 = np.abs(ya - yb).sum(axis=0)
     reactive = yb[:8].sum(axis=0) > 1e-9
     return float(l1.mean()), float(l1[reactive].mean()) if reactive.any() else 0.0
+
+
+def reacting_block(args, model, gate, local, dt=2e-8):
+    """The kinetics-dominated case: a quiescent 48 x 32 x 32 block of hot
+    2H2+O2/N2 (eu3d_cases.hot_reacting_block, 1300-2600 K, 0.1-1 MPa) at
+    dt = 2e-8 s, stepped by the plain FP64 stiff path and by the learned +
+    mixed path from the same state. Reports both throughputs, the substeps of
+    the last step, the learned/fallback split and the species L1 difference
+    (mean over cells of sum_s |dY_s|) after warm-up + steps. The block ignites:
+    the stiff path's Nchem reaches ~100 in the igniting cells. (At the
+    shock-bubble's dt of ~1e-7 s the reference's own scheme fails on this
+    gas: its Nchem prediction, which ignores species below Y = 1e-6, lets the
+    first radicals overshoot into a non-positive Nchem or non-finite state.)"""
+    import torch
+    import learned
+    grid = (48, 32, 32)
+    ext = (0.0, 0.012, 0.0, 0.008, 0.0, 0.008)
+    mech = eu3d.parse_mechanism(cases.MECH_JA919, cases.THERMO)
+    prim = cases.hot_reacting_block(grid[0] + 4, grid[1] + 4, grid[2] + 4, mech["mw"], mech["ns"])
+    ncell = grid[0] * grid[1] * grid[2]
+    out, ys = {}, {}
+    for name, chem, prec in (("stiff_fp64", "stiff", "fp64"), ("learned_mixed", "learned", "mixed")):
+        s = eu3d.Solver(*grid, ext, precision=prec, chemistry=chem, arith="fast", device=local)
+        s.set_mechanism(mech)
+        s.set_primitive(*prim)
+        if chem == "learned":
+            learned.attach(s, model, gate)
+        s.step(args.warmup, dt)
+        torch.cuda.synchronize()
+        st = s.step(args.steps, dt)
+        torch.cuda.synchronize()
+        out[name] = {"value": round(ncell * args.steps / (st["device_ms"] / 1e3) / 1e6, 3),
+                     "ms_per_step": round(st["device_ms"] / args.steps, 4), "substeps_last_step": st["sum_nchem"],
+                     "max_nchem": st["max_nchem"], "learned_cells": st["learned"], "fallback_cells": st["fallback"]}
+        ys[name] = s.get("Yi")
+        s.close()
+    l1 = np.abs(ys["learned_mixed"] - ys["stiff_fp64"])[:, 2:-2, 2:-2, 2:-2].sum(axis=0)
+    return {"grid": list(grid), "cells": ncell, **out,
+            "speedup": round(out["learned_mixed"]["value"] / out["stiff_fp64"]["value"], 3),
+            "species_l1_mean": float(l1.mean()), "species_l1_max": float(l1.max()),
+            "dt": dt, "after_steps": args.warmup + args.steps}
 
 
 def our_arm(args):
@@ -328,6 +371,9 @@ def our_arm(args):
                  "species_l1_vs_plain": err_all, "species_l1_vs_plain_reactive_cells": err_reactive,
                  "after_steps": args.warmup + args.steps}
 
+    # -- reacting gas: the chemistry phase the learned model replaces ---------------------------
+    block = reacting_block(args, model, gate, local) if args.chem == "learned" else None
+
     # -- per-kernel times (same stream, CUDA events around each kernel phase) -----------------
     sp = make_solver(args.chem, args.precision, args.arith, profile=True)
     sp.step(args.warmup, dt)
@@ -385,6 +431,7 @@ def our_arm(args):
                            "arith": args.arith, "parallelism": f"replicas x{world}",
                            "l2": f"inputs larger than L2: {sd['CS'].nbytes * 3 // 2**20} MiB state > 126 MiB"},
                 "plain_fp64": plain,
+                "reacting_block": block,
                 "roofline": roofline, "kernels_ms_per_step": per_kernel,
                 "max_nchem": stats["max_nchem"], "reacting_cells": stats["reacting"],
                 "learned_cells": stats["learned"], "fallback_cells": stats["fallback"],

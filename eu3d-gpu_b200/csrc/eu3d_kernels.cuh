@@ -218,9 +218,192 @@ __global__ void __launch_bounds__(kFluxTK *kFluxTJ, 1)
     }
 }
 
+// Plane-tiled flux divergence and update: the same faces, arithmetic and RHS
+// order as k_flux_update (bitwise the same result), with every primitive read
+// from HBM once per plane instead of once per stencil point.
+//
+// A block owns a kTileJ x kTileK tile of (j, k) columns and marches along x.
+// Each thread keeps its column's x-stencil (planes i-1 .. i+2 of every
+// primitive) in registers and loads plane i+3 one node ahead. Plane i of the
+// tile plus a two-node halo in j and k is staged in shared memory, from which
+// the y- and z-face fluxes are formed. Face indices: sG[q][r] is the y face
+// below tile row r (r = kTileJ: above the last row), sQ[q][r][c] the z face
+// left of column c. Partial tiles: the faces of the valid rows/columns are
+// formed, including the one past the last valid row/column.
+constexpr int kTileK = 32, kTileJ = 8, kTileCI = 16;
+constexpr int kTileRows = kTileJ + 4, kTileCols = kTileK + 4;
+constexpr int kTileHalo = 4 * kTileCols + 4 * kTileJ; // two rows above, two below, two columns each side
+
+template <int NS, typename R>
+constexpr size_t tiled_flux_smem_bytes()
+{
+    return sizeof(R) * ((7 + NS) * kTileRows * kTileCols +
+                        (NS + 4) * ((kTileJ + 1) * kTileK + kTileJ * (kTileK + 1)));
+}
+
+// Face flux from four consecutive stencil points of the staged plane tile,
+// starting at (r, c) and stepping (DR, DC).
+template <int NS, int DIR, int DR, int DC, typename R, bool kStrict>
+__device__ __forceinline__ void tile_face_flux(const R (*sP)[kTileRows][kTileCols], int r, int c, R (&F)[NS + 4])
+{
+    R L[7], Rt[7], YL[NS], YR[NS];
+#pragma unroll
+    for (int f = 0; f < 7; ++f)
+        muscl<R, kStrict>(sP[f][r][c], sP[f][r + DR][c + DC], sP[f][r + 2 * DR][c + 2 * DC],
+                          sP[f][r + 3 * DR][c + 3 * DC], L[f], Rt[f]);
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+        muscl<R, kStrict>(sP[kY0 + s][r][c], sP[kY0 + s][r + DR][c + DC], sP[kY0 + s][r + 2 * DR][c + 2 * DC],
+                          sP[kY0 + s][r + 3 * DR][c + 3 * DC], YL[s], YR[s]);
+    ausm<NS, DIR, R, kStrict, R>(L, Rt, YL, YR, F);
+}
+
+template <int NS, typename R, bool kStrict>
+__device__ __forceinline__ void window_face_flux(const R (&w)[4][7 + NS], R (&F)[NS + 4])
+{
+    R L[7], Rt[7], YL[NS], YR[NS];
+#pragma unroll
+    for (int f = 0; f < 7; ++f) muscl<R, kStrict>(w[0][f], w[1][f], w[2][f], w[3][f], L[f], Rt[f]);
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+        muscl<R, kStrict>(w[0][kY0 + s], w[1][kY0 + s], w[2][kY0 + s], w[3][kY0 + s], YL[s], YR[s]);
+    ausm<NS, 0, R, kStrict, R>(L, Rt, YL, YR, F);
+}
+
+template <int NS, typename R, bool kStrict>
+__global__ void __launch_bounds__(kTileK *kTileJ, 2)
+    k_flux_update_tiled(const DevGrid g, const DevState st, const R *__restrict__ prim, const double *__restrict__ dt_dev)
+{
+    constexpr int NP = 7 + NS, NV = NS + 4;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R(*sP)[kTileRows][kTileCols] = reinterpret_cast<R(*)[kTileRows][kTileCols]>(smem_raw);
+    unsigned char *flux_raw = smem_raw + sizeof(R) * NP * kTileRows * kTileCols;
+    R(*sG)[kTileJ + 1][kTileK] = reinterpret_cast<R(*)[kTileJ + 1][kTileK]>(flux_raw);
+    R(*sQ)[kTileJ][kTileK + 1] =
+        reinterpret_cast<R(*)[kTileJ][kTileK + 1]>(flux_raw + sizeof(R) * NV * (kTileJ + 1) * kTileK);
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTileK + tx;
+    const int k0 = blockIdx.x * kTileK, j0 = blockIdx.y * kTileJ;
+    const int k = g.bc + k0 + tx, j = g.bc + j0 + ty;
+    const int rows = min(kTileJ, g.nj - j0), cols = min(kTileK, g.nk - k0); // valid rows / columns
+    const bool valid = ty < rows && tx < cols;
+    const bool resident = j < g.ny && k < g.nz; // inside the haloed arrays: staged for the neighbours
+    // faces this thread forms (see above)
+    const bool yface = tx < cols && ty <= rows;
+    const bool ytop = ty == 0 && tx < cols && rows == kTileJ;
+    const bool zface = ty < rows && tx <= cols;
+    const int zrow = tx; // lanes 0..kTileJ-1 of warp 1: the z face right of the last column
+    const bool zright = ty == 1 && zrow < rows && cols == kTileK;
+
+    // the halo cell this thread stages, if any
+    int hr = -1, hc = 0;
+    if (tid < 4 * kTileCols) {
+        const int band = tid / kTileCols;
+        hr = band < 2 ? band : kTileJ + band;
+        hc = tid % kTileCols;
+    } else if (tid < kTileHalo) {
+        const int h = tid - 4 * kTileCols, side = h % 4;
+        hr = 2 + h / 4;
+        hc = side < 2 ? side : kTileK + side;
+    }
+    const int hj = g.bc + j0 - 2 + hr, hk = g.bc + k0 - 2 + hc;
+    const bool halo = hr >= 0 && hj < g.ny && hk < g.nz;
+
+    const long long n3 = g.n3, sx = (long long)g.ny * g.nz;
+    const double dt = *dt_dev;
+    const double cy = valid ? dt / (g.y[j] - g.y[j - 1]) : 0.0;
+    const double cz = valid ? dt / (g.z[k] - g.z[k - 1]) : 0.0;
+    const int i_begin = g.bc + blockIdx.z * kTileCI;
+    const int i_end = min(i_begin + kTileCI, g.bc + g.ni);
+    const long long col = resident ? cell_index(g, 0, j, k) : 0;
+    const long long hcol = halo ? cell_index(g, 0, hj, hk) : 0;
+
+    R w[4][NP];
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int f = 0; f < NP; ++f) w[p][f] = resident ? __ldg(prim + f * n3 + col + (i_begin - 2 + p) * sx) : R(0);
+    R Fm[NV];
+    if (valid)
+        window_face_flux<NS, R, kStrict>(w, Fm);
+#pragma unroll
+    for (int f = 0; f < NP; ++f) {
+        w[0][f] = w[1][f];
+        w[1][f] = w[2][f];
+        w[2][f] = w[3][f];
+        w[3][f] = resident ? __ldg(prim + f * n3 + col + (i_begin + 2) * sx) : R(0);
+    }
+
+    for (int i = i_begin; i < i_end; ++i) {
+        // window: planes i-1, i, i+1, i+2; stage plane i of the tile
+        if (resident) {
+#pragma unroll
+            for (int f = 0; f < NP; ++f) sP[f][ty + 2][tx + 2] = w[1][f];
+        }
+        if (halo) {
+#pragma unroll
+            for (int f = 0; f < NP; ++f) sP[f][hr][hc] = __ldg(prim + f * n3 + hcol + i * sx);
+        }
+        R next[NP];
+        const bool more = resident && i + 1 < i_end;
+#pragma unroll
+        for (int f = 0; f < NP; ++f) next[f] = more ? __ldg(prim + f * n3 + col + (i + 3) * sx) : R(0);
+        __syncthreads();
+        R Fp[NV];
+        if (valid)
+            window_face_flux<NS, R, kStrict>(w, Fp);
+        if (yface) {
+            R G[NV];
+            tile_face_flux<NS, 1, 1, 0, R, kStrict>(sP, ty, tx + 2, G);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) sG[q][ty][tx] = G[q];
+        }
+        if (ytop) {
+            R G[NV];
+            tile_face_flux<NS, 1, 1, 0, R, kStrict>(sP, kTileJ, tx + 2, G);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) sG[q][kTileJ][tx] = G[q];
+        }
+        if (zface) {
+            R Q[NV];
+            tile_face_flux<NS, 2, 0, 1, R, kStrict>(sP, ty + 2, tx, Q);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) sQ[q][ty][tx] = Q[q];
+        }
+        if (zright) {
+            R Q[NV];
+            tile_face_flux<NS, 2, 0, 1, R, kStrict>(sP, zrow + 2, kTileK, Q);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) sQ[q][zrow][kTileK] = Q[q];
+        }
+        __syncthreads();
+        if (valid) {
+            const long long c = col + i * sx;
+            const double cx = -dt / (g.x[i] - g.x[i - 1]);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
+                const double rhs = cx * (double(Fp[q]) - double(Fm[q])) -
+                                   cy * (double(sG[q][ty + 1][tx]) - double(sG[q][ty][tx])) -
+                                   cz * (double(sQ[q][ty][tx + 1]) - double(sQ[q][ty][tx]));
+                st.cs[q * n3 + c] = st.cs[q * n3 + c] + rhs;
+                Fm[q] = Fp[q];
+            }
+        }
+#pragma unroll
+        for (int f = 0; f < NP; ++f) {
+            w[0][f] = w[1][f];
+            w[1][f] = w[2][f];
+            w[2][f] = w[3][f];
+            w[3][f] = next[f];
+        }
+    }
+}
+
 // ------------------------------------------------- recovery + kinetics
 
-template <int NS>
+// kWriteCs false: the conserved planes are unchanged (recovery alone reads
+// them and changes nothing there), so they are not written back.
+template <int NS, bool kWriteCs = true>
 __device__ __forceinline__ void store_cell(const DevMech &m, const DevState &st, long long n3, long long c,
                                            const CellState<NS> &cell)
 {
@@ -237,8 +420,10 @@ __device__ __forceinline__ void store_cell(const DevMech &m, const DevState &st,
 #pragma unroll
         for (int s = 0; s < NS; ++s) st.prim32[(kY0 + s) * n3 + c] = float(cell.Y[s]);
     }
+    if (kWriteCs) {
 #pragma unroll
-    for (int q = 0; q < NS + 4; ++q) st.cs[q * n3 + c] = cell.cs[q];
+        for (int q = 0; q < NS + 4; ++q) st.cs[q * n3 + c] = cell.cs[q];
+    }
     st.T[c] = cell.T;
     st.E[c] = cell.E;
     if (!(isfinite(cell.D) && isfinite(cell.T)))
@@ -362,7 +547,7 @@ __global__ void __launch_bounds__(128) k_recover_react(const __grid_constant__ D
     if (kReact)
         st.nchem[c] = react_cell<NS, Rt>(m, cell, *dt_dev, max_substeps, st.counters, st.cms ? st.cms + c : nullptr,
                                          n3);
-    store_cell<NS>(m, st, n3, c, cell);
+    store_cell<NS, kReact>(m, st, n3, c, cell);
 }
 
 // ------------------------------------------------- learned chemistry
@@ -387,7 +572,7 @@ __global__ void __launch_bounds__(128) k_recover_classify(const __grid_constant_
         CellState<NS> cell;
         load_cell<NS>(st, n3, c, cell);
         recover_state<NS>(m, cell);
-        store_cell<NS>(m, st, n3, c, cell);
+        store_cell<NS, false>(m, st, n3, c, cell);
         double reactive = 0, radical = 0;
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
@@ -471,6 +656,7 @@ __global__ void __launch_bounds__(128) k_learned_apply(const __grid_constant__ D
             // spread and mean in the model's output space, the change back in physical units
             spread = fmax(spread, sqrt(var) * lp.out_scale[o]);
             mean[o] = lp.out_eps[o] > 0 ? lp.out_eps[o] * sinh(mu) : mu;
+            ok = ok && (lp.out_bound[o] <= 0 || fabs(mean[o]) <= lp.out_bound[o]);
         }
         ok = ok && spread <= lp.tau && isfinite(spread);
         if (ok) {

@@ -46,12 +46,32 @@ cudaError_t flux_launch(const LaunchArgs &a, const R *prim)
     return cudaGetLastError();
 }
 
+template <int NS, typename R, bool kStrict>
+cudaError_t tiled_flux_launch(const LaunchArgs &a, const R *prim)
+{
+    const DevGrid &g = a.g;
+    const size_t smem = tiled_flux_smem_bytes<NS, R>();
+    static bool configured = false; // per instantiation, once per process
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_flux_update_tiled<NS, R, kStrict>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess)
+            return e;
+        configured = true;
+    }
+    const dim3 block(kTileK, kTileJ);
+    const dim3 grid((g.nk + kTileK - 1) / kTileK, (g.nj + kTileJ - 1) / kTileJ, (g.ni + kTileCI - 1) / kTileCI);
+    k_flux_update_tiled<NS, R, kStrict><<<grid, block, smem, a.stream>>>(g, a.st, prim, a.dt_dev);
+    return cudaGetLastError();
+}
+
 template <int NS, int NR>
 cudaError_t flux_t(const LaunchArgs &a)
 {
-    // mixed precision: FP32 reconstruction and AUSM (always the division-light forms)
+    // mixed precision: FP32 reconstruction and AUSM (always the division-light
+    // forms), plane-tiled
     if (a.precision == 1)
-        return flux_launch<NS, float, false>(a, a.st.prim32);
+        return tiled_flux_launch<NS, float, false>(a, a.st.prim32);
     return flux_launch<NS, double, kStrictFlux>(a, a.st.prim);
 }
 
@@ -194,6 +214,10 @@ cudaError_t launch_set_value(double *dst, double v, cudaStream_t s)
     k_set_value<<<1, 1, 0, s>>>(dst, v);
     return cudaGetLastError();
 }
+
+const Launchers launchers = {&launch_boundary,         &launch_flux_update,      &launch_recover_react,
+                             &launch_derived,          &launch_recover_classify, &launch_learned_features,
+                             &launch_learned_apply,    &launch_react_queue};
 
 #undef EU3D_DISPATCH
 

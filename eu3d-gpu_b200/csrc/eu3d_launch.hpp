@@ -23,6 +23,18 @@ struct LaunchArgs {
 
 bool sizes_supported(int ns, int nr);
 
+// The launchers of one arithmetic flavour, so the host picks a flavour once.
+struct Launchers {
+    cudaError_t (*boundary)(const LaunchArgs &a);
+    cudaError_t (*flux_update)(const LaunchArgs &a);
+    cudaError_t (*recover_react)(const LaunchArgs &a, bool react);
+    cudaError_t (*derived)(const LaunchArgs &a, int which, double *out);
+    cudaError_t (*recover_classify)(const LaunchArgs &a, const LearnedParams &lp);
+    cudaError_t (*learned_features)(const LaunchArgs &a, const LearnedParams &lp, int nq);
+    cudaError_t (*learned_apply)(const LaunchArgs &a, const LearnedParams &lp, int nq);
+    cudaError_t (*react_queue)(const LaunchArgs &a, const int *queue, const int *count, int nq, int counter);
+};
+
 #define EU3D_DECLARE_LAUNCHERS(NSP)                                                                \
     namespace NSP {                                                                                \
     cudaError_t launch_boundary(const LaunchArgs &a);                                              \
@@ -39,9 +51,11 @@ bool sizes_supported(int ns, int nr);
                                       const double *p, const double *Y, double *cs, double *E);    \
     cudaError_t launch_chem_samples(const LaunchArgs &a, long long n, double *cs, double *T,       \
                                     double *E, const double *dt, int *nchem);                      \
+    extern const Launchers launchers;                                                              \
     }
 
 EU3D_DECLARE_LAUNCHERS(strict)
 EU3D_DECLARE_LAUNCHERS(fast)
+EU3D_DECLARE_LAUNCHERS(mixed)
 
 } // namespace eu3d

@@ -79,6 +79,7 @@ struct LearnedParams {
     double box_lo[kMaxS + 3], box_hi[kMaxS + 3]; // accepted input ranges
     double out_scale[kMaxS + 1];
     double out_eps[kMaxS + 1]; // model output o is asinh(change / eps) when eps > 0
+    double out_bound[kMaxS + 1]; // |mean change| above it (> 0) sends the cell to the stiff kinetics
     double proj[kMaxS][kMaxS]; // element-conservation projector
     int inert[kMaxS];
     int radical[kMaxS];

@@ -47,7 +47,7 @@ class MechanismC(ctypes.Structure):
 
 class LearnedConfig(ctypes.Structure):
     _fields_ = [("tau", _D), ("frozen_y", _D), ("frozen_T", _D), ("frozen_radical", _D), ("box_lo", _P),
-                ("box_hi", _P), ("out_scale", _P), ("out_eps", _P)]
+                ("box_hi", _P), ("out_scale", _P), ("out_eps", _P), ("out_bound", _P)]
 
 
 class StepStats(ctypes.Structure):
@@ -285,9 +285,9 @@ class Solver:
                                               None if nchem is None else nchem.data_ptr()), "chem_advance")
 
     def set_learned(self, model, tau, box_lo, box_hi, out_scale, frozen_y=1e-9, frozen_T=0.0,
-                    frozen_radical=1e-9, out_eps=None):
+                    frozen_radical=1e-9, out_eps=None, out_bound=None):
         keep = [np.ascontiguousarray(v, dtype=np.float64) for v in (box_lo, box_hi, out_scale)]
-        keep.append(None if out_eps is None else np.ascontiguousarray(out_eps, dtype=np.float64))
+        keep += [None if v is None else np.ascontiguousarray(v, dtype=np.float64) for v in (out_eps, out_bound)]
         self._learned_keep = keep
         cfg = LearnedConfig(float(tau), float(frozen_y), float(frozen_T), float(frozen_radical),
                             *[None if v is None else v.ctypes.data for v in keep])

@@ -180,3 +180,25 @@ def cfl_dt(x, y, P, D, U, V, G, cfl, bc=2):
     C = np.sqrt(G[s] * P[s] / D[s])
     t = np.minimum(dx / (np.abs(U[s]) + C), dy / (np.abs(V[s]) + C))
     return cfl * float(t.min())
+
+
+def hot_reacting_block(nx, ny, nz, mw, ns, t_range=(1300.0, 2600.0), p_range=(1e5, 1e6), n2_max=0.6, bc=2):
+    """Quiescent reacting gas over a haloed nx x ny x nz node array (ghosts
+    included): T rises linearly along x over t_range, p log-linearly along y
+    over p_range, and stoichiometric 2H2+O2 is diluted with 0..n2_max N2 (mass)
+    along z. Velocity is zero and the fields are smooth, so a timestep is
+    almost entirely kinetics: the case isolates the chemistry phase."""
+    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    fx = np.clip((ii - bc) / max(nx - 2 * bc - 1, 1), 0, 1)
+    fy = np.clip((jj - bc) / max(ny - 2 * bc - 1, 1), 0, 1)
+    fz = np.clip((kk - bc) / max(nz - 2 * bc - 1, 1), 0, 1)
+    T = t_range[0] + (t_range[1] - t_range[0]) * fx
+    P = p_range[0] * (p_range[1] / p_range[0]) ** fy
+    n2 = n2_max * fz
+    y_h2 = 2 * mw[S_H2] / (2 * mw[S_H2] + mw[S_O2])
+    Y = np.zeros((ns, nx, ny, nz))
+    Y[S_H2] = (1 - n2) * y_h2
+    Y[S_O2] = (1 - n2) * (1 - y_h2)
+    Y[S_N2] = n2
+    Z = np.zeros((nx, ny, nz))
+    return P, T, Z, Z.copy(), Z.copy(), Y

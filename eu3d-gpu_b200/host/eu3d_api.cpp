@@ -205,6 +205,16 @@ LaunchArgs launch_args(eu_handle *h)
 
 bool is_strict(const eu_handle *h) { return h->cfg.arith == EU_ARITH_STRICT; }
 
+// Kernels of the handle's flavour: mixed precision has its own translation
+// unit (FP32 fluxes, fast FP64 forms) whatever cfg.arith says; FP64 follows
+// cfg.arith.
+const Launchers &flavour(const eu_handle *h)
+{
+    if (h->cfg.precision == EU_PREC_MIXED)
+        return mixed::launchers;
+    return is_strict(h) ? strict::launchers : fast::launchers;
+}
+
 
 } // namespace
 
@@ -601,28 +611,37 @@ void element_projector(const MechanismTables &m, double (&P)[kMaxS][kMaxS])
 
 // One learned-chemistry phase of a step: recover + classify every cell,
 // features of the queued cells, the ensemble, gate + apply, stiff fallback.
-eu_status learned_chemistry(eu_handle *h, const LaunchArgs &a, bool strict_, long long *reacting)
+eu_status learned_chemistry(eu_handle *h, const LaunchArgs &a, const Launchers &L, long long *reacting,
+                            int *launches)
 {
     LearnedParams &lp = h->lp;
     CK(h, cudaMemsetAsync(lp.counts, 0, 2 * sizeof(int), h->stream));
-    CK(h, strict_ ? strict::launch_recover_classify(a, lp) : fast::launch_recover_classify(a, lp));
+    CK(h, L.recover_classify(a, lp));
+    ++*launches;
     CK(h, cudaMemcpyAsync(h->h_counts, lp.counts, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
     const int nq = h->h_counts[0];
     *reacting = nq;
     if (nq == 0)
         return EU_OK;
-    CK(h, strict_ ? strict::launch_learned_features(a, lp, nq) : fast::launch_learned_features(a, lp, nq));
+    CK(h, L.learned_features(a, lp, nq));
     eu_status s = mlp_predict_stream(h->model, lp.feat, nq, lp.pred, h->stream);
     if (s != EU_OK)
         return fail(h, s, "learned model: %s", eu_mlp_last_error(h->model));
-    CK(h, strict_ ? strict::launch_learned_apply(a, lp, nq) : fast::launch_learned_apply(a, lp, nq));
+    CK(h, L.learned_apply(a, lp, nq));
+    // features, apply, and per batch of rows: packing, then the layers and the
+    // unscaling of every member
+    int n_in = 0, n_out = 0, members = 0;
+    mlp_shape(h->model, &n_in, &n_out, &members);
+    const int batches = mlp_batches(h->model, nq);
+    *launches += 2 + batches * (1 + members * (mlp_layers(h->model) + 1));
     CK(h, cudaMemcpyAsync(h->h_counts + 1, lp.counts + 1, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
     const int nf = h->h_counts[1];
-    if (nf > 0)
-        CK(h, strict_ ? strict::launch_react_queue(a, lp.fallback, lp.counts + 1, nf, kCntFallback)
-                      : fast::launch_react_queue(a, lp.fallback, lp.counts + 1, nf, kCntFallback));
+    if (nf > 0) {
+        CK(h, L.react_queue(a, lp.fallback, lp.counts + 1, nf, kCntFallback));
+        ++*launches;
+    }
     return EU_OK;
 }
 
@@ -706,6 +725,7 @@ eu_status eu_set_learned(eu_handle *h, eu_mlp *model, const eu_learned_config *l
     for (int o = 0; o < ns + 1; ++o) {
         lp.out_scale[o] = lc->out_scale[o];
         lp.out_eps[o] = lc->out_eps ? lc->out_eps[o] : 0.0;
+        lp.out_bound[o] = lc->out_bound ? lc->out_bound[o] : 0.0;
     }
     for (int s = 0; s < ns; ++s) {
         std::string up;
@@ -740,7 +760,7 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
     if (learned && !h->model)
         return fail(h, EU_ERR_NOT_READY, "learned chemistry needs eu_set_learned first");
     long long reacting = 0;
-    const bool st_ = is_strict(h);
+    const Launchers &L = flavour(h);
     double phase[4] = {0, 0, 0, 0};
     int launches = 0;
     if (stats)
@@ -751,17 +771,18 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
     for (int n = 0; n < nsteps; ++n) {
         CK(h, cudaMemsetAsync(h->st.counters, 0, kCntPerStep * sizeof(unsigned long long), h->stream));
         if (prof) CK(h, cudaEventRecord(h->pev[0], h->stream));
-        CK(h, st_ ? strict::launch_boundary(a) : fast::launch_boundary(a));
+        CK(h, L.boundary(a));
         if (prof) CK(h, cudaEventRecord(h->pev[1], h->stream));
-        CK(h, st_ ? strict::launch_flux_update(a) : fast::launch_flux_update(a));
+        CK(h, L.flux_update(a));
         if (prof) CK(h, cudaEventRecord(h->pev[2], h->stream));
+        launches += 2;
         if (learned) {
-            eu_status ls = learned_chemistry(h, a, st_, &reacting);
+            eu_status ls = learned_chemistry(h, a, L, &reacting, &launches);
             if (ls != EU_OK)
                 return ls;
-            launches += 4;
         } else {
-            CK(h, st_ ? strict::launch_recover_react(a, react) : fast::launch_recover_react(a, react));
+            CK(h, L.recover_react(a, react));
+            ++launches;
         }
         if (prof) {
             CK(h, cudaEventRecord(h->pev[3], h->stream));
@@ -772,7 +793,6 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
                 phase[q] += ms;
             }
         }
-        launches += 3;
     }
     if (!stats)
         return EU_OK;
@@ -852,7 +872,7 @@ eu_status eu_get_field(eu_handle *h, const char *name, double *out)
     for (int w = 0; w < 5; ++w)
         if (n == derived[w]) {
             const LaunchArgs a = launch_args(h);
-            CK(h, is_strict(h) ? strict::launch_derived(a, w, h->d_scratch) : fast::launch_derived(a, w, h->d_scratch));
+            CK(h, flavour(h).derived(a, w, h->d_scratch));
             CK(h, cudaMemcpyAsync(out, h->d_scratch, b, cudaMemcpyDeviceToHost, h->stream));
             CK(h, cudaStreamSynchronize(h->stream));
             return EU_OK;

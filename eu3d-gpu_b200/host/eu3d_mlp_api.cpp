@@ -202,6 +202,13 @@ bool mlp_shape(const eu_mlp *m, int *n_in, int *n_out, int *members)
     return true;
 }
 
+int mlp_layers(const eu_mlp *m) { return m && m->ready ? m->hidden + 1 : 0; }
+
+int mlp_batches(const eu_mlp *m, long long n)
+{
+    return m && m->ready && m->max_batch > 0 ? int((n + m->max_batch - 1) / m->max_batch) : 0;
+}
+
 bool mlp_view(const eu_mlp *m, MlpView *v)
 {
     if (!m || !m->ready || !v)

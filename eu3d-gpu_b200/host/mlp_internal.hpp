@@ -8,6 +8,11 @@
 namespace eu3d {
 // Model shape; false when the model is not initialised.
 bool mlp_shape(const eu_mlp *m, int *n_in, int *n_out, int *members);
+// Layers per member (hidden + output) and the row batches mlp_predict_stream
+// splits n rows into: what it launches is, per batch, one packing kernel and
+// per member one GEMM per layer and one unscaling kernel.
+int mlp_layers(const eu_mlp *m);
+int mlp_batches(const eu_mlp *m, long long n);
 // Physical outputs of every member for n fp32 input rows, on `stream`:
 // out[member][row][n_out]. Uses the model's scratch buffers.
 eu_status mlp_predict_stream(eu_mlp *m, const float *X, long long n, float *out, cudaStream_t stream);

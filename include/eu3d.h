@@ -269,7 +269,9 @@ eu_status eu_mlp_predict_noalloc(eu_mlp *m, const float *X, long long n, float *
  * otherwise the stiff kinetics advances it. Cells whose non-inert mass
  * fraction is below frozen_y, or that are colder than frozen_T with a radical
  * pool (H, O, OH, HO2, H2O2 by species name) below frozen_radical, skip
- * chemistry. When out_eps[o] > 0 the model's output o is asinh(change/out_eps[o]). */
+ * chemistry. When out_eps[o] > 0 the model's output o is asinh(change/out_eps[o]).
+ * When out_bound[o] > 0, a mean change of magnitude above it (outside the
+ * range the model was trained on) also sends the cell to the stiff kinetics. */
 typedef struct {
     double tau;
     double frozen_y;
@@ -279,6 +281,7 @@ typedef struct {
     const double *box_hi;    /* [ns + 3] */
     const double *out_scale; /* [ns + 1] */
     const double *out_eps;   /* [ns + 1], NULL: linear outputs */
+    const double *out_bound; /* [ns + 1], NULL: no output range check */
 } eu_learned_config;
 
 eu_status eu_set_learned(eu_handle *h, eu_mlp *model, const eu_learned_config *cfg);

@@ -82,3 +82,43 @@ def test_gate_box_sends_cells_to_fallback(gpu):
     b.set_learned(m, tau=1e30, box_lo=lo, box_hi=hi, out_scale=np.ones(NS + 1), frozen_y=1e-9)
     st = b.step(1, float(z["dt"]))
     assert st["learned"] == 0 and st["fallback"] == st["reacting"] > 0
+
+
+def hot_mixture(gpu, chemistry, precision="fp64"):
+    """A quiescent 24 x 8 x 8 block of reacting gas: T from 1300 to 2600 K along x,
+    p from 0.1 to 1 MPa along y, 2H2+O2 diluted with 0-60 % N2 along z. No flux
+    acts (velocity 0, smooth fields), so a step is the kinetics."""
+    ni, nj, nk = 24, 8, 8
+    ext = (0.0, 0.024, 0.0, 0.008, 0.0, 0.008)
+    mech = gpu.parse_mechanism(cases.MECH_JA919, cases.THERMO)
+    prim = cases.hot_reacting_block(ni + 4, nj + 4, nk + 4, mech["mw"], mech["ns"])
+    s = gpu.Solver(ni, nj, nk, ext, chemistry=chemistry, precision=precision, arith="fast")
+    s.set_mechanism(mech)
+    s.set_primitive(*prim)
+    return s
+
+
+def test_trained_model_replaces_stiff_substeps(gpu):
+    """What the trained network gains over the stiff kinetics alone: on hot
+    reacting gas the committed checkpoint advances most cells itself, so far
+    fewer trapezoid substeps run, at a species error (mean over cells of
+    sum_s |dY_s| against the stiff step) within 1e-3."""
+    import learned
+    dt = 5e-8
+    a = hot_mixture(gpu, "stiff")
+    b = hot_mixture(gpu, "learned")
+    model, gate = learned.load()
+    learned.attach(b, model, gate)
+    sa = a.step(1, dt)
+    sb = b.step(1, dt)
+    n = 24 * 8 * 8
+    assert sa["reacting"] == n and sb["reacting"] == n
+    assert sb["learned"] + sb["fallback"] == n
+    assert sb["learned"] >= 0.5 * n, sb
+    assert sb["sum_nchem"] <= 0.5 * sa["sum_nchem"], (sa["sum_nchem"], sb["sum_nchem"])
+    ya, yb = interior(a.get("Yi")), interior(b.get("Yi"))
+    l1 = np.abs(ya - yb).sum(axis=0)
+    assert l1.mean() <= 1e-3, l1.mean()
+    assert np.allclose(yb.sum(axis=0), 1.0, atol=1e-12)
+    print(f"stiff substeps {sa['sum_nchem']}, learned path {sb['sum_nchem']}; learned cells {sb['learned']} of {n}; "
+          f"species L1 mean {l1.mean():.2e} max {l1.max():.2e}")
