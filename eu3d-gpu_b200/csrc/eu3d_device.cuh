@@ -227,6 +227,7 @@ __device__ __forceinline__ void recover_state(const DevMech &m, CellState<NS> &c
     double D = 0;
 #pragma unroll
     for (int s = 0; s < NS; ++s) D += c.cs[s];
+#ifdef EU_EXACT_CHEM
 #pragma unroll
     for (int s = 0; s < NS; ++s) c.Y[s] = c.cs[s] / D;
     c.D = D;
@@ -235,6 +236,18 @@ __device__ __forceinline__ void recover_state(const DevMech &m, CellState<NS> &c
     c.V = c.cs[NS + 1] / D;
     c.W = c.cs[NS + 2] / D;
     c.E = (c.cs[NS + 3] - 0.5 * D * (c.U * c.U + c.V * c.V + c.W * c.W)) / D;
+#else
+    // one refined reciprocal of the density instead of NS + 4 divisions
+    const double invD = rcp_nr(D);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) c.Y[s] = c.cs[s] * invD;
+    c.D = D;
+    c.T = newton_temperature<NS>(m, c.T, c.E, c.Y);
+    c.U = c.cs[NS + 0] * invD;
+    c.V = c.cs[NS + 1] * invD;
+    c.W = c.cs[NS + 2] * invD;
+    c.E = (c.cs[NS + 3] - 0.5 * D * (c.U * c.U + c.V * c.V + c.W * c.W)) * invD;
+#endif
 }
 
 // P, H, Gamma of Update_after_CS (src/Flowfield.cpp:1606-1614).
@@ -242,6 +255,7 @@ template <int NS>
 __device__ __forceinline__ void finish_primitives(const DevMech &m, const CellState<NS> &c, double &P, double &H,
                                                   double &G)
 {
+#ifdef EU_EXACT_CHEM
     double inv_w = 0;
 #pragma unroll
     for (int s = 0; s < NS; ++s) inv_w += c.Y[s] / m.mw[s];
@@ -249,20 +263,28 @@ __device__ __forceinline__ void finish_primitives(const DevMech &m, const CellSt
     const double Rgas = kRUniv * 1000 / Wav;
     P = c.T * c.D * Rgas;
     H = P / c.D + c.E;
-#ifdef EU_EXACT_CHEM
     const TPow p = make_tpow(c.T, false);
     double cp = 0;
 #pragma unroll
     for (int s = 0; s < NS; ++s) cp += cp_species<NS>(m, p, m.ri[s], s) * c.Y[s];
+    const double Cp = cp * 1000;
+    G = Cp / (Cp - kRUniv * inv_w * 1000);
 #else
+    // R_mix = 1000 sum_s Y_s R_s (R_s = R/W_s), so p/rho = T R_mix: no divisions
+    double rg = 0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) rg = fma(c.Y[s], m.ri[s], rg);
+    const double Rgas = rg * 1000;
+    P = c.T * c.D * Rgas;
+    H = c.T * Rgas + c.E;
     MixPoly<NS> mp;
     mix_poly<NS>(m, c.Y, c.T < kThermoSwitch, mp);
     const double T0 = c.T, inv = rcp_nr(T0);
     const double cp = fma(T0, fma(T0, fma(T0, fma(T0, mp.a6, mp.a5), mp.a4), mp.a3), mp.a2) +
                       inv * fma(mp.a0, inv, mp.a1);
-#endif
     const double Cp = cp * 1000;
-    G = Cp / (Cp - kRUniv * inv_w * 1000);
+    G = div_fast(Cp, Cp - Rgas);
+#endif
 }
 
 // ------------------------------------------------------------- kinetics
