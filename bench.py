@@ -46,6 +46,12 @@ L2_BYTES = 126 * 2 ** 20
 # Algorithmic bytes per cell-step of the flux + update kernel: 16 primitives
 # read, 13 conserved read and written (FP64); FP32 primitives in mixed mode.
 FLUX_BYTES = {"fp64": (16 + 26) * 8, "mixed": 16 * 4 + 26 * 8}
+# FP64 flops per cell-substep of the stiff kinetics (rates, trapezoid update,
+# state rebuild with its temperature Newton), counted on the oracle over the
+# thin RSBI case by oracle/flop_count.cpp.
+F_SUB = 6017
+# FP64 vector peak of a B200 (datasheet; no measured FP64 figure is available).
+FP64_PEAK_TFLOPS = 37.0
 
 
 def env_int(name, default):
@@ -366,7 +372,19 @@ def our_arm(args):
         y_ref = sp_.get("Yi")
         sp_.close()
         err_all, err_reactive = species_error(y_fast, y_ref)
-        plain = {"value": round(ncell * args.steps * world / (pms / 1e3) / 1e6, 3), "ms_per_step":
+        # the kinetics phase of the plain step against the FP64 roofline
+        spk = make_solver("stiff", "fp64", "fast", profile=True)
+        spk.step(args.warmup, dt)
+        kst = spk.step(args.steps, dt)
+        spk.close()
+        kin_ms = kst["phase_ms"][2] / args.steps
+        kin_tf = F_SUB * kst["sum_nchem"] / (kin_ms / 1e3) / 1e12
+        kin = {"kernel": "recover_react", "bound": "fp64", "achieved": round(kin_tf, 3),
+               "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": round(kin_tf / FP64_PEAK_TFLOPS, 4),
+               "peak_source": "datasheet", "flop_per_substep": F_SUB, "substeps_per_step": kst["sum_nchem"],
+               "ms_per_step": round(kin_ms, 4)}
+        plain = {"kinetics_roofline": kin,
+                 "value": round(ncell * args.steps * world / (pms / 1e3) / 1e6, 3), "ms_per_step":
                  round(pms / args.steps, 4), "speedup": round(value / (ncell * args.steps * world / (pms / 1e3) / 1e6), 3),
                  "species_l1_vs_plain": err_all, "species_l1_vs_plain_reactive_cells": err_reactive,
                  "after_steps": args.warmup + args.steps}
