@@ -5,6 +5,7 @@
 
 #include "eu3d_device.cuh"
 #include "eu3d_mech_JA919.cuh"
+#include "eu3d_tc.cuh"
 
 #ifndef EU3D_NS
 #error "define EU3D_NS (the arithmetic flavour's namespace) before including eu3d_kernels.cuh"
@@ -59,10 +60,12 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
             rebuild = true;
         }
     } else {
+        // the ghost index runs fastest: the 2 bc ghosts of one (i, j) row sit in
+        // two contiguous pairs, so a warp touches 16 pairs instead of 32 rows
         t -= nxf + nyf;
-        const int j = bc + int(t % nj);
-        const int i = bc + int((t / nj) % ni);
-        const int q = int(t / ((long long)nj * ni));
+        const int q = int(t % (2 * bc));
+        const int j = bc + int((t / (2 * bc)) % nj);
+        const int i = bc + int(t / (2LL * bc * nj));
         const int k = q < bc ? q : nk + q;
         const int sk = q < bc ? 2 * bc - 1 - k : 2 * (nk + bc) - 1 - k;
         dst = cell_index(g, i, j, k);
@@ -220,16 +223,19 @@ __global__ void __launch_bounds__(kFluxTK *kFluxTJ, 1)
 
 // Plane-tiled flux divergence and update: the same faces, arithmetic and RHS
 // order as k_flux_update (bitwise the same result), with every primitive read
-// from HBM once per plane instead of once per stencil point.
+// from HBM once per plane instead of once per stencil point, and the loads of
+// the next plane overlapped with the current plane's arithmetic.
 //
 // A block owns a kTileJ x kTileK tile of (j, k) columns and marches along x.
 // Each thread keeps its column's x-stencil (planes i-1 .. i+2 of every
 // primitive) in registers and loads plane i+3 one node ahead. Plane i of the
 // tile plus a two-node halo in j and k is staged in shared memory, from which
-// the y- and z-face fluxes are formed. Face indices: sG[q][r] is the y face
-// below tile row r (r = kTileJ: above the last row), sQ[q][r][c] the z face
-// left of column c. Partial tiles: the faces of the valid rows/columns are
-// formed, including the one past the last valid row/column.
+// the y- and z-face fluxes are formed; two stages alternate, and while plane i
+// is computed the halo of plane i+1 (cp.async) and the conserved values of
+// plane i (cp.async, read by the update) are in flight. Face indices: sG[q][r]
+// is the y face below tile row r (r = kTileJ: above the last row), sQ[q][r][c]
+// the z face left of column c. Partial tiles: the faces of the valid
+// rows/columns are formed, including the one past the last valid row/column.
 constexpr int kTileK = 32, kTileJ = 8, kTileCI = 16;
 constexpr int kTileRows = kTileJ + 4, kTileCols = kTileK + 4;
 constexpr int kTileHalo = 4 * kTileCols + 4 * kTileJ; // two rows above, two below, two columns each side
@@ -237,8 +243,8 @@ constexpr int kTileHalo = 4 * kTileCols + 4 * kTileJ; // two rows above, two bel
 template <int NS, typename R>
 constexpr size_t tiled_flux_smem_bytes()
 {
-    return sizeof(R) * ((7 + NS) * kTileRows * kTileCols +
-                        (NS + 4) * ((kTileJ + 1) * kTileK + kTileJ * (kTileK + 1)));
+    return sizeof(double) * (NS + 4) * kTileJ * kTileK + sizeof(R) * 2 * (7 + NS) * kTileRows * kTileCols +
+           sizeof(R) * (NS + 4) * ((kTileJ + 1) * kTileK + kTileJ * (kTileK + 1));
 }
 
 // Face flux from four consecutive stencil points of the staged plane tile,
@@ -275,9 +281,11 @@ __global__ void __launch_bounds__(kTileK *kTileJ, 2)
     k_flux_update_tiled(const DevGrid g, const DevState st, const R *__restrict__ prim, const double *__restrict__ dt_dev)
 {
     constexpr int NP = 7 + NS, NV = NS + 4;
+    using Plane = R[NP][kTileRows][kTileCols];
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R(*sP)[kTileRows][kTileCols] = reinterpret_cast<R(*)[kTileRows][kTileCols]>(smem_raw);
-    unsigned char *flux_raw = smem_raw + sizeof(R) * NP * kTileRows * kTileCols;
+    double(*sC)[kTileJ][kTileK] = reinterpret_cast<double(*)[kTileJ][kTileK]>(smem_raw);
+    Plane *stage = reinterpret_cast<Plane *>(smem_raw + sizeof(double) * NV * kTileJ * kTileK);
+    unsigned char *flux_raw = reinterpret_cast<unsigned char *>(stage + 2);
     R(*sG)[kTileJ + 1][kTileK] = reinterpret_cast<R(*)[kTileJ + 1][kTileK]>(flux_raw);
     R(*sQ)[kTileJ][kTileK + 1] =
         reinterpret_cast<R(*)[kTileJ][kTileK + 1]>(flux_raw + sizeof(R) * NV * (kTileJ + 1) * kTileK);
@@ -318,6 +326,20 @@ __global__ void __launch_bounds__(kTileK *kTileJ, 2)
     const long long col = resident ? cell_index(g, 0, j, k) : 0;
     const long long hcol = halo ? cell_index(g, 0, hj, hk) : 0;
 
+    // plane p of the tile into stage s: the own node from registers, the halo
+    // node by cp.async; one commit group per call (empty when nothing to copy)
+    auto stage_plane = [&](int p, const R(&own)[NP], int s) {
+        if (resident) {
+#pragma unroll
+            for (int f = 0; f < NP; ++f) stage[s][f][ty + 2][tx + 2] = own[f];
+        }
+        if (halo) {
+#pragma unroll
+            for (int f = 0; f < NP; ++f) tc::cp_async4(&stage[s][f][hr][hc], prim + f * n3 + hcol + p * sx);
+        }
+        tc::cp_async_commit();
+    };
+
     R w[4][NP];
 #pragma unroll
     for (int p = 0; p < 4; ++p)
@@ -333,50 +355,58 @@ __global__ void __launch_bounds__(kTileK *kTileJ, 2)
         w[2][f] = w[3][f];
         w[3][f] = resident ? __ldg(prim + f * n3 + col + (i_begin + 2) * sx) : R(0);
     }
+    stage_plane(i_begin, w[1], 0);
 
     for (int i = i_begin; i < i_end; ++i) {
-        // window: planes i-1, i, i+1, i+2; stage plane i of the tile
-        if (resident) {
+        // window: planes i-1, i, i+1, i+2. Stage s holds plane i (its halo may
+        // still be in flight); the other stage was last read before the
+        // previous iteration's second barrier.
+        const int s = (i - i_begin) & 1;
+        if (valid) {
 #pragma unroll
-            for (int f = 0; f < NP; ++f) sP[f][ty + 2][tx + 2] = w[1][f];
+            for (int q = 0; q < NV; ++q) tc::cp_async8(&sC[q][ty][tx], st.cs + q * n3 + col + i * sx);
         }
-        if (halo) {
-#pragma unroll
-            for (int f = 0; f < NP; ++f) sP[f][hr][hc] = __ldg(prim + f * n3 + hcol + i * sx);
-        }
+        tc::cp_async_commit();
+        if (i + 1 < i_end)
+            stage_plane(i + 1, w[2], s ^ 1);
+        else
+            tc::cp_async_commit();
         R next[NP];
         const bool more = resident && i + 1 < i_end;
 #pragma unroll
         for (int f = 0; f < NP; ++f) next[f] = more ? __ldg(prim + f * n3 + col + (i + 3) * sx) : R(0);
+        // groups in flight, oldest first: halo(i), conserved(i), halo(i+1)
+        tc::cp_async_wait<2>();
         __syncthreads();
         R Fp[NV];
         if (valid)
             window_face_flux<NS, R, kStrict>(w, Fp);
         if (yface) {
             R G[NV];
-            tile_face_flux<NS, 1, 1, 0, R, kStrict>(sP, ty, tx + 2, G);
+            tile_face_flux<NS, 1, 1, 0, R, kStrict>(stage[s], ty, tx + 2, G);
 #pragma unroll
             for (int q = 0; q < NV; ++q) sG[q][ty][tx] = G[q];
         }
         if (ytop) {
             R G[NV];
-            tile_face_flux<NS, 1, 1, 0, R, kStrict>(sP, kTileJ, tx + 2, G);
+            tile_face_flux<NS, 1, 1, 0, R, kStrict>(stage[s], kTileJ, tx + 2, G);
 #pragma unroll
             for (int q = 0; q < NV; ++q) sG[q][kTileJ][tx] = G[q];
         }
         if (zface) {
             R Q[NV];
-            tile_face_flux<NS, 2, 0, 1, R, kStrict>(sP, ty + 2, tx, Q);
+            tile_face_flux<NS, 2, 0, 1, R, kStrict>(stage[s], ty + 2, tx, Q);
 #pragma unroll
             for (int q = 0; q < NV; ++q) sQ[q][ty][tx] = Q[q];
         }
         if (zright) {
             R Q[NV];
-            tile_face_flux<NS, 2, 0, 1, R, kStrict>(sP, zrow + 2, kTileK, Q);
+            tile_face_flux<NS, 2, 0, 1, R, kStrict>(stage[s], zrow + 2, kTileK, Q);
 #pragma unroll
             for (int q = 0; q < NV; ++q) sQ[q][zrow][kTileK] = Q[q];
         }
         __syncthreads();
+        tc::cp_async_wait<1>(); // this thread's conserved values of plane i
         if (valid) {
             const long long c = col + i * sx;
             const double cx = -dt / (g.x[i] - g.x[i - 1]);
@@ -385,7 +415,7 @@ __global__ void __launch_bounds__(kTileK *kTileJ, 2)
                 const double rhs = cx * (double(Fp[q]) - double(Fm[q])) -
                                    cy * (double(sG[q][ty + 1][tx]) - double(sG[q][ty][tx])) -
                                    cz * (double(sQ[q][ty][tx + 1]) - double(sQ[q][ty][tx]));
-                st.cs[q * n3 + c] = st.cs[q * n3 + c] + rhs;
+                st.cs[q * n3 + c] = sC[q][ty][tx] + rhs;
                 Fm[q] = Fp[q];
             }
         }
@@ -397,6 +427,7 @@ __global__ void __launch_bounds__(kTileK *kTileJ, 2)
             w[3][f] = next[f];
         }
     }
+    tc::cp_async_wait<0>();
 }
 
 // ------------------------------------------------- recovery + kinetics

@@ -9,11 +9,16 @@ T ~ U[300, 3500] K, p ~ logU[0.05, 5] MPa, dt ~ logU[1e-9, 3e-7] s per step.
 Only rows the step's classifier would hand to the model are used (hot or
 radical-bearing, some reactive species). 90 % train the 3-member ensemble
 (BF16 tensor-core forward/backward/Adam kernels of libeu3d), 10 % calibrate
-the trust gate. Seeded; the whole run takes about five minutes on a B200.
+the trust gate at a mean species L1 error of 2e-5 per step over the accepted rows
+(over 13 steps of igniting gas, 1300-2600 K, the gate calibrated at 2e-4 let the
+error compound to a species L1 of 1.8e-2, while 0.3 x that threshold stayed at 1e-6).
+Seeded; the whole run takes about five minutes on a B200. --calibrate-only keeps
+the weights and re-calibrates the gate on fresh samples.
 """
 from __future__ import annotations
 
 import argparse
+import ast
 import json
 import os
 import sys
@@ -37,9 +42,13 @@ def main():
     ap.add_argument("--train-steps", type=int, default=40000)
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=5e-4)
-    ap.add_argument("--target", type=float, default=2e-4, help="mean species L1 error of accepted rows")
+    ap.add_argument("--target", type=float, default=2e-5, help="mean species L1 error of accepted rows")
     ap.add_argument("--seed", type=int, default=11)
+    ap.add_argument("--calibrate-only", action="store_true",
+                    help="keep the checkpoint's weights; re-calibrate its gate on fresh samples")
     args = ap.parse_args()
+    if args.calibrate_only:
+        return calibrate_only(args)
 
     t0 = time.time()
     s = eu3d.Solver(5, 5, 5, (0, 1, 0, 1, 0, 1), max_substeps=20000)
@@ -66,6 +75,33 @@ def main():
     meta = {"traj": args.traj, "steps_per_traj": args.steps_per_traj, "train_steps": args.train_steps,
             "batch": args.batch, "lr": args.lr, "seed": args.seed, "samples": n,
             "accepted_fraction": gate["accepted_fraction"], "l1_accepted": gate["l1_accepted"], "tau": gate["tau"]}
+    learned.save(args.out, model, scaling, gate, meta)
+    print(json.dumps(meta), flush=True)
+    model.close()
+
+
+def calibrate_only(args):
+    """Fresh samples (a different seed from training's), the stored model, a
+    new gate at args.target."""
+    import numpy as np
+    import torch
+
+    import eu3d
+    import eu3d_cases as cases
+    import learned
+    torch.manual_seed(args.seed + 1000)
+    s = eu3d.Solver(5, 5, 5, (0, 1, 0, 1, 0, 1), max_substeps=20000)
+    s.load_mechanism(cases.MECH_JA919, cases.THERMO)
+    X, T = learned.generate(s, args.traj, args.steps_per_traj, seed=args.seed + 1000)
+    s.close()
+    model, old = learned.load(args.out)
+    z = np.load(args.out)
+    scaling = {k: z[k] for k in ("in_shift", "in_scale", "out_shift", "out_scale")}
+    bound = old["out_bound"]
+    gate = learned.calibrate(model, scaling, X, T, target=args.target, eps=old["out_eps"], bound=bound)
+    meta = dict(ast.literal_eval(str(z["meta"])))
+    meta.update(calibrated_on=int(learned.active_rows(X).sum()), target=args.target, tau=gate["tau"],
+                accepted_fraction=gate["accepted_fraction"], l1_accepted=gate["l1_accepted"])
     learned.save(args.out, model, scaling, gate, meta)
     print(json.dumps(meta), flush=True)
     model.close()
