@@ -484,13 +484,35 @@ struct TableRates {
 // on a recovered cell state. The prediction's rate evaluation is reused by
 // the first substep: both evaluate the same expression on the same state.
 // Returns Nchem; a prediction <= 0 or above max_substeps is counted as an error.
-template <int NS, class Rt>
-__device__ __forceinline__ int react_cell(const DevMech &m, CellState<NS> &cell, double dtm, int max_substeps,
-                                          unsigned long long *counters, double *cms, long long cms_stride)
+// Nchem = ceil(dtm / min_s |Di_s / Wi_s|) over species with Y_s >= 1e-6
+// (src/Reaction.cpp:919-940); a prediction <= 0 or above max_substeps is
+// counted as an error and gives 0 or max_substeps.
+__device__ __forceinline__ int nchem_from_dt(double dtm, double dt, int max_substeps, unsigned long long *counters)
 {
-    double mc[NS];
+    const double ratio = ceil(dtm / dt);
+    if (!(ratio >= 1.0) || ratio > double(max_substeps)) {
+        atomicAdd(&counters[kCntBadNchem], 1ULL);
+        return (ratio > double(max_substeps)) ? max_substeps : 0;
+    }
+    return int(ratio);
+}
+
+__device__ __forceinline__ void count_nchem(unsigned long long *counters, int nchem)
+{
+    if (nchem > 0) {
+        atomicMax(&counters[kCntMaxNchem], (unsigned long long)nchem);
+        atomicAdd(&counters[kCntSumNchem], (unsigned long long)nchem);
+    }
+}
+
+// The prediction: start-of-step rates (kept in `rates` for the first substep)
+// and Nchem.
+template <int NS, class Rt>
+__device__ __forceinline__ int predict_nchem(const DevMech &m, const CellState<NS> &cell, double dtm,
+                                             int max_substeps, unsigned long long *counters, double (&mc)[NS],
+                                             SpeciesRates<NS> &rates)
+{
     scaled_concentrations<NS>(m, cell, mc);
-    SpeciesRates<NS> rates;
     Rt::rates(m, cell.T, mc, rates);
     double dt = dtm;
 #pragma unroll
@@ -501,18 +523,15 @@ __device__ __forceinline__ int react_cell(const DevMech &m, CellState<NS> &cell,
                 dt = dt_temp;
         }
     }
-    const double ratio = ceil(dtm / dt);
-    int nchem;
-    if (!(ratio >= 1.0) || ratio > double(max_substeps)) {
-        atomicAdd(&counters[kCntBadNchem], 1ULL);
-        nchem = (ratio > double(max_substeps)) ? max_substeps : 0;
-    } else {
-        nchem = int(ratio);
-    }
-    if (nchem > 0) {
-        atomicMax(&counters[kCntMaxNchem], (unsigned long long)nchem);
-        atomicAdd(&counters[kCntSumNchem], (unsigned long long)nchem);
-    }
+    return nchem_from_dt(dtm, dt, max_substeps, counters);
+}
+
+// The Nchem substeps, the first one on the prediction's rates.
+template <int NS, class Rt>
+__device__ __forceinline__ void run_substeps(const DevMech &m, CellState<NS> &cell, double dtm, int nchem,
+                                             double (&mc)[NS], SpeciesRates<NS> &rates, double *cms,
+                                             long long cms_stride)
+{
     const double dts = dtm / nchem;
     for (int step = 0; step < nchem; ++step) {
         if (step > 0) {
@@ -525,7 +544,51 @@ __device__ __forceinline__ int react_cell(const DevMech &m, CellState<NS> &cell,
         }
         trapezoid_substep<NS>(m, rates, dts, mc, cell);
     }
+}
+
+template <int NS, class Rt>
+__device__ __forceinline__ int react_cell(const DevMech &m, CellState<NS> &cell, double dtm, int max_substeps,
+                                          unsigned long long *counters, double *cms, long long cms_stride)
+{
+    double mc[NS];
+    SpeciesRates<NS> rates;
+    const int nchem = predict_nchem<NS, Rt>(m, cell, dtm, max_substeps, counters, mc, rates);
+    count_nchem(counters, nchem);
+    run_substeps<NS, Rt>(m, cell, dtm, nchem, mc, rates, cms, cms_stride);
     return nchem;
+}
+
+// Cells whose predicted Nchem exceeds kHeavyNchem are, in the mixed-precision
+// flavour (EU_HEAVY_QUEUE), deferred to k_react_heavy: one warp per cell
+// instead of one thread, so the long serial substep chains of igniting cells
+// do not set the step's time. st.heavy = {count, next, cells...}.
+constexpr int kHeavyNchem = 16;
+
+__device__ __forceinline__ void push_heavy(int *heavy, long long c)
+{
+    const int q = atomicAdd(&heavy[0], 1);
+    heavy[2 + q] = int(c);
+}
+
+// React one recovered cell, or (mixed flavour, heavy queue present) defer it
+// when its Nchem is large. Returns false when deferred.
+template <int NS, class Rt>
+__device__ __forceinline__ bool react_or_defer(const DevMech &m, const DevState &st, long long n3, long long c,
+                                               CellState<NS> &cell, double dtm, int max_substeps)
+{
+    double mc[NS];
+    SpeciesRates<NS> rates;
+    const int nchem = predict_nchem<NS, Rt>(m, cell, dtm, max_substeps, st.counters, mc, rates);
+#ifdef EU_HEAVY_QUEUE
+    if (st.heavy && nchem > kHeavyNchem) {
+        push_heavy(st.heavy, c);
+        return false;
+    }
+#endif
+    count_nchem(st.counters, nchem);
+    run_substeps<NS, Rt>(m, cell, dtm, nchem, mc, rates, st.cms ? st.cms + c : nullptr, n3);
+    st.nchem[c] = nchem;
+    return true;
 }
 
 template <int NS>
@@ -575,9 +638,12 @@ __global__ void __launch_bounds__(128) k_recover_react(const __grid_constant__ D
     CellState<NS> cell;
     load_cell<NS>(st, n3, c, cell);
     recover_state<NS>(m, cell);
-    if (kReact)
-        st.nchem[c] = react_cell<NS, Rt>(m, cell, *dt_dev, max_substeps, st.counters, st.cms ? st.cms + c : nullptr,
-                                         n3);
+    if (kReact) {
+        if (!react_or_defer<NS, Rt>(m, st, n3, c, cell, *dt_dev, max_substeps)) {
+            store_cell<NS, false>(m, st, n3, c, cell); // recovered state for k_react_heavy
+            return;
+        }
+    }
     store_cell<NS, kReact>(m, st, n3, c, cell);
 }
 
@@ -743,9 +809,162 @@ __global__ void __launch_bounds__(128) k_react_queue(const __grid_constant__ Dev
     const long long n3 = g.n3, c = queue[q];
     CellState<NS> cell;
     load_recovered<NS>(st, n3, c, cell);
-    st.nchem[c] = react_cell<NS, Rt>(m, cell, *dt_dev, max_substeps, st.counters, st.cms ? st.cms + c : nullptr, n3);
-    store_cell<NS>(m, st, n3, c, cell);
     atomicAdd(&st.counters[counter], 1ULL);
+    if (react_or_defer<NS, Rt>(m, st, n3, c, cell, *dt_dev, max_substeps))
+        store_cell<NS>(m, st, n3, c, cell);
+}
+
+// ------------------------------------------------- warp-per-cell kinetics
+// The same kinetics as react_cell (prediction, Nchem trapezoid substeps,
+// state rebuild after each) with one warp per cell: lane r evaluates reaction
+// r, lane s owns species s's sums and trapezoid update, and every lane keeps
+// the whole cell state (the rebuild runs redundantly on all lanes). The sums
+// run in the same order as the one-thread form. Tables that lanes index by
+// reaction or species are read from a shared-memory copy of the mechanism;
+// the uniform reads of the state rebuild stay on the kernel parameter.
+
+template <int NS>
+__device__ __forceinline__ double lane_pick(const double (&v)[NS], int lane)
+{
+    double r = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) r = (lane == s) ? v[s] : r;
+    return r;
+}
+
+// Fast-form rates (the mixed flavour's eval_rates) across a warp. On return
+// lane s < NS holds P_s, Q_s and W_s (W with the molecular weight applied).
+// Every lane runs every loop (lanes past NR evaluate reaction 0 and drop it)
+// so the shuffles stay convergent.
+template <int NS, int NR>
+__device__ __forceinline__ void warp_rates(const DevMech &ms, double T, const double (&mc)[NS], int lane, double &Pl,
+                                           double &Ql, double &Wl)
+{
+    static_assert(NR <= 32 && NS <= 32, "one lane per reaction and per species");
+    const TPow p = make_tpow(T, true);
+    const double invRT = 1.0 / (kRUniv * T);
+    const int sl = lane < NS ? lane : 0;
+    const double egl = exp((h_species<NS>(ms, p, kRUniv, sl) - s_species<NS>(ms, p, kRUniv, sl) * T) * invRT);
+    const double iegl = rcp_nr(egl);
+    const int r = lane < NR ? lane : 0;
+    const double invRuT = 1.0 / (kRuCal * T);
+    const double rt_p0 = (kRUniv * T) / (kP0 * 1e-6);
+    const double p0_rt = rcp_nr(rt_p0);
+    double rrf = 1.0, rrb = 1.0, kc_inv = 1.0, rtb = 0.0;
+    const double b = ms.bf[r];
+    double kf;
+    if (ms.eaf[r] == 0.0 && (b == 0.0 || b == 1.0 || b == -1.0 || b == -2.0))
+        kf = ms.af[r] * (b == 0.0 ? 1.0 : b == 1.0 ? T : b == -1.0 ? p.inv : p.inv2);
+    else
+        kf = ms.af[r] * exp(b * p.lnT - ms.eaf[r] * invRuT);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const double eg = __shfl_sync(0xffffffffu, egl, s), ieg = __shfl_sync(0xffffffffu, iegl, s);
+        const double f = ms.sf[r][s], bb = ms.sb[r][s];
+        rrf *= (f == 0.0 ? 1.0 : (f == 1.0 ? mc[s] : mc[s] * mc[s]));
+        rrb *= (bb == 0.0 ? 1.0 : (bb == 1.0 ? mc[s] : mc[s] * mc[s]));
+        const double d = bb - f;
+        kc_inv *= (d == 0.0 ? 1.0 : d == 1.0 ? eg : d == -1.0 ? ieg : d == 2.0 ? eg * eg : ieg * ieg);
+        rtb += mc[s] * ms.tb[r][s];
+    }
+    const double Xr = ms.xr[r];
+    kc_inv *= (Xr == 0.0 ? 1.0 : Xr == 1.0 ? rt_p0 : p0_rt);
+    if (rtb == 0.0)
+        rtb = 1.0;
+    const double fwd = kf * rrf, bwd = kf * kc_inv * rrb;
+    double P = 0.0, Q = 0.0, W = 0.0;
+#pragma unroll 1
+    for (int q = 0; q < NR; ++q) {
+        const double fr = __shfl_sync(0xffffffffu, fwd, q);
+        const double br = __shfl_sync(0xffffffffu, bwd, q);
+        const double tr = __shfl_sync(0xffffffffu, rtb, q);
+        const double bb = ms.sb[q][sl], f = ms.sf[q][sl];
+        if (bb != 0.0 || f != 0.0) {
+            W += (bb - f) * tr * (fr - br);
+            Q += (bb * fr + f * br) * tr;
+            P += (bb * br + f * fr) * tr;
+        }
+    }
+    Pl = P;
+    Ql = Q;
+    Wl = ms.mw[sl] * W;
+}
+
+template <int NS, int NR>
+__global__ void __launch_bounds__(128, 1) k_react_heavy(const __grid_constant__ DevMech m, const DevGrid g,
+                                                     const DevState st, const double *__restrict__ dt_dev,
+                                                     int max_substeps)
+{
+    __shared__ DevMech ms;
+    {
+        const int *src = reinterpret_cast<const int *>(&m);
+        int *dst = reinterpret_cast<int *>(&ms);
+        for (int w = threadIdx.x; w < int(sizeof(DevMech) / sizeof(int)); w += blockDim.x) dst[w] = src[w];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int count = st.heavy[0];
+    const double dtm = *dt_dev;
+    const long long n3 = g.n3;
+    for (;;) {
+        int q = 0;
+        if (lane == 0)
+            q = atomicAdd(&st.heavy[1], 1);
+        q = __shfl_sync(0xffffffffu, q, 0);
+        if (q >= count)
+            break;
+        const long long c = st.heavy[2 + q];
+        CellState<NS> cell;
+        load_recovered<NS>(st, n3, c, cell);
+        double mc[NS], P, Q, W;
+        scaled_concentrations<NS>(m, cell, mc);
+        warp_rates<NS, NR>(ms, cell.T, mc, lane, P, Q, W);
+        // prediction: min over the species lanes, then every lane has Nchem
+        double dt = dtm;
+        if (lane < NS && lane_pick<NS>(cell.Y, lane) >= 1e-6 && W != 0)
+            dt = fmin(dt, fabs(-(lane_pick<NS + 4>(cell.cs, lane) * 1e-3) / W));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) dt = fmin(dt, __shfl_xor_sync(0xffffffffu, dt, o));
+        int nchem = 0;
+        if (lane == 0) {
+            nchem = nchem_from_dt(dtm, dt, max_substeps, st.counters);
+            count_nchem(st.counters, nchem);
+        }
+        nchem = __shfl_sync(0xffffffffu, nchem, 0);
+        const double dts = dtm / nchem, half = dts / 2.0;
+        for (int step = 0; step < nchem; ++step) {
+            if (step > 0) {
+                scaled_concentrations<NS>(m, cell, mc);
+                warp_rates<NS, NR>(ms, cell.T, mc, lane, P, Q, W);
+            }
+            if (st.cms && lane < NS)
+                st.cms[lane * n3 + c] = W * 1e3;
+            double nd = 0.0;
+            if (lane < NS) {
+                const double di = lane_pick<NS + 4>(cell.cs, lane) * 1e-3;
+                const double mcl = lane_pick<NS>(mc, lane);
+                const double qv = ms.mw[lane] * Q;
+                const double pv = (mcl == 0) ? 0.0 : P / mcl;
+                nd = ((1.0 - half * pv) * di + dts * qv) / (1.0 + half * pv) * 1e3;
+            }
+            double D = 0.0;
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                cell.cs[s] = __shfl_sync(0xffffffffu, nd, s);
+                D += cell.cs[s];
+            }
+            cell.cs[NS + 0] = cell.U * D;
+            cell.cs[NS + 1] = cell.V * D;
+            cell.cs[NS + 2] = cell.W * D;
+            cell.cs[NS + 3] = D * cell.E + 0.5 * (cell.U * cell.U + cell.V * cell.V + cell.W * cell.W) * D;
+            recover_state<NS>(m, cell);
+        }
+        if (lane == 0) {
+            st.nchem[c] = nchem;
+            store_cell<NS>(m, st, n3, c, cell);
+        }
+        __syncwarp();
+    }
 }
 
 // ------------------------------------------------- independent cell samples

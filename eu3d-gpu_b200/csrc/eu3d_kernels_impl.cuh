@@ -171,6 +171,14 @@ cudaError_t chem_samples_t(const LaunchArgs &a, long long n, double *cs, double 
     return cudaGetLastError();
 }
 
+template <int NS, int NR>
+cudaError_t heavy_t(const LaunchArgs &a, int blocks)
+{
+    k_react_heavy<NS, NR><<<dim3(unsigned(blocks)), 128, 0, a.stream>>>(*a.mech, a.g, a.st, a.dt_dev,
+                                                                         a.max_substeps);
+    return cudaGetLastError();
+}
+
 } // namespace
 
 // Supported (NS, NR): the repository mechanism H2_JA919 (9 species, 19
@@ -209,6 +217,8 @@ cudaError_t launch_chem_samples(const LaunchArgs &a, long long n, double *cs, do
     EU3D_DISPATCH(chem_samples_t, a, n, cs, T, E, dt, nchem)
 }
 
+cudaError_t launch_react_heavy(const LaunchArgs &a, int blocks) { EU3D_DISPATCH(heavy_t, a, blocks) }
+
 cudaError_t launch_set_value(double *dst, double v, cudaStream_t s)
 {
     k_set_value<<<1, 1, 0, s>>>(dst, v);
@@ -217,7 +227,7 @@ cudaError_t launch_set_value(double *dst, double v, cudaStream_t s)
 
 const Launchers launchers = {&launch_boundary,         &launch_flux_update,      &launch_recover_react,
                              &launch_derived,          &launch_recover_classify, &launch_learned_features,
-                             &launch_learned_apply,    &launch_react_queue};
+                             &launch_learned_apply,    &launch_react_queue,      &launch_react_heavy};
 
 #undef EU3D_DISPATCH
 

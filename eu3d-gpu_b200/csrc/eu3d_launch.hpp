@@ -33,6 +33,7 @@ struct Launchers {
     cudaError_t (*learned_features)(const LaunchArgs &a, const LearnedParams &lp, int nq);
     cudaError_t (*learned_apply)(const LaunchArgs &a, const LearnedParams &lp, int nq);
     cudaError_t (*react_queue)(const LaunchArgs &a, const int *queue, const int *count, int nq, int counter);
+    cudaError_t (*react_heavy)(const LaunchArgs &a, int blocks);
 };
 
 #define EU3D_DECLARE_LAUNCHERS(NSP)                                                                \
@@ -51,6 +52,7 @@ struct Launchers {
                                       const double *p, const double *Y, double *cs, double *E);    \
     cudaError_t launch_chem_samples(const LaunchArgs &a, long long n, double *cs, double *T,       \
                                     double *E, const double *dt, int *nchem);                      \
+    cudaError_t launch_react_heavy(const LaunchArgs &a, int blocks);                               \
     extern const Launchers launchers;                                                              \
     }
 

@@ -48,6 +48,7 @@ struct DevState {
     int *nchem;       // plane
     double *cms;      // ns planes (or null)
     unsigned long long *counters; // see CounterIdx
+    int *heavy;       // mixed precision: {count, next, cells...} of cells left to the warp-per-cell kinetics
 };
 
 // Device counters. The first kCntPerStep are statistics of the latest step

@@ -89,6 +89,11 @@ def library():
         lib.eu_get_field.argtypes = [_P, ctypes.c_char_p, _P]
         lib.eu_sync.argtypes = [_P]
         lib.eu_device_info.argtypes = [_P, ctypes.POINTER(_P), ctypes.POINTER(ctypes.c_size_t)]
+        lib.eu_write_state.argtypes = [_P, ctypes.c_char_p, _I, _I, _D, _D]
+        lib.eu_write_state.restype = _I
+        lib.eu_read_state.argtypes = [_P, ctypes.c_char_p, ctypes.POINTER(_I), ctypes.POINTER(_I),
+                                      ctypes.POINTER(_D), ctypes.POINTER(_D)]
+        lib.eu_read_state.restype = _I
         lib.eu_chem_states.argtypes = [_P, ctypes.c_longlong, _P, _P, _P, _P, _P]
         lib.eu_chem_advance.argtypes = [_P, ctypes.c_longlong, _P, _P, _P, _P, _P]
         lib.eu_set_learned.argtypes = [_P, _P, ctypes.POINTER(LearnedConfig)]
@@ -293,6 +298,18 @@ class Solver:
                             *[None if v is None else v.ctypes.data for v in keep])
         self._model = model
         self._check(library().eu_set_learned(self.h, model.h, ctypes.byref(cfg)), "set_learned")
+
+    def write_state(self, path, iteration=0, num=0, final_time=0.0, dt=0.0):
+        """EU3D_STATE_V1_LE dump of the current state (the reference's format)."""
+        self._check(library().eu_write_state(self.h, str(path).encode(), int(iteration), int(num),
+                                             float(final_time), float(dt)), "write_state")
+
+    def read_state(self, path):
+        """Restart from an EU3D_STATE_V1_LE dump; returns (iteration, num, final_time, dt)."""
+        it, num, t, dt = _I(), _I(), _D(), _D()
+        self._check(library().eu_read_state(self.h, str(path).encode(), ctypes.byref(it), ctypes.byref(num),
+                                            ctypes.byref(t), ctypes.byref(dt)), "read_state")
+        return it.value, num.value, t.value, dt.value
 
     def device_info(self):
         stream = _P()

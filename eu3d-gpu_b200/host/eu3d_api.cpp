@@ -46,6 +46,7 @@ struct eu_handle {
     LearnedParams lp{};
     long long lp_capacity = 0;
     int *h_counts = nullptr; // pinned [2]
+    int heavy_blocks = 0;    // persistent grid of the warp-per-cell kinetics
     std::string err;
 };
 
@@ -175,6 +176,10 @@ eu_status install_mechanism(eu_handle *h, const MechanismTables &m)
         if ((s = dalloc(h, &h->st.cms, size_t(ns) * n3)) != EU_OK) return s;
     if ((s = dalloc(h, &h->st.counters, size_t(kCntCount))) != EU_OK) return s;
     if ((s = dalloc(h, &h->d_scratch, size_t(n3))) != EU_OK) return s;
+    if (h->cfg.precision == EU_PREC_MIXED) {
+        if ((s = dalloc(h, &h->st.heavy, size_t(2) + size_t(h->ni) * h->nj * h->nk)) != EU_OK) return s;
+        CK(h, cudaMemsetAsync(h->st.heavy, 0, 2 * sizeof(int), h->stream));
+    }
     CK(h, cudaMemsetAsync(h->st.prim, 0, size_t(7 + ns) * n3 * sizeof(double), h->stream));
     if (h->st.prim32)
         CK(h, cudaMemsetAsync(h->st.prim32, 0, size_t(7 + ns) * n3 * sizeof(float), h->stream));
@@ -362,6 +367,10 @@ eu_status eu_create(const eu_config *cfg, eu_handle **out)
             eu_destroy(h);
             return EU_ERR_CUDA;
         }
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg->device) != cudaSuccess || sms < 1)
+        sms = 1;
+    h->heavy_blocks = 4 * sms; // 4 blocks of 4 warps per SM, each warp a cell at a time
     eu_status s;
     if ((s = dalloc(h, &h->d_xyz, size_t(h->nx + h->ny + h->nz))) != EU_OK ||
         (s = dalloc(h, &h->d_dt, size_t(1))) != EU_OK) {
@@ -776,12 +785,19 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
         CK(h, L.flux_update(a));
         if (prof) CK(h, cudaEventRecord(h->pev[2], h->stream));
         launches += 2;
+        const bool heavy = h->st.heavy && (learned || react);
+        if (heavy)
+            CK(h, cudaMemsetAsync(h->st.heavy, 0, 2 * sizeof(int), h->stream));
         if (learned) {
             eu_status ls = learned_chemistry(h, a, L, &reacting, &launches);
             if (ls != EU_OK)
                 return ls;
         } else {
             CK(h, L.recover_react(a, react));
+            ++launches;
+        }
+        if (heavy) { // warp-per-cell kinetics of the cells deferred above
+            CK(h, L.react_heavy(a, h->heavy_blocks));
             ++launches;
         }
         if (prof) {
@@ -878,6 +894,172 @@ eu_status eu_get_field(eu_handle *h, const char *name, double *out)
             return EU_OK;
         }
     return fail(h, EU_ERR_INVALID_ARGUMENT, "unknown field %s", name);
+}
+
+// ------------------------------------------------------------ state dumps
+// The reference's EU3D_STATE_V1_LE dump (Euler::Output, src/Euler.cpp:1540-1598):
+// a text header "EU3D_STATE_V1_LE", one line of sizes and times (17 significant
+// digits), one line of column names, then one row of 22 + 5 ns little-endian
+// doubles per interior node in (i, j, k) order, k fastest. Written here as the
+// single rank of a 1 x 1 x 1 decomposition.
+
+namespace {
+const char *kDumpMagic = "EU3D_STATE_V1_LE";
+const char *kDumpFixed[17] = {"X", "Y", "Z", "D", "T", "U", "V", "W", "E", "Wav", "Rgas", "Cp", "P", "H", "Gamma",
+                              "C", "Ma"};
+
+std::string dump_columns(int ns)
+{
+    std::string line;
+    for (int f = 0; f < 17; ++f) line += (f ? " " : "") + std::string(kDumpFixed[f]);
+    for (const char *field : {"Di", "Yi", "Mc"})
+        for (int n = 0; n < ns; ++n) line += " " + std::string(field) + std::to_string(n);
+    for (int n = 0; n < ns + 4; ++n) line += " CS" + std::to_string(n);
+    for (int n = 0; n < ns; ++n) line += " CMS" + std::to_string(n);
+    return line + " Nchem";
+}
+} // namespace
+
+eu_status eu_write_state(eu_handle *h, const char *path, int iteration, int num, double final_time, double dt)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!path)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "null path");
+    if (!h->has_mech || !h->has_state)
+        return fail(h, EU_ERR_NOT_READY, "no state");
+    const int ns = h->mech.ns;
+    const long long n3 = h->n3;
+    // every column as haloed planes, in the dump's order
+    std::vector<std::vector<double>> cols;
+    auto field = [&](const char *name, int planes) -> eu_status {
+        std::vector<double> v(size_t(planes) * n3);
+        eu_status st = eu_get_field(h, name, v.data());
+        if (st != EU_OK)
+            return st;
+        for (int p = 0; p < planes; ++p) cols.emplace_back(v.begin() + p * n3, v.begin() + (p + 1) * n3);
+        return EU_OK;
+    };
+    const char *plane1[14] = {"D", "T", "U", "V", "W", "E", "Wav", "Rgas", "Cp", "P", "H", "Gamma", "C", "Ma"};
+    for (const char *f : plane1) {
+        eu_status st = field(f, 1);
+        if (st != EU_OK)
+            return st;
+    }
+    for (const char *f : {"Di", "Yi", "Mc"}) {
+        eu_status st = field(f, ns);
+        if (st != EU_OK)
+            return st;
+    }
+    eu_status st = field("CS", ns + 4);
+    if (st == EU_OK && h->st.cms)
+        st = field("CMS", ns);
+    else if (st == EU_OK) // no recorded sources: the reference's CMS array holds zeros until written
+        for (int p = 0; p < ns; ++p) cols.emplace_back(size_t(n3), 0.0);
+    if (st == EU_OK)
+        st = field("Nchem", 1);
+    if (st != EU_OK)
+        return st;
+    std::FILE *f = std::fopen(path, "wb");
+    if (!f)
+        return fail(h, EU_ERR_IO, "cannot open %s for writing", path);
+    // header: NS, total_n*, local n* (one rank: the same), rank coordinates 0 0 0,
+    // blocks 1 1 1, rank 0 of 1, iteration, output number, time, dt
+    std::fprintf(f, "%s\n%d %d %d %d %d %d %d 0 0 0 1 1 1 0 1 %d %d %.17g %.17g\n%s\n", kDumpMagic, ns, h->ni, h->nj,
+                 h->nk, h->ni, h->nj, h->nk, iteration, num, final_time, dt, dump_columns(ns).c_str());
+    const int ncols = 22 + 5 * ns;
+    std::vector<double> row(ncols);
+    bool ok = true;
+    for (int i = h->bc; i < h->bc + h->ni && ok; ++i)
+        for (int j = h->bc; j < h->bc + h->nj && ok; ++j)
+            for (int k = h->bc; k < h->bc + h->nk; ++k) {
+                const long long c = (static_cast<long long>(i) * h->ny + j) * h->nz + k;
+                row[0] = h->x[i];
+                row[1] = h->y[j];
+                row[2] = h->z[k];
+                // D T U V W E Wav Rgas Cp P H Gamma C Ma
+                for (int q = 0; q < 14; ++q) row[3 + q] = cols[q][c];
+                for (int q = 14; q < (int)cols.size(); ++q) row[3 + q] = cols[q][c];
+                if (std::fwrite(row.data(), sizeof(double), ncols, f) != size_t(ncols)) {
+                    ok = false;
+                    break;
+                }
+            }
+    if (std::fclose(f) != 0 || !ok)
+        return fail(h, EU_ERR_IO, "writing %s failed", path);
+    return EU_OK;
+}
+
+eu_status eu_read_state(eu_handle *h, const char *path, int *iteration, int *num, double *final_time, double *dt)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!path)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "null path");
+    if (!h->has_mech)
+        return fail(h, EU_ERR_NOT_READY, "load a mechanism first");
+    std::FILE *f = std::fopen(path, "rb");
+    if (!f)
+        return fail(h, EU_ERR_IO, "cannot open %s", path);
+    char magic[64] = {0};
+    int v[17];
+    double t = 0, d = 0;
+    const int ns = h->mech.ns;
+    bool ok = std::fgets(magic, sizeof magic, f) && std::strncmp(magic, kDumpMagic, std::strlen(kDumpMagic)) == 0;
+    ok = ok && std::fscanf(f, "%d %d %d %d %d %d %d %d %d %d %d %d %d %d %d %d %d %lf %lf", &v[0], &v[1], &v[2],
+                           &v[3], &v[4], &v[5], &v[6], &v[7], &v[8], &v[9], &v[10], &v[11], &v[12], &v[13], &v[14],
+                           &v[15], &v[16], &t, &d) == 19;
+    // rest of the sizes line, then the column line
+    int ch = 0;
+    while (ok && (ch = std::fgetc(f)) != '\n' && ch != EOF) {}
+    std::string columns;
+    while (ok && (ch = std::fgetc(f)) != '\n' && ch != EOF) columns += char(ch);
+    if (!ok || ch == EOF) {
+        std::fclose(f);
+        return fail(h, EU_ERR_IO, "%s is not an EU3D_STATE_V1_LE dump", path);
+    }
+    if (v[0] != ns || v[4] != h->ni || v[5] != h->nj || v[6] != h->nk || columns != dump_columns(ns)) {
+        std::fclose(f);
+        return fail(h, EU_ERR_INVALID_ARGUMENT,
+                    "%s holds ns %d and %d x %d x %d local nodes; the handle has ns %d and %d x %d x %d", path, v[0],
+                    v[4], v[5], v[6], ns, h->ni, h->nj, h->nk);
+    }
+    const long long n3 = h->n3;
+    const int ncols = 22 + 5 * ns;
+    std::vector<double> row(ncols), P(n3, 0.0), D(n3, 0.0), U(n3, 0.0), V(n3, 0.0), W(n3, 0.0), H(n3, 0.0),
+        G(n3, 0.0), T(n3, 0.0), E(n3, 0.0), Y(size_t(ns) * n3, 0.0), CS(size_t(ns + 4) * n3, 0.0);
+    for (int i = h->bc; i < h->bc + h->ni && ok; ++i)
+        for (int j = h->bc; j < h->bc + h->nj && ok; ++j)
+            for (int k = h->bc; k < h->bc + h->nk; ++k) {
+                if (std::fread(row.data(), sizeof(double), ncols, f) != size_t(ncols)) {
+                    ok = false;
+                    break;
+                }
+                const long long c = (static_cast<long long>(i) * h->ny + j) * h->nz + k;
+                D[c] = row[3];
+                T[c] = row[4];
+                U[c] = row[5];
+                V[c] = row[6];
+                W[c] = row[7];
+                E[c] = row[8];
+                P[c] = row[12];
+                H[c] = row[13];
+                G[c] = row[14];
+                for (int s = 0; s < ns; ++s) Y[s * n3 + c] = row[17 + ns + s];
+                for (int q = 0; q < ns + 4; ++q) CS[q * n3 + c] = row[17 + 3 * ns + q];
+            }
+    std::fclose(f);
+    if (!ok)
+        return fail(h, EU_ERR_IO, "%s ends before its last node", path);
+    eu_status st = eu_set_state(h, CS.data(), T.data(), E.data(), P.data(), D.data(), U.data(), V.data(), W.data(),
+                                H.data(), G.data(), Y.data());
+    if (st != EU_OK)
+        return st;
+    if (iteration) *iteration = v[15];
+    if (num) *num = v[16];
+    if (final_time) *final_time = t;
+    if (dt) *dt = d;
+    return EU_OK;
 }
 
 eu_status eu_sync(eu_handle *h)

@@ -176,6 +176,18 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats);
  * (1 plane, as doubles). Synchronises the handle's stream. */
 eu_status eu_get_field(eu_handle *h, const char *name, double *host_out);
 
+/* Write the solution in the reference's EU3D_STATE_V1_LE dump format
+ * (Euler::Output with EU3D_DUMP_STATE=1, src/Euler.cpp:1540-1598): header line,
+ * sizes/times line, column names, then 22 + 5 ns little-endian doubles per
+ * interior node, (i, j, k) order with k fastest, as rank 0 of a 1 x 1 x 1
+ * decomposition. CMS columns are zeros unless cfg.record_sources. */
+eu_status eu_write_state(eu_handle *h, const char *path, int iteration, int num, double final_time, double dt);
+/* Restart from such a dump (one rank's file whose local sizes and ns match the
+ * handle): the conserved, thermodynamic and primitive fields are injected as by
+ * eu_set_state; the header's iteration, output number, time and dt are returned
+ * (NULL to skip). */
+eu_status eu_read_state(eu_handle *h, const char *path, int *iteration, int *num, double *final_time, double *dt);
+
 /* Wait for all work queued on the handle. */
 eu_status eu_sync(eu_handle *h);
 

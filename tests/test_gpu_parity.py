@@ -159,3 +159,29 @@ def test_deterministic(gpu):
     a.step(10, float(z["dt"]))
     b.step(10, float(z["dt"]))
     assert n_unequal(a.get("CS"), b.get("CS")) == 0
+
+
+def test_mixed_stiff_heavy_cells_match_fp64(gpu):
+    """Igniting gas in mixed precision: cells whose predicted Nchem exceeds 16
+    are advanced one warp per cell (k_react_heavy). Over 8 steps of a hot
+    2H2+O2/N2 block (1300-2600 K, dt 2e-8 s) the run must reach such cells and
+    stay within a species L1 (mean over cells of sum_s |dY_s|) of 1e-4 and a
+    relative temperature error of 1e-4 of the FP64 stiff run."""
+    ni, nj, nk = 24, 8, 8
+    ext = (0.0, 0.006, 0.0, 0.002, 0.0, 0.002)
+    mech = gpu.parse_mechanism(cases.MECH_JA919, cases.THERMO)
+    prim = cases.hot_reacting_block(ni + 4, nj + 4, nk + 4, mech["mw"], mech["ns"])
+    out, peak = {}, {}
+    for precision in ("fp64", "mixed"):
+        s = gpu.Solver(ni, nj, nk, ext, precision=precision, arith="fast")
+        s.set_mechanism(mech)
+        s.set_primitive(*prim)
+        peak[precision] = 0
+        for _ in range(8):
+            peak[precision] = max(peak[precision], s.step(1, 2e-8)["max_nchem"])
+        out[precision] = (interior(s.get("Yi")), interior(s.get("T")))
+        s.close()
+    assert peak["mixed"] > 16, peak
+    l1 = np.abs(out["mixed"][0] - out["fp64"][0]).sum(axis=0)
+    terr = np.abs(out["mixed"][1] - out["fp64"][1]) / out["fp64"][1]
+    assert l1.mean() <= 1e-4 and terr.max() <= 1e-4, (l1.mean(), l1.max(), terr.max(), peak)

@@ -1,0 +1,93 @@
+"""EU3D_STATE_V1_LE state dumps (the reference's Euler::Output format,
+src/Euler.cpp:1540-1598), written and read through the C ABI.
+
+The dump is parsed here independently with numpy, following the reference's
+writer: a header line, a line of 17 integers and two doubles (NS, total and
+local node counts, rank coordinates, block counts, rank, rank count,
+iteration, output number, time, dt), a line of column names, then 22 + 5 NS
+little-endian doubles per interior node in (i, j, k) order, k fastest.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import eu3d_cases as cases
+from helpers import golden, interior, n_unequal
+
+pytestmark = pytest.mark.gpu
+
+FIXED = ["X", "Y", "Z", "D", "T", "U", "V", "W", "E", "Wav", "Rgas", "Cp", "P", "H", "Gamma", "C", "Ma"]
+
+
+def parse_dump(path):
+    with open(path, "rb") as f:
+        magic = f.readline().decode().strip()
+        sizes = f.readline().decode().split()
+        names = f.readline().decode().split()
+        rows = np.frombuffer(f.read(), dtype="<f8")
+    head = [int(v) for v in sizes[:17]] + [float(v) for v in sizes[17:]]
+    return magic, head, names, rows.reshape(-1, len(names))
+
+
+def bubble(gpu):
+    z = golden("bubble_25x13x13_s20.npz")
+    s = gpu.Solver(int(z["ni"]), int(z["nj"]), int(z["nk"]), tuple(z["extent"]), arith="strict",
+                   record_sources=True)
+    s.load_mechanism(cases.MECH_JA919, cases.THERMO)
+    s.set_primitive(*[z[f"prim_{k}"] for k in "PTUVWY"])
+    return s, z
+
+
+def test_dump_layout_matches_the_reference_writer(gpu):
+    s, z = bubble(gpu)
+    ni, nj, nk = int(z["ni"]), int(z["nj"]), int(z["nk"])
+    s.step(5, float(z["dt"]))
+    path = os.path.join(tempfile.mkdtemp(), "state_check_5_rank0.bin")
+    s.write_state(path, iteration=5, num=5, final_time=5 * float(z["dt"]), dt=float(z["dt"]))
+    magic, head, names, rows = parse_dump(path)
+    ns = 9
+    assert magic == "EU3D_STATE_V1_LE"
+    assert head[:17] == [ns, ni, nj, nk, ni, nj, nk, 0, 0, 0, 1, 1, 1, 0, 1, 5, 5]
+    assert head[17] == 5 * float(z["dt"]) and head[18] == float(z["dt"])
+    want = FIXED + [f"{f}{n}" for f in ("Di", "Yi", "Mc") for n in range(ns)] + \
+        [f"CS{n}" for n in range(ns + 4)] + [f"CMS{n}" for n in range(ns)] + ["Nchem"]
+    assert names == want and rows.shape == (ni * nj * nk, 22 + 5 * ns)
+    col = {n: q for q, n in enumerate(names)}
+    x, y, zc = s.nodes()
+    X, Y, Z = np.meshgrid(x[2:-2], y[2:-2], zc[2:-2], indexing="ij")
+    for name, grid in (("X", X), ("Y", Y), ("Z", Z)):
+        assert np.array_equal(rows[:, col[name]], grid.ravel()), name
+    for name in ["D", "T", "U", "V", "W", "E", "Wav", "Rgas", "Cp", "P", "H", "Gamma", "C", "Ma", "Nchem"]:
+        assert np.array_equal(rows[:, col[name]], interior(s.get(name)).ravel()), name
+    for field, planes in (("Di", ns), ("Yi", ns), ("Mc", ns), ("CS", ns + 4), ("CMS", ns)):
+        got = interior(s.get(field))
+        for n in range(planes):
+            assert np.array_equal(rows[:, col[f"{field}{n}"]], got[n].ravel()), (field, n)
+
+
+def test_restart_from_dump_continues_bitwise(gpu):
+    a, z = bubble(gpu)
+    dt = float(z["dt"])
+    a.step(5, dt)
+    path = os.path.join(tempfile.mkdtemp(), "state.bin")
+    a.write_state(path, iteration=5, num=1, final_time=5 * dt, dt=dt)
+    b, _ = bubble(gpu)
+    assert b.read_state(path) == (5, 1, 5 * dt, dt)
+    a.step(5, dt)
+    b.step(5, dt)
+    for f in ["CS", "T", "E", "Nchem"]:
+        assert n_unequal(interior(a.get(f)), interior(b.get(f))) == 0, f
+
+
+def test_dump_of_another_size_is_refused(gpu):
+    a, z = bubble(gpu)
+    a.step(1, float(z["dt"]))
+    path = os.path.join(tempfile.mkdtemp(), "state.bin")
+    a.write_state(path)
+    other = gpu.Solver(int(z["ni"]) + 1, int(z["nj"]), int(z["nk"]), tuple(z["extent"]))
+    other.load_mechanism(cases.MECH_JA919, cases.THERMO)
+    with pytest.raises(gpu.EU3DError) as e:
+        other.read_state(path)
+    assert e.value.name == "EU_ERR_INVALID_ARGUMENT"
