@@ -498,51 +498,82 @@ __device__ __forceinline__ R minmod(R r)
 // L > 0 the reference's slope term 0.25((1-k) min(L,1) + (1+k) min(1/L,1) L) A0
 // equals 0.5 min(L,1) A0 (k = 1/3); for L <= 0 it is 0. L is formed with a
 // Newton-refined reciprocal. Results agree to a few units in the last place.
+// The 1e-12 guard is kept in every form: it flattens the slopes of fields
+// whose differences are below it (trace species), so the first-order value
+// the reference takes there is kept.
+
+// Slope term t of one side: the left state is f0 + t(A0, A1), the right state
+// f1 - t(A2, A1).
+template <typename R, bool kStrict>
+__device__ __forceinline__ R muscl_slope(R a, R A1)
+{
+    if (kStrict) {
+        const R kk = R(1.0) / R(3.0);
+        const R L = A1 / (a + R(1e-12));
+        const R L1 = minmod(L), L2 = minmod(R(1.0) / L);
+        return R(0.25) * ((R(1.0) - kk) * L1 + (R(1) + kk) * L2 * L) * a;
+    } else {
+        const R L = div_fast(A1, a + R(1e-12));
+        return L > R(0) ? R(0.5) * a * fmin(L, R(1)) : R(0);
+    }
+}
+
 template <typename R, bool kStrict>
 __device__ __forceinline__ void muscl(R fm1, R f0, R f1, R f2, R &left, R &right)
 {
     const R A0 = f0 - fm1;
     const R A1 = f1 - f0;
     const R A2 = f2 - f1;
-    if (kStrict) {
-        const R kk = R(1.0) / R(3.0);
-        const R L = A1 / (A0 + R(1e-12));
-        const R Rr = A1 / (A2 + R(1e-12));
-        const R L1 = minmod(L), L2 = minmod(R(1.0) / L), R1 = minmod(Rr), R2 = minmod(R(1.0) / Rr);
-        left = f0 + R(0.25) * ((R(1.0) - kk) * L1 + (R(1) + kk) * L2 * L) * A0;
-        right = f1 - R(0.25) * ((R(1.0) - kk) * R1 + (R(1) + kk) * R2 * Rr) * A2;
-    } else {
-        const R L = div_fast(A1, A0 + R(1e-12));
-        const R Rr = div_fast(A1, A2 + R(1e-12));
-        left = f0 + (L > R(0) ? R(0.5) * A0 * fmin(L, R(1)) : R(0));
-        right = f1 - (Rr > R(0) ? R(0.5) * A2 * fmin(Rr, R(1)) : R(0));
-    }
+    left = f0 + muscl_slope<R, kStrict>(A0, A1);
+    right = f1 - muscl_slope<R, kStrict>(A2, A1);
 }
 
-// AUSM+ flux of one face (src/Flowfield.cpp:1811-1930) for direction DIR
-// (0: x, 1: y, 2: z). lr holds the reconstructed left/right primitives
-// {P, D, U, V, W, H, Gamma} and species. Output F[NS+4] in FP64.
-template <int NS, int DIR, typename R, bool kStrict, typename FOut>
-__device__ __forceinline__ void ausm(const R (&L)[7], const R (&Rt)[7], const R (&YL)[NS], const R (&YR)[NS],
-                                     FOut (&F)[NS + 4])
+// Only the upwind side of the face: the left state when up, else the right.
+// The same expression as that side of muscl(), so the same value.
+template <typename R, bool kStrict>
+__device__ __forceinline__ R muscl_upwind(bool up, R fm1, R f0, R f1, R f2)
 {
-    const R PL = L[kP], PR = Rt[kP], DL = L[kD], DR = Rt[kD];
+    const R A1 = f1 - f0;
+    const R a = up ? f0 - fm1 : f2 - f1;
+    const R t = muscl_slope<R, kStrict>(a, A1);
+    return up ? f0 + t : f1 - t;
+}
+
+// MUSCL reconstruction and AUSM+ flux of one face (src/Flowfield.cpp:1794-1930)
+// for direction DIR (0: x, 1: y, 2: z). get(f, p) returns stencil point p
+// (0..3: cells m-1, m, m+1, m+2 across the face m+1/2) of primitive f.
+//
+// AUSM+ reads both reconstructed sides only of p, rho, gamma and the normal
+// velocity (sound speeds, Mach numbers, pressure split). Every other flux
+// term takes the upwind side (VI >= 0: left, src/Flowfield.cpp:1870): the two
+// tangential velocities, H and the species. Those twelve quantities are
+// reconstructed on the upwind side alone, with the same expression as
+// before, so the flux is the same as with both sides formed.
+template <int NS, int DIR, typename R, bool kStrict, typename FOut, class Get>
+__device__ __forceinline__ void face_ausm(Get get, FOut (&F)[NS + 4])
+{
+    constexpr int kN = kU + DIR;
+    R PL, PR, DL, DR, UnL, UnR, GaL, GaR;
+    muscl<R, kStrict>(get(kP, 0), get(kP, 1), get(kP, 2), get(kP, 3), PL, PR);
+    muscl<R, kStrict>(get(kD, 0), get(kD, 1), get(kD, 2), get(kD, 3), DL, DR);
+    muscl<R, kStrict>(get(kN, 0), get(kN, 1), get(kN, 2), get(kN, 3), UnL, UnR);
+    muscl<R, kStrict>(get(kG, 0), get(kG, 1), get(kG, 2), get(kG, 3), GaL, GaR);
     R CL, CR, CI, MaL, MaR;
     if (kStrict) {
-        CL = sqrt(L[kG] * PL / DL);
-        CR = sqrt(Rt[kG] * PR / DR);
+        CL = sqrt(GaL * PL / DL);
+        CR = sqrt(GaR * PR / DR);
         CI = R(0.5) * (CL + CR);
-        MaL = L[kU + DIR] / CI;
-        MaR = Rt[kU + DIR] / CI;
+        MaL = UnL / CI;
+        MaR = UnR / CI;
     } else {
         // c = sqrt(g p / rho) = (g p) / sqrt(g p rho)
-        const R gpL = L[kG] * PL, gpR = Rt[kG] * PR;
+        const R gpL = GaL * PL, gpR = GaR * PR;
         CL = gpL * rsqrt(gpL * DL);
         CR = gpR * rsqrt(gpR * DR);
         CI = R(0.5) * (CL + CR);
         const R inv = div_fast(R(1), CI);
-        MaL = L[kU + DIR] * inv;
-        MaR = Rt[kU + DIR] * inv;
+        MaL = UnL * inv;
+        MaR = UnR * inv;
     }
     R B1, G1, B2, G2;
     if (fabs(MaL) < R(1.0)) {
@@ -551,7 +582,8 @@ __device__ __forceinline__ void ausm(const R (&L)[7], const R (&Rt)[7], const R 
         G1 = R(0.25) * (a * a) * (R(2.0) - MaL) + R(3.0) / R(16.0) * MaL * (t * t);
     } else {
         B1 = R(0.5) * (MaL + fabs(MaL));
-        G1 = B1 / MaL;
+        // B1 / MaL is exactly 1 (MaL >= 1) or 0 (MaL <= -1)
+        G1 = kStrict ? B1 / MaL : (MaL > R(0) ? R(1) : R(0));
     }
     if (fabs(MaR) < R(1.0)) {
         const R a = MaR - R(1.0), t = MaR * MaR - R(1.0);
@@ -559,22 +591,26 @@ __device__ __forceinline__ void ausm(const R (&L)[7], const R (&Rt)[7], const R 
         G2 = R(0.25) * (a * a) * (R(2.0) + MaR) - R(3.0) / R(16.0) * MaR * (t * t);
     } else {
         B2 = R(0.5) * (MaR - fabs(MaR));
-        G2 = B2 / MaR;
+        G2 = kStrict ? B2 / MaR : (MaR < R(0) ? R(1) : R(0));
     }
     const R MaI = B1 + B2;
     const R VI = MaI * CI;
     const bool up = VI >= R(0.0);
-    const R Du = up ? DL : DR, Uu = up ? L[kU] : Rt[kU], Vu = up ? L[kV] : Rt[kV], Wu = up ? L[kW] : Rt[kW],
-            Hu = up ? L[kH] : Rt[kH];
+    auto side = [&](int f) { return muscl_upwind<R, kStrict>(up, get(f, 0), get(f, 1), get(f, 2), get(f, 3)); };
+    const R Du = up ? DL : DR;
     const R m = VI * Du;
 #pragma unroll
-    for (int s = 0; s < NS; ++s) F[s] = FOut(m * (up ? YL[s] : YR[s]));
-    R mom[3] = {m * Uu, m * Vu, m * Wu};
+    for (int s = 0; s < NS; ++s) F[s] = FOut(m * side(kY0 + s));
+    R vel[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) vel[d] = (d == DIR) ? (up ? UnL : UnR) : side(kU + d);
+    const R Hu = side(kH);
+    R mom[3] = {m * vel[0], m * vel[1], m * vel[2]};
     mom[DIR] = mom[DIR] + G1 * PL + G2 * PR;
     F[NS + 0] = FOut(mom[0]);
     F[NS + 1] = FOut(mom[1]);
     F[NS + 2] = FOut(mom[2]);
-    F[NS + 3] = FOut(VI * (Du * Hu + R(0.5) * Du * (Uu * Uu + Vu * Vu + Wu * Wu)));
+    F[NS + 3] = FOut(VI * (Du * Hu + R(0.5) * Du * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2])));
 }
 
 } // namespace eu3d

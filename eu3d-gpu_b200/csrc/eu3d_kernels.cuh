@@ -72,9 +72,11 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
         src = cell_index(g, i, j, sk);
         sw = -1;
     }
+    // mixed precision keeps only the FP32 primitive planes current (the flux
+    // kernel's input); the FP64 path its FP64 planes
     double v[7 + NS];
 #pragma unroll
-    for (int f = 0; f < 7 + NS; ++f) v[f] = st.prim[f * n3 + src];
+    for (int f = 0; f < 7 + NS; ++f) v[f] = st.prim32 ? double(st.prim32[f * n3 + src]) : st.prim[f * n3 + src];
     v[kV] = sv * v[kV];
     v[kW] = sw * v[kW];
     const double T = st.T[src];
@@ -103,9 +105,10 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
     st.T[dst] = T;
 #pragma unroll
     for (int f = 0; f < 7 + NS; ++f) {
-        st.prim[f * n3 + dst] = v[f];
         if (st.prim32)
             st.prim32[f * n3 + dst] = float(v[f]);
+        else
+            st.prim[f * n3 + dst] = v[f];
     }
 }
 
@@ -117,18 +120,8 @@ template <int NS, int DIR, typename R, bool kStrict>
 __device__ __forceinline__ void face_flux(const R *__restrict__ prim, long long n3, long long c, long long stride,
                                           R (&F)[NS + 4])
 {
-    R L[7], Rt[7], YL[NS], YR[NS];
-#pragma unroll
-    for (int f = 0; f < 7; ++f) {
-        const R *a = prim + f * n3 + c;
-        muscl<R, kStrict>(__ldg(a - stride), __ldg(a), __ldg(a + stride), __ldg(a + 2 * stride), L[f], Rt[f]);
-    }
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-        const R *a = prim + (kY0 + s) * n3 + c;
-        muscl<R, kStrict>(__ldg(a - stride), __ldg(a), __ldg(a + stride), __ldg(a + 2 * stride), YL[s], YR[s]);
-    }
-    ausm<NS, DIR, R, kStrict, R>(L, Rt, YL, YR, F);
+    const R *a = prim + c - stride;
+    face_ausm<NS, DIR, R, kStrict, R>([&](int f, int p) { return __ldg(a + f * n3 + p * stride); }, F);
 }
 
 // Flux divergence and the Euler-explicit update (TimeAdv::EE, src/TimeAdv.cpp:42-56,
@@ -252,28 +245,13 @@ constexpr size_t tiled_flux_smem_bytes()
 template <int NS, int DIR, int DR, int DC, typename R, bool kStrict>
 __device__ __forceinline__ void tile_face_flux(const R (*sP)[kTileRows][kTileCols], int r, int c, R (&F)[NS + 4])
 {
-    R L[7], Rt[7], YL[NS], YR[NS];
-#pragma unroll
-    for (int f = 0; f < 7; ++f)
-        muscl<R, kStrict>(sP[f][r][c], sP[f][r + DR][c + DC], sP[f][r + 2 * DR][c + 2 * DC],
-                          sP[f][r + 3 * DR][c + 3 * DC], L[f], Rt[f]);
-#pragma unroll
-    for (int s = 0; s < NS; ++s)
-        muscl<R, kStrict>(sP[kY0 + s][r][c], sP[kY0 + s][r + DR][c + DC], sP[kY0 + s][r + 2 * DR][c + 2 * DC],
-                          sP[kY0 + s][r + 3 * DR][c + 3 * DC], YL[s], YR[s]);
-    ausm<NS, DIR, R, kStrict, R>(L, Rt, YL, YR, F);
+    face_ausm<NS, DIR, R, kStrict, R>([&](int f, int p) { return sP[f][r + p * DR][c + p * DC]; }, F);
 }
 
 template <int NS, typename R, bool kStrict>
 __device__ __forceinline__ void window_face_flux(const R (&w)[4][7 + NS], R (&F)[NS + 4])
 {
-    R L[7], Rt[7], YL[NS], YR[NS];
-#pragma unroll
-    for (int f = 0; f < 7; ++f) muscl<R, kStrict>(w[0][f], w[1][f], w[2][f], w[3][f], L[f], Rt[f]);
-#pragma unroll
-    for (int s = 0; s < NS; ++s)
-        muscl<R, kStrict>(w[0][kY0 + s], w[1][kY0 + s], w[2][kY0 + s], w[3][kY0 + s], YL[s], YR[s]);
-    ausm<NS, 0, R, kStrict, R>(L, Rt, YL, YR, F);
+    face_ausm<NS, 0, R, kStrict, R>([&](int f, int p) { return w[p][f]; }, F);
 }
 
 template <int NS, typename R, bool kStrict>
@@ -410,13 +388,27 @@ __global__ void __launch_bounds__(kTileK *kTileJ, 2)
         if (valid) {
             const long long c = col + i * sx;
             const double cx = -dt / (g.x[i] - g.x[i - 1]);
+            if (sizeof(R) == 4) {
+                // FP32 fluxes: the flux differences and their sum in FP32 (a
+                // difference of two FP32 values within a factor of two is exact),
+                // accumulated onto the FP64 conserved value
+                const float cx32 = float(cx), cy32 = float(cy), cz32 = float(cz);
 #pragma unroll
-            for (int q = 0; q < NV; ++q) {
-                const double rhs = cx * (double(Fp[q]) - double(Fm[q])) -
-                                   cy * (double(sG[q][ty + 1][tx]) - double(sG[q][ty][tx])) -
-                                   cz * (double(sQ[q][ty][tx + 1]) - double(sQ[q][ty][tx]));
-                st.cs[q * n3 + c] = sC[q][ty][tx] + rhs;
-                Fm[q] = Fp[q];
+                for (int q = 0; q < NV; ++q) {
+                    const float rhs = cx32 * float(Fp[q] - Fm[q]) - cy32 * float(sG[q][ty + 1][tx] - sG[q][ty][tx]) -
+                                      cz32 * float(sQ[q][ty][tx + 1] - sQ[q][ty][tx]);
+                    st.cs[q * n3 + c] = sC[q][ty][tx] + double(rhs);
+                    Fm[q] = Fp[q];
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < NV; ++q) {
+                    const double rhs = cx * (double(Fp[q]) - double(Fm[q])) -
+                                       cy * (double(sG[q][ty + 1][tx]) - double(sG[q][ty][tx])) -
+                                       cz * (double(sQ[q][ty][tx + 1]) - double(sQ[q][ty][tx]));
+                    st.cs[q * n3 + c] = sC[q][ty][tx] + rhs;
+                    Fm[q] = Fp[q];
+                }
             }
         }
 #pragma unroll
@@ -441,15 +433,16 @@ __device__ __forceinline__ void store_cell(const DevMech &m, const DevState &st,
     double P, H, G;
     finish_primitives<NS>(m, cell, P, H, G);
     const double v[7] = {P, cell.D, cell.U, cell.V, cell.W, H, G};
-#pragma unroll
-    for (int f = 0; f < 7; ++f) st.prim[f * n3 + c] = v[f];
-#pragma unroll
-    for (int s = 0; s < NS; ++s) st.prim[(kY0 + s) * n3 + c] = cell.Y[s];
-    if (st.prim32) {
+    if (st.prim32) { // mixed precision: the FP64 planes are formed on demand (k_materialize)
 #pragma unroll
         for (int f = 0; f < 7; ++f) st.prim32[f * n3 + c] = float(v[f]);
 #pragma unroll
         for (int s = 0; s < NS; ++s) st.prim32[(kY0 + s) * n3 + c] = float(cell.Y[s]);
+    } else {
+#pragma unroll
+        for (int f = 0; f < 7; ++f) st.prim[f * n3 + c] = v[f];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) st.prim[(kY0 + s) * n3 + c] = cell.Y[s];
     }
     if (kWriteCs) {
 #pragma unroll
@@ -610,12 +603,59 @@ __device__ __forceinline__ void load_recovered(const DevState &st, long long n3,
     double D = 0;
 #pragma unroll
     for (int s = 0; s < NS; ++s) D += cell.cs[s];
+    cell.D = D;
+#ifdef EU_EXACT_CHEM
 #pragma unroll
     for (int s = 0; s < NS; ++s) cell.Y[s] = cell.cs[s] / D;
-    cell.D = D;
     cell.U = cell.cs[NS + 0] / D;
     cell.V = cell.cs[NS + 1] / D;
     cell.W = cell.cs[NS + 2] / D;
+#else
+    const double invD = rcp_nr(D);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) cell.Y[s] = cell.cs[s] * invD;
+    cell.U = cell.cs[NS + 0] * invD;
+    cell.V = cell.cs[NS + 1] * invD;
+    cell.W = cell.cs[NS + 2] * invD;
+#endif
+}
+
+// Mixed precision keeps the FP64 primitive planes out of the timestep (the
+// FP32 planes feed the fluxes). This forms them on demand, for output: interior
+// nodes from the stored conserved state, T and E (the values the FP64 store
+// would have written), ghost nodes from the FP32 ghost planes.
+template <int NS>
+__global__ void __launch_bounds__(128) k_materialize(const __grid_constant__ DevMech m, const DevGrid g,
+                                                     const DevState st)
+{
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.n3)
+        return;
+    const long long n3 = g.n3;
+    const int k = int(c % g.nz), j = int((c / g.nz) % g.ny), i = int(c / ((long long)g.nz * g.ny));
+    const bool interior = i >= g.bc && i < g.bc + g.ni && j >= g.bc && j < g.bc + g.nj && k >= g.bc &&
+                          k < g.bc + g.nk;
+    if (!interior) {
+#pragma unroll
+        for (int f = 0; f < 7 + NS; ++f) st.prim[f * n3 + c] = double(st.prim32[f * n3 + c]);
+        return;
+    }
+    CellState<NS> cell;
+    load_recovered<NS>(st, n3, c, cell);
+    double P, H, G;
+    finish_primitives<NS>(m, cell, P, H, G);
+    const double v[7] = {P, cell.D, cell.U, cell.V, cell.W, H, G};
+#pragma unroll
+    for (int f = 0; f < 7; ++f) st.prim[f * n3 + c] = v[f];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) st.prim[(kY0 + s) * n3 + c] = cell.Y[s];
+}
+
+// FP32 copy of the FP64 primitive planes (state upload in mixed precision).
+__global__ void k_to_f32(const double *__restrict__ src, float *__restrict__ dst, long long n)
+{
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        dst[t] = float(src[t]);
 }
 
 // Post-advection state recovery (Flowfield::Update_after_Adv ->
@@ -653,7 +693,7 @@ __global__ void __launch_bounds__(128) k_recover_react(const __grid_constant__ D
 // appended to the learned queue (warp-aggregated atomics), the others are
 // final. Every cell's recovered state is stored.
 template <int NS>
-__global__ void __launch_bounds__(128) k_recover_classify(const __grid_constant__ DevMech m, const DevGrid g,
+__global__ void __launch_bounds__(128, 5) k_recover_classify(const __grid_constant__ DevMech m, const DevGrid g,
                                                           const DevState st, LearnedParams lp)
 {
     const long long ncell = (long long)g.ni * g.nj * g.nk;

@@ -3,6 +3,8 @@
 // eu3d_kernels_fast.cu, with EU3D_NS naming the namespace.
 #pragma once
 
+#include <algorithm>
+
 #include "eu3d_kernels.cuh"
 #include "eu3d_launch.hpp"
 
@@ -105,6 +107,15 @@ cudaError_t derived_t(const LaunchArgs &a, int which, double *out)
 }
 
 template <int NS, int NR>
+cudaError_t materialize_t(const LaunchArgs &a)
+{
+    if (!a.st.prim32)
+        return cudaSuccess;
+    k_materialize<NS><<<dim3(unsigned((a.g.n3 + 127) / 128)), 128, 0, a.stream>>>(*a.mech, a.g, a.st);
+    return cudaGetLastError();
+}
+
+template <int NS, int NR>
 cudaError_t classify_t(const LaunchArgs &a, const LearnedParams &lp)
 {
     const long long n = (long long)a.g.ni * a.g.nj * a.g.nk;
@@ -195,6 +206,14 @@ cudaError_t launch_boundary(const LaunchArgs &a) { EU3D_DISPATCH(boundary_t, a) 
 cudaError_t launch_flux_update(const LaunchArgs &a) { EU3D_DISPATCH(flux_t, a) }
 cudaError_t launch_recover_react(const LaunchArgs &a, bool react) { EU3D_DISPATCH(react_t, a, react) }
 cudaError_t launch_derived(const LaunchArgs &a, int which, double *out) { EU3D_DISPATCH(derived_t, a, which, out) }
+cudaError_t launch_materialize(const LaunchArgs &a) { EU3D_DISPATCH(materialize_t, a) }
+cudaError_t launch_to_f32(const double *src, float *dst, long long n, cudaStream_t s)
+{
+    if (n <= 0)
+        return cudaSuccess;
+    k_to_f32<<<dim3(unsigned(std::min<long long>((n + 255) / 256, 148LL * 16))), 256, 0, s>>>(src, dst, n);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_recover_classify(const LaunchArgs &a, const LearnedParams &lp) { EU3D_DISPATCH(classify_t, a, lp) }
 cudaError_t launch_learned_features(const LaunchArgs &a, const LearnedParams &lp, int nq)
@@ -227,7 +246,8 @@ cudaError_t launch_set_value(double *dst, double v, cudaStream_t s)
 
 const Launchers launchers = {&launch_boundary,         &launch_flux_update,      &launch_recover_react,
                              &launch_derived,          &launch_recover_classify, &launch_learned_features,
-                             &launch_learned_apply,    &launch_react_queue,      &launch_react_heavy};
+                             &launch_learned_apply,    &launch_react_queue,      &launch_react_heavy,
+                             &launch_materialize};
 
 #undef EU3D_DISPATCH
 

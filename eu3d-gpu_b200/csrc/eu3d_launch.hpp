@@ -34,6 +34,7 @@ struct Launchers {
     cudaError_t (*learned_apply)(const LaunchArgs &a, const LearnedParams &lp, int nq);
     cudaError_t (*react_queue)(const LaunchArgs &a, const int *queue, const int *count, int nq, int counter);
     cudaError_t (*react_heavy)(const LaunchArgs &a, int blocks);
+    cudaError_t (*materialize)(const LaunchArgs &a);
 };
 
 #define EU3D_DECLARE_LAUNCHERS(NSP)                                                                \
@@ -53,6 +54,8 @@ struct Launchers {
     cudaError_t launch_chem_samples(const LaunchArgs &a, long long n, double *cs, double *T,       \
                                     double *E, const double *dt, int *nchem);                      \
     cudaError_t launch_react_heavy(const LaunchArgs &a, int blocks);                               \
+    cudaError_t launch_materialize(const LaunchArgs &a);                                           \
+    cudaError_t launch_to_f32(const double *src, float *dst, long long n, cudaStream_t s);          \
     extern const Launchers launchers;                                                              \
     }
 

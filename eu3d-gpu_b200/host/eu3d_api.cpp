@@ -47,6 +47,9 @@ struct eu_handle {
     long long lp_capacity = 0;
     int *h_counts = nullptr; // pinned [2]
     int heavy_blocks = 0;    // persistent grid of the warp-per-cell kinetics
+    // mixed precision: the timestep keeps only the FP32 primitive planes
+    // current; the FP64 ones are formed on demand (k_materialize) for output
+    bool prim_stale = false;
     std::string err;
 };
 
@@ -498,17 +501,11 @@ eu_status eu_set_state(eu_handle *h, const double *cs, const double *T, const do
     CK(h, cudaMemcpyAsync(h->st.cs, cs, (ns + 4) * b, cudaMemcpyHostToDevice, h->stream));
     CK(h, cudaMemcpyAsync(h->st.T, T, b, cudaMemcpyHostToDevice, h->stream));
     CK(h, cudaMemcpyAsync(h->st.E, E, b, cudaMemcpyHostToDevice, h->stream));
-    if (h->st.prim32) {
-        std::vector<float> f32(size_t(7 + ns) * n3);
-        for (int f = 0; f < 7; ++f)
-            for (long long c = 0; c < n3; ++c) f32[f * n3 + c] = float(planes[f][c]);
-        for (long long c = 0; c < ns * n3; ++c) f32[7 * n3 + c] = float(Y[c]);
-        CK(h, cudaMemcpyAsync(h->st.prim32, f32.data(), f32.size() * sizeof(float), cudaMemcpyHostToDevice,
-                              h->stream));
-        CK(h, cudaStreamSynchronize(h->stream));
-    }
+    if (h->st.prim32) // the FP32 planes the mixed-precision fluxes read, converted on the device
+        CK(h, strict::launch_to_f32(h->st.prim, h->st.prim32, (long long)(7 + ns) * n3, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
     h->has_state = true;
+    h->prim_stale = false;
     return EU_OK;
 }
 
@@ -777,6 +774,8 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
     CK(h, cudaMemsetAsync(h->st.counters, 0, kCntCount * sizeof(unsigned long long), h->stream));
     CK(h, strict::launch_set_value(h->d_dt, dt, h->stream));
     ++launches;
+    if (h->st.prim32 && nsteps > 0)
+        h->prim_stale = true;
     for (int n = 0; n < nsteps; ++n) {
         CK(h, cudaMemsetAsync(h->st.counters, 0, kCntPerStep * sizeof(unsigned long long), h->stream));
         if (prof) CK(h, cudaEventRecord(h->pev[0], h->stream));
@@ -850,6 +849,11 @@ eu_status eu_get_field(eu_handle *h, const char *name, double *out)
     const size_t b = size_t(n3) * sizeof(double);
     const std::string n(name);
     const char *prim_names[7] = {"P", "D", "U", "V", "W", "H", "Gamma"};
+    if (h->prim_stale && n != "T" && n != "E" && n != "CS" && n != "Di" && n != "Mc" && n != "CMS" && n != "Nchem") {
+        const LaunchArgs a = launch_args(h);
+        CK(h, flavour(h).materialize(a));
+        h->prim_stale = false;
+    }
     for (int f = 0; f < 7; ++f)
         if (n == prim_names[f]) {
             CK(h, cudaMemcpyAsync(out, h->st.prim + f * n3, b, cudaMemcpyDeviceToHost, h->stream));
