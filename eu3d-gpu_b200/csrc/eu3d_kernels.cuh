@@ -739,21 +739,22 @@ template <int NS>
 __global__ void k_learned_features(const __grid_constant__ DevMech m, const DevGrid g, const DevState st,
                                    LearnedParams lp, const double *__restrict__ dt_dev)
 {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= lp.counts[0])
-        return;
-    const long long n3 = g.n3, c = lp.queue[q];
-    CellState<NS> cell;
-    load_recovered<NS>(st, n3, c, cell);
-    float *f = lp.feat + (long long)q * (NS + 3);
-    double inv_w = 0;
+    // a fixed grid walks the queue (its length is read on the device)
+    const int nq = lp.counts[0];
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        const long long n3 = g.n3, c = lp.queue[q];
+        CellState<NS> cell;
+        load_recovered<NS>(st, n3, c, cell);
+        float *f = lp.feat + (long long)q * (NS + 3);
+        double inv_w = 0;
 #pragma unroll
-    for (int s = 0; s < NS; ++s) inv_w += cell.Y[s] / m.mw[s];
-    f[0] = float(cell.T);
-    f[1] = float(log10(cell.T * cell.D * (kRUniv * 1000 * inv_w)));
+        for (int s = 0; s < NS; ++s) inv_w += cell.Y[s] / m.mw[s];
+        f[0] = float(cell.T);
+        f[1] = float(log10(cell.T * cell.D * (kRUniv * 1000 * inv_w)));
 #pragma unroll
-    for (int s = 0; s < NS; ++s) f[2 + s] = float(cell.Y[s]);
-    f[NS + 2] = float(log10(*dt_dev));
+        for (int s = 0; s < NS; ++s) f[2 + s] = float(cell.Y[s]);
+        f[NS + 2] = float(log10(*dt_dev));
+    }
 }
 
 // Apply the ensemble's prediction to each queued cell, or send it to the stiff
@@ -768,90 +769,107 @@ template <int NS>
 __global__ void __launch_bounds__(128) k_learned_apply(const __grid_constant__ DevMech m, const DevGrid g,
                                                        const DevState st, LearnedParams lp)
 {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    // a fixed grid walks the queue in whole warps (the fallback append is
+    // warp-aggregated)
     const int nq = lp.counts[0];
-    bool fallback = false;
-    int c = 0;
-    if (q < nq) {
-        const long long n3 = g.n3;
-        c = lp.queue[q];
-        const float *f = lp.feat + (long long)q * (NS + 3);
-        bool ok = true;
+    const int stride = gridDim.x * blockDim.x;
+    const int span = (nq + 31) / 32 * 32;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < span; q += stride) {
+        bool fallback = false;
+        int c = 0;
+        if (q < nq) {
+            const long long n3 = g.n3;
+            c = lp.queue[q];
+            const float *f = lp.feat + (long long)q * (NS + 3);
+            bool ok = true;
 #pragma unroll
-        for (int a = 0; a < NS + 3; ++a) ok = ok && f[a] >= float(lp.box_lo[a]) && f[a] <= float(lp.box_hi[a]);
-        double mean[NS + 1], spread = 0;
+            for (int a = 0; a < NS + 3; ++a) ok = ok && f[a] >= float(lp.box_lo[a]) && f[a] <= float(lp.box_hi[a]);
+            double mean[NS + 1], spread = 0;
 #pragma unroll
-        for (int o = 0; o < NS + 1; ++o) {
-            double s1 = 0, s2 = 0;
-            for (int e = 0; e < lp.members; ++e) {
-                const double v = lp.pred[((long long)e * nq + q) * (NS + 1) + o];
-                s1 += v;
-                s2 += v * v;
+            for (int o = 0; o < NS + 1; ++o) {
+                double s1 = 0, s2 = 0;
+                for (int e = 0; e < lp.members; ++e) {
+                    const double v = lp.pred[(long long)q * lp.pred_row + (long long)e * lp.pred_mem + o];
+                    s1 += v;
+                    s2 += v * v;
+                }
+                const double mu = s1 / lp.members;
+                const double var = fmax(s2 / lp.members - mu * mu, 0.0);
+                // spread and mean in the model's output space, the change back in physical units
+                spread = fmax(spread, sqrt(var) * lp.out_scale[o]);
+                mean[o] = lp.out_eps[o] > 0 ? lp.out_eps[o] * sinh(mu) : mu;
+                ok = ok && (lp.out_bound[o] <= 0 || fabs(mean[o]) <= lp.out_bound[o]);
             }
-            const double mu = s1 / lp.members;
-            const double var = fmax(s2 / lp.members - mu * mu, 0.0);
-            // spread and mean in the model's output space, the change back in physical units
-            spread = fmax(spread, sqrt(var) * lp.out_scale[o]);
-            mean[o] = lp.out_eps[o] > 0 ? lp.out_eps[o] * sinh(mu) : mu;
-            ok = ok && (lp.out_bound[o] <= 0 || fabs(mean[o]) <= lp.out_bound[o]);
+            ok = ok && spread <= lp.tau && isfinite(spread);
+            if (ok) {
+                CellState<NS> cell;
+                load_recovered<NS>(st, n3, c, cell);
+                double dY[NS], Y[NS], sum = 0;
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    double d = 0;
+#pragma unroll
+                    for (int r = 0; r < NS; ++r) d += lp.proj[s][r] * mean[r];
+                    dY[s] = d;
+                }
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    Y[s] = fmax(cell.Y[s] + dY[s], 0.0);
+                    sum += Y[s];
+                }
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    cell.Y[s] = Y[s] / sum;
+                    cell.cs[s] = cell.D * cell.Y[s];
+                }
+                cell.T = newton_temperature<NS>(m, cell.T + mean[NS], cell.E, cell.Y);
+                store_cell<NS>(m, st, n3, c, cell);
+                atomicAdd(&st.counters[kCntLearned], 1ULL);
+            } else {
+                fallback = true;
+            }
         }
-        ok = ok && spread <= lp.tau && isfinite(spread);
-        if (ok) {
-            CellState<NS> cell;
-            load_recovered<NS>(st, n3, c, cell);
-            double dY[NS], Y[NS], sum = 0;
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-                double d = 0;
-#pragma unroll
-                for (int r = 0; r < NS; ++r) d += lp.proj[s][r] * mean[r];
-                dY[s] = d;
-            }
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-                Y[s] = fmax(cell.Y[s] + dY[s], 0.0);
-                sum += Y[s];
-            }
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-                cell.Y[s] = Y[s] / sum;
-                cell.cs[s] = cell.D * cell.Y[s];
-            }
-            cell.T = newton_temperature<NS>(m, cell.T + mean[NS], cell.E, cell.Y);
-            store_cell<NS>(m, st, n3, c, cell);
-            atomicAdd(&st.counters[kCntLearned], 1ULL);
-        } else {
-            fallback = true;
+        const unsigned mask = __ballot_sync(0xffffffffu, fallback);
+        if (mask) {
+            const int lane = threadIdx.x & 31;
+            int base = 0;
+            if (lane == __ffs(mask) - 1)
+                base = atomicAdd(&lp.counts[1], __popc(mask));
+            base = __shfl_sync(0xffffffffu, base, __ffs(mask) - 1);
+            if (fallback)
+                lp.fallback[base + __popc(mask & ((1u << lane) - 1))] = c;
         }
-    }
-    const unsigned mask = __ballot_sync(0xffffffffu, fallback);
-    if (mask) {
-        const int lane = threadIdx.x & 31;
-        int base = 0;
-        if (lane == __ffs(mask) - 1)
-            base = atomicAdd(&lp.counts[1], __popc(mask));
-        base = __shfl_sync(0xffffffffu, base, __ffs(mask) - 1);
-        if (fallback)
-            lp.fallback[base + __popc(mask & ((1u << lane) - 1))] = c;
     }
 }
 
 // The stiff kinetics on a queue of cells whose recovered state is stored.
 template <int NS, class Rt>
 __global__ void __launch_bounds__(128) k_react_queue(const __grid_constant__ DevMech m, const DevGrid g,
-                                                     const DevState st, const int *__restrict__ queue,
-                                                     const int *__restrict__ count, const double *__restrict__ dt_dev,
-                                                     int max_substeps, int counter)
+                                                     const DevState st, const int *__restrict__ queue, int *count,
+                                                     const double *__restrict__ dt_dev, int max_substeps, int counter)
 {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= *count)
-        return;
-    const long long n3 = g.n3, c = queue[q];
-    CellState<NS> cell;
-    load_recovered<NS>(st, n3, c, cell);
-    atomicAdd(&st.counters[counter], 1ULL);
-    if (react_or_defer<NS, Rt>(m, st, n3, c, cell, *dt_dev, max_substeps))
-        store_cell<NS>(m, st, n3, c, cell);
+    // A fixed grid drains the queue (its length is read on the device): each
+    // warp takes the next 32 cells from count[1] (reset before the launch).
+    const int nq = *(volatile int *)count;
+    const int lane = threadIdx.x & 31;
+    int *next = count + 1;
+    for (;;) {
+        int base = 0;
+        if (lane == 0)
+            base = atomicAdd(next, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= nq)
+            break;
+        const int q = base + lane;
+        if (q < nq) {
+            const long long n3 = g.n3, c = queue[q];
+            CellState<NS> cell;
+            load_recovered<NS>(st, n3, c, cell);
+            atomicAdd(&st.counters[counter], 1ULL);
+            if (react_or_defer<NS, Rt>(m, st, n3, c, cell, *dt_dev, max_substeps))
+                store_cell<NS>(m, st, n3, c, cell);
+        }
+    }
 }
 
 // ------------------------------------------------- warp-per-cell kinetics

@@ -123,30 +123,29 @@ cudaError_t classify_t(const LaunchArgs &a, const LearnedParams &lp)
     return cudaGetLastError();
 }
 
+// The learned-chemistry kernels run on fixed grids that read the queue lengths
+// on the device, so a step needs no host-side count and can be captured.
+inline unsigned queue_grid(const LaunchArgs &a, int per_sm) { return unsigned((a.sms > 0 ? a.sms : 148) * per_sm); }
+
 template <int NS, int NR>
-cudaError_t features_t(const LaunchArgs &a, const LearnedParams &lp, int nq)
+cudaError_t features_t(const LaunchArgs &a, const LearnedParams &lp)
 {
-    if (nq <= 0)
-        return cudaSuccess;
-    k_learned_features<NS><<<dim3(unsigned((nq + 127) / 128)), 128, 0, a.stream>>>(*a.mech, a.g, a.st, lp, a.dt_dev);
+    k_learned_features<NS><<<dim3(queue_grid(a, 8)), 128, 0, a.stream>>>(*a.mech, a.g, a.st, lp, a.dt_dev);
     return cudaGetLastError();
 }
 
 template <int NS, int NR>
-cudaError_t apply_t(const LaunchArgs &a, const LearnedParams &lp, int nq)
+cudaError_t apply_t(const LaunchArgs &a, const LearnedParams &lp)
 {
-    if (nq <= 0)
-        return cudaSuccess;
-    k_learned_apply<NS><<<dim3(unsigned((nq + 127) / 128)), 128, 0, a.stream>>>(*a.mech, a.g, a.st, lp);
+    k_learned_apply<NS><<<dim3(queue_grid(a, 8)), 128, 0, a.stream>>>(*a.mech, a.g, a.st, lp);
     return cudaGetLastError();
 }
 
+// count[0]: queue length, count[1]: cells taken so far (zero at launch)
 template <int NS, int NR>
-cudaError_t react_queue_t(const LaunchArgs &a, const int *queue, const int *count, int nq, int counter)
+cudaError_t react_queue_t(const LaunchArgs &a, const int *queue, int *count, int counter)
 {
-    if (nq <= 0)
-        return cudaSuccess;
-    const dim3 grid(unsigned((nq + 127) / 128));
+    const dim3 grid(queue_grid(a, 4));
     if (a.spec == 1 && NS == Mech_JA919::NS && NR == Mech_JA919::NR)
         k_react_queue<NS, Mech_JA919><<<grid, 128, 0, a.stream>>>(*a.mech, a.g, a.st, queue, count, a.dt_dev,
                                                                   a.max_substeps, counter);
@@ -216,14 +215,11 @@ cudaError_t launch_to_f32(const double *src, float *dst, long long n, cudaStream
 }
 
 cudaError_t launch_recover_classify(const LaunchArgs &a, const LearnedParams &lp) { EU3D_DISPATCH(classify_t, a, lp) }
-cudaError_t launch_learned_features(const LaunchArgs &a, const LearnedParams &lp, int nq)
+cudaError_t launch_learned_features(const LaunchArgs &a, const LearnedParams &lp) { EU3D_DISPATCH(features_t, a, lp) }
+cudaError_t launch_learned_apply(const LaunchArgs &a, const LearnedParams &lp) { EU3D_DISPATCH(apply_t, a, lp) }
+cudaError_t launch_react_queue(const LaunchArgs &a, const int *queue, int *count, int counter)
 {
-    EU3D_DISPATCH(features_t, a, lp, nq)
-}
-cudaError_t launch_learned_apply(const LaunchArgs &a, const LearnedParams &lp, int nq) { EU3D_DISPATCH(apply_t, a, lp, nq) }
-cudaError_t launch_react_queue(const LaunchArgs &a, const int *queue, const int *count, int nq, int counter)
-{
-    EU3D_DISPATCH(react_queue_t, a, queue, count, nq, counter)
+    EU3D_DISPATCH(react_queue_t, a, queue, count, counter)
 }
 cudaError_t launch_state_from_tpy(const LaunchArgs &a, long long n, const double *T, const double *p, const double *Y,
                                   double *cs, double *E)

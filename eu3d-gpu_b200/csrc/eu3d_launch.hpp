@@ -18,6 +18,7 @@ struct LaunchArgs {
     int precision; // eu_precision
     int chemistry; // eu_chemistry
     int spec;      // 1: tables are bitwise H2_JA919, use the generated rate code
+    int sms;       // multiprocessors of the device (fixed grids of the queue kernels)
     cudaStream_t stream;
 };
 
@@ -30,9 +31,9 @@ struct Launchers {
     cudaError_t (*recover_react)(const LaunchArgs &a, bool react);
     cudaError_t (*derived)(const LaunchArgs &a, int which, double *out);
     cudaError_t (*recover_classify)(const LaunchArgs &a, const LearnedParams &lp);
-    cudaError_t (*learned_features)(const LaunchArgs &a, const LearnedParams &lp, int nq);
-    cudaError_t (*learned_apply)(const LaunchArgs &a, const LearnedParams &lp, int nq);
-    cudaError_t (*react_queue)(const LaunchArgs &a, const int *queue, const int *count, int nq, int counter);
+    cudaError_t (*learned_features)(const LaunchArgs &a, const LearnedParams &lp);
+    cudaError_t (*learned_apply)(const LaunchArgs &a, const LearnedParams &lp);
+    cudaError_t (*react_queue)(const LaunchArgs &a, const int *queue, int *count, int counter);
     cudaError_t (*react_heavy)(const LaunchArgs &a, int blocks);
     cudaError_t (*materialize)(const LaunchArgs &a);
 };
@@ -45,10 +46,9 @@ struct Launchers {
     cudaError_t launch_derived(const LaunchArgs &a, int which, double *out);                       \
     cudaError_t launch_set_value(double *dst, double v, cudaStream_t s);                           \
     cudaError_t launch_recover_classify(const LaunchArgs &a, const LearnedParams &lp);             \
-    cudaError_t launch_learned_features(const LaunchArgs &a, const LearnedParams &lp, int nq);     \
-    cudaError_t launch_learned_apply(const LaunchArgs &a, const LearnedParams &lp, int nq);        \
-    cudaError_t launch_react_queue(const LaunchArgs &a, const int *queue, const int *count, int nq, \
-                                   int counter);                                                   \
+    cudaError_t launch_learned_features(const LaunchArgs &a, const LearnedParams &lp);             \
+    cudaError_t launch_learned_apply(const LaunchArgs &a, const LearnedParams &lp);                \
+    cudaError_t launch_react_queue(const LaunchArgs &a, const int *queue, int *count, int counter); \
     cudaError_t launch_state_from_tpy(const LaunchArgs &a, long long n, const double *T,           \
                                       const double *p, const double *Y, double *cs, double *E);    \
     cudaError_t launch_chem_samples(const LaunchArgs &a, long long n, double *cs, double *T,       \

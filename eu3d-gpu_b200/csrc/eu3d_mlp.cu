@@ -6,6 +6,7 @@
 
 #include "eu3d.h"
 #include "eu3d_gemm.cuh"
+#include "eu3d_mlp_fused.cuh"
 #include "eu3d_mlp_kernels.hpp"
 
 using namespace eu3d;
@@ -235,6 +236,33 @@ cudaError_t refresh_weights(const float *W, int out, int in, int out_pad, int in
 cudaError_t random_rows(int *rows, int count, long long n, unsigned long long key, cudaStream_t s)
 {
     k_random_rows<<<blocks(count, 256), 256, 0, s>>>(rows, count, n, key);
+    return cudaGetLastError();
+}
+
+cudaError_t mlp_fused(const FusedMlpParams &p, const float *feat, int ld_feat, int count_host, const int *count_dev,
+                      int max_rows, float *out, long long s_row, long long s_mem, int *err, int grid, cudaStream_t s)
+{
+    if (!fused_supported(p.in_pad, p.width, p.out_pad, p.members, p.layers))
+        return cudaErrorInvalidValue;
+    const size_t smem = fused_smem_bytes(p.in_pad, p.width);
+    static size_t configured = 0;
+    if (configured < smem) {
+        cudaError_t e = cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess)
+            return e;
+        configured = smem;
+    }
+    if (grid < 1)
+        return cudaSuccess;
+    k_mlp_fused<<<grid, kFusedThreads, smem, s>>>(p, feat, ld_feat, count_host, count_dev, max_rows, out, s_row, s_mem,
+                                                  err);
+    return cudaGetLastError();
+}
+
+cudaError_t pack_slabs(const void *W, int N, int K, void *out, cudaStream_t s)
+{
+    k_pack_slabs<<<blocks((long long)N * K, 256), 256, 0, s>>>(static_cast<const __nv_bfloat16 *>(W), N, K,
+                                                                static_cast<__nv_bfloat16 *>(out));
     return cudaGetLastError();
 }
 

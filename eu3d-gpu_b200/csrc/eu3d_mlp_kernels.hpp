@@ -7,6 +7,34 @@
 
 namespace eu3d {
 
+// The fused inference kernel (eu3d_mlp_fused.cuh): model shape, packed weight
+// slabs and per-layer biases.
+constexpr int kFusedMaxMembers = 8, kFusedMaxLayers = 9, kFusedSlabK = 64;
+struct FusedMlpParams {
+    int members, layers; // layers = hidden + output
+    int n_in, in_pad, width, out_pad, n_out;
+    const void *slabs;                                    // bf16, K-slabs of 64 columns in core-matrix layout
+    long long off[kFusedMaxMembers][kFusedMaxLayers];     // element offset of layer (e, l)'s first slab
+    const float *bias[kFusedMaxMembers][kFusedMaxLayers]; // [N] per layer
+    const float *in_shift, *in_scale, *out_shift, *out_scale;
+};
+
+// Shapes the fused kernel takes: every layer's N fits the 256 TMEM columns and
+// the ring slot (sized for width), the input tile fits its buffer.
+inline bool fused_supported(int in_pad, int width, int out_pad, int members, int layers)
+{
+    return width % 16 == 0 && width >= 16 && width <= 256 && in_pad <= 64 && out_pad <= width &&
+           members <= kFusedMaxMembers && layers <= kFusedMaxLayers;
+}
+
+// Predictions of every member for the first `count` rows of feat (count read
+// from count_dev when it is not null, capped at max_rows): out[row * s_row +
+// member * s_mem + o]. `grid` CTAs (one per SM is the intent).
+cudaError_t mlp_fused(const FusedMlpParams &p, const float *feat, int ld_feat, int count_host, const int *count_dev,
+                      int max_rows, float *out, long long s_row, long long s_mem, int *err, int grid, cudaStream_t s);
+// One layer's bf16 [N x K] weights into K-slabs (see k_pack_slabs).
+cudaError_t pack_slabs(const void *W, int N, int K, void *out, cudaStream_t s);
+
 // C = epilogue(A B^T): A (M x K), B (N x K) row-major bf16; act 0 none, 1 SiLU,
 // 2 times SiLU'(Z), 3 atomically accumulate into Cf (split-K partial sums).
 cudaError_t gemm_bf16(const void *A, int lda, const void *B, int ldb, int M, int N, int K, const float *bias, int act,

@@ -71,7 +71,8 @@ struct LearnedParams {
     float *feat;           // [queue capacity x (3 + NS)] fp32 model inputs
     float *pred;           // [members x queue length x (NS + 1)] fp32 physical outputs
     int *queue, *fallback; // cell indices
-    int *counts;           // [0] learned queue length, [1] fallback queue length
+    int *counts;           // [0] learned queue length, [1] fallback queue length, [2] fallback cells taken
+    long long pred_row, pred_mem; // ensemble output o of member e for queue row q: pred[q pred_row + e pred_mem + o]
     int members;
     double frozen_y;       // a cell whose non-inert mass fraction is below this is frozen
     double frozen_T;       // a cell colder than this whose radical pool is below frozen_radical is frozen

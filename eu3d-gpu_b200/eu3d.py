@@ -37,7 +37,7 @@ class Config(ctypes.Structure):
     _fields_ = [("total_ni", _I), ("total_nj", _I), ("total_nk", _I),
                 ("xa", _D), ("xb", _D), ("ya", _D), ("yb", _D), ("za", _D), ("zb", _D),
                 ("bc", _I), ("device", _I), ("precision", _I), ("chemistry", _I), ("arith", _I),
-                ("max_substeps", _I), ("record_sources", _I), ("profile", _I)]
+                ("max_substeps", _I), ("record_sources", _I), ("profile", _I), ("eager", _I)]
 
 
 class MechanismC(ctypes.Structure):
@@ -114,6 +114,8 @@ def library():
         lib.eu_mlp_train.argtypes = [_P, _P, _P, ctypes.c_longlong, _I, _I, ctypes.c_float, ctypes.c_uint, _P]
         lib.eu_mlp_predict.argtypes = [_P, _P, ctypes.c_longlong, _P]
         lib.eu_mlp_predict_noalloc.argtypes = [_P, _P, ctypes.c_longlong, _P]
+        lib.eu_mlp_predict_fused.argtypes = [_P, _P, ctypes.c_longlong, _P]
+        lib.eu_mlp_predict_fused.restype = _I
         lib.eu_mlp_predict_noalloc.restype = _I
         for fn in ("eu_mlp_create", "eu_mlp_destroy", "eu_mlp_gemm", "eu_mlp_init", "eu_mlp_set_scaling",
                    "eu_mlp_get_params", "eu_mlp_set_params", "eu_mlp_loss_grad", "eu_mlp_train", "eu_mlp_predict"):
@@ -181,11 +183,11 @@ class Solver:
     """One eu_handle: a haloed node grid, a mechanism and the device state."""
 
     def __init__(self, total_ni, total_nj, total_nk, extent, precision="fp64", chemistry="stiff", arith="strict",
-                 device=0, max_substeps=0, record_sources=False, profile=False, bc=2):
+                 device=0, max_substeps=0, record_sources=False, profile=False, bc=2, graphs=True):
         lib = library()
         self.cfg = Config(int(total_ni), int(total_nj), int(total_nk), *[float(v) for v in extent], int(bc),
                           int(device), PRECISION[precision], CHEMISTRY[chemistry], ARITH[arith], int(max_substeps),
-                          int(bool(record_sources)), int(bool(profile)))
+                          int(bool(record_sources)), int(bool(profile)), int(not graphs))
         h = _P()
         st = lib.eu_create(ctypes.byref(self.cfg), ctypes.byref(h))
         if st:
@@ -381,6 +383,11 @@ class Mlp:
     def predict(self, X, out):
         """out: torch CUDA fp32 tensor (members x n x n_out)."""
         self._check(library().eu_mlp_predict(self.h, X.data_ptr(), X.shape[0], out.data_ptr()), "predict")
+
+    def predict_fused(self, X, out):
+        """predict() from the one persistent tensor-core kernel the learned
+        timestep uses (eu_mlp_predict_fused)."""
+        self._check(library().eu_mlp_predict_fused(self.h, X.data_ptr(), X.shape[0], out.data_ptr()), "predict_fused")
 
     def predict_noalloc(self, X, out):
         """predict() with its scratch in the library's fixed device array

@@ -50,6 +50,13 @@ struct eu_handle {
     // mixed precision: the timestep keeps only the FP32 primitive planes
     // current; the FP64 ones are formed on demand (k_materialize) for output
     bool prim_stale = false;
+    int sms = 0;
+    // one timestep captured as a CUDA graph (recaptured when what its kernels
+    // take by value changes: the mechanism, the learned-chemistry settings)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_launches = 0;
+    bool graph_dirty = true;
     std::string err;
 };
 
@@ -161,6 +168,7 @@ eu_status install_mechanism(eu_handle *h, const MechanismTables &m)
     h->mech = m;
     h->dmech = d;
     h->has_mech = true;
+    h->graph_dirty = true; // the kernels take the tables by value
     if (!first)
         return EU_OK;
 
@@ -207,8 +215,20 @@ LaunchArgs launch_args(eu_handle *h)
     a.precision = h->cfg.precision;
     a.chemistry = h->cfg.chemistry;
     a.spec = h->spec;
+    a.sms = h->sms;
     a.stream = h->stream;
     return a;
+}
+
+void drop_graph(eu_handle *h)
+{
+    if (h->graph_exec)
+        cudaGraphExecDestroy(h->graph_exec);
+    if (h->graph)
+        cudaGraphDestroy(h->graph);
+    h->graph_exec = nullptr;
+    h->graph = nullptr;
+    h->graph_dirty = true;
 }
 
 bool is_strict(const eu_handle *h) { return h->cfg.arith == EU_ARITH_STRICT; }
@@ -374,6 +394,7 @@ eu_status eu_create(const eu_config *cfg, eu_handle **out)
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg->device) != cudaSuccess || sms < 1)
         sms = 1;
     h->heavy_blocks = 4 * sms; // 4 blocks of 4 warps per SM, each warp a cell at a time
+    h->sms = sms;
     eu_status s;
     if ((s = dalloc(h, &h->d_xyz, size_t(h->nx + h->ny + h->nz))) != EU_OK ||
         (s = dalloc(h, &h->d_dt, size_t(1))) != EU_OK) {
@@ -410,6 +431,7 @@ eu_status eu_destroy(eu_handle *h)
     cudaSetDevice(h->cfg.device);
     if (h->stream)
         cudaStreamSynchronize(h->stream);
+    drop_graph(h);
     free_all(h);
     if (h->h_counts)
         cudaFreeHost(h->h_counts);
@@ -617,37 +639,99 @@ void element_projector(const MechanismTables &m, double (&P)[kMaxS][kMaxS])
 
 // One learned-chemistry phase of a step: recover + classify every cell,
 // features of the queued cells, the ensemble, gate + apply, stiff fallback.
-eu_status learned_chemistry(eu_handle *h, const LaunchArgs &a, const Launchers &L, long long *reacting,
-                            int *launches)
+// The queue kernels read the queue lengths on the device; with the model's
+// fused inference kernel nothing here waits on the host, so the phase can be
+// captured in the step's graph. Otherwise (a model shape without the fused
+// kernel) the queue length is read back to size the layer-wise GEMMs.
+eu_status learned_chemistry(eu_handle *h, const LaunchArgs &a, const Launchers &L, int *launches)
 {
-    LearnedParams &lp = h->lp;
-    CK(h, cudaMemsetAsync(lp.counts, 0, 2 * sizeof(int), h->stream));
+    LearnedParams lp = h->lp;
+    const int ns = h->mech.ns;
+    CK(h, cudaMemsetAsync(lp.counts, 0, 3 * sizeof(int), h->stream));
     CK(h, L.recover_classify(a, lp));
-    ++*launches;
-    CK(h, cudaMemcpyAsync(h->h_counts, lp.counts, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-    CK(h, cudaStreamSynchronize(h->stream));
-    const int nq = h->h_counts[0];
-    *reacting = nq;
-    if (nq == 0)
-        return EU_OK;
-    CK(h, L.learned_features(a, lp, nq));
-    eu_status s = mlp_predict_stream(h->model, lp.feat, nq, lp.pred, h->stream);
-    if (s != EU_OK)
-        return fail(h, s, "learned model: %s", eu_mlp_last_error(h->model));
-    CK(h, L.learned_apply(a, lp, nq));
-    // features, apply, and per batch of rows: packing, then the layers and the
-    // unscaling of every member
-    int n_in = 0, n_out = 0, members = 0;
-    mlp_shape(h->model, &n_in, &n_out, &members);
-    const int batches = mlp_batches(h->model, nq);
-    *launches += 2 + batches * (1 + members * (mlp_layers(h->model) + 1));
-    CK(h, cudaMemcpyAsync(h->h_counts + 1, lp.counts + 1, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-    CK(h, cudaStreamSynchronize(h->stream));
-    const int nf = h->h_counts[1];
-    if (nf > 0) {
-        CK(h, L.react_queue(a, lp.fallback, lp.counts + 1, nf, kCntFallback));
+    CK(h, L.learned_features(a, lp));
+    *launches += 2;
+    if (mlp_has_fused(h->model)) {
+        lp.pred_row = (long long)lp.members * (ns + 1);
+        lp.pred_mem = ns + 1;
+        eu_status s = mlp_predict_queue(h->model, lp.feat, lp.counts, int(h->lp_capacity), lp.pred, lp.pred_row,
+                                        lp.pred_mem, h->stream);
+        if (s != EU_OK)
+            return fail(h, s, "learned model: %s", eu_mlp_last_error(h->model));
+        ++*launches;
+    } else {
+        CK(h, cudaMemcpyAsync(h->h_counts, lp.counts, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        const int nq = h->h_counts[0];
+        lp.pred_row = ns + 1;
+        lp.pred_mem = (long long)nq * (ns + 1);
+        if (nq > 0) {
+            eu_status s = mlp_predict_stream(h->model, lp.feat, nq, lp.pred, h->stream);
+            if (s != EU_OK)
+                return fail(h, s, "learned model: %s", eu_mlp_last_error(h->model));
+            // per batch of rows: packing, then the layers and the unscaling of every member
+            *launches += mlp_batches(h->model, nq) * (1 + lp.members * (mlp_layers(h->model) + 1));
+        }
+    }
+    CK(h, L.learned_apply(a, lp));
+    CK(h, L.react_queue(a, lp.fallback, lp.counts + 1, kCntFallback));
+    *launches += 2;
+    return EU_OK;
+}
+
+// The launches of one timestep on h->stream (run eagerly or recorded into the
+// step's graph). phase (profile mode) receives per-phase event times.
+eu_status step_launches(eu_handle *h, const LaunchArgs &a, const Launchers &L, bool prof, int *launches)
+{
+    const bool react = h->cfg.chemistry == EU_CHEM_STIFF;
+    const bool learned = h->cfg.chemistry == EU_CHEM_LEARNED;
+    CK(h, cudaMemsetAsync(h->st.counters, 0, kCntPerStep * sizeof(unsigned long long), h->stream));
+    if (prof) CK(h, cudaEventRecord(h->pev[0], h->stream));
+    CK(h, L.boundary(a));
+    if (prof) CK(h, cudaEventRecord(h->pev[1], h->stream));
+    CK(h, L.flux_update(a));
+    if (prof) CK(h, cudaEventRecord(h->pev[2], h->stream));
+    *launches += 2;
+    const bool heavy = h->st.heavy && (learned || react);
+    if (heavy)
+        CK(h, cudaMemsetAsync(h->st.heavy, 0, 2 * sizeof(int), h->stream));
+    if (learned) {
+        eu_status ls = learned_chemistry(h, a, L, launches);
+        if (ls != EU_OK)
+            return ls;
+    } else {
+        CK(h, L.recover_react(a, react));
         ++*launches;
     }
+    if (heavy) { // warp-per-cell kinetics of the cells deferred above
+        CK(h, L.react_heavy(a, h->heavy_blocks));
+        ++*launches;
+    }
+    if (prof)
+        CK(h, cudaEventRecord(h->pev[3], h->stream));
+    return EU_OK;
+}
+
+// Records one timestep into h->graph and instantiates it.
+eu_status capture_step(eu_handle *h, const LaunchArgs &a, const Launchers &L)
+{
+    drop_graph(h);
+    int launches = 0;
+    CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    eu_status s = step_launches(h, a, L, false, &launches);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (s != EU_OK) {
+        if (g)
+            cudaGraphDestroy(g);
+        return s;
+    }
+    if (e != cudaSuccess)
+        return cuda_fail(h, e, "cudaStreamEndCapture");
+    h->graph = g;
+    CK(h, cudaGraphInstantiate(&h->graph_exec, g, 0));
+    h->graph_launches = launches;
+    h->graph_dirty = false;
     return EU_OK;
 }
 
@@ -714,7 +798,7 @@ eu_status eu_set_learned(eu_handle *h, eu_mlp *model, const eu_learned_config *l
         if ((s = dalloc(h, &lp.pred, size_t(cap) * members * (ns + 1))) != EU_OK) return s;
         if ((s = dalloc(h, &lp.queue, size_t(cap))) != EU_OK) return s;
         if ((s = dalloc(h, &lp.fallback, size_t(cap))) != EU_OK) return s;
-        if ((s = dalloc(h, &lp.counts, size_t(2))) != EU_OK) return s;
+        if ((s = dalloc(h, &lp.counts, size_t(3))) != EU_OK) return s;
         h->lp_capacity = cap;
     }
     if (!h->h_counts)
@@ -747,6 +831,9 @@ eu_status eu_set_learned(eu_handle *h, eu_mlp *model, const eu_learned_config *l
         lp.inert[s] = used ? 0 : 1;
     }
     h->model = model;
+    h->graph_dirty = true; // the kernels take these settings by value
+    // the model's weights were packed on its own stream
+    CK(h, cudaStreamSynchronize(mlp_stream(model)));
     return EU_OK;
 }
 
@@ -765,8 +852,11 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
     const bool learned = h->cfg.chemistry == EU_CHEM_LEARNED;
     if (learned && !h->model)
         return fail(h, EU_ERR_NOT_READY, "learned chemistry needs eu_set_learned first");
-    long long reacting = 0;
     const Launchers &L = flavour(h);
+    // A step is replayed from its captured graph unless the caller asked for
+    // eager launches, times phases, or a learned model has no fused kernel
+    // (then the step reads the queue length back on the host).
+    const bool graphs = !h->cfg.eager && !prof && (!learned || mlp_has_fused(h->model));
     double phase[4] = {0, 0, 0, 0};
     int launches = 0;
     if (stats)
@@ -776,31 +866,27 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
     ++launches;
     if (h->st.prim32 && nsteps > 0)
         h->prim_stale = true;
-    for (int n = 0; n < nsteps; ++n) {
-        CK(h, cudaMemsetAsync(h->st.counters, 0, kCntPerStep * sizeof(unsigned long long), h->stream));
-        if (prof) CK(h, cudaEventRecord(h->pev[0], h->stream));
-        CK(h, L.boundary(a));
-        if (prof) CK(h, cudaEventRecord(h->pev[1], h->stream));
-        CK(h, L.flux_update(a));
-        if (prof) CK(h, cudaEventRecord(h->pev[2], h->stream));
-        launches += 2;
-        const bool heavy = h->st.heavy && (learned || react);
-        if (heavy)
-            CK(h, cudaMemsetAsync(h->st.heavy, 0, 2 * sizeof(int), h->stream));
-        if (learned) {
-            eu_status ls = learned_chemistry(h, a, L, &reacting, &launches);
-            if (ls != EU_OK)
-                return ls;
-        } else {
-            CK(h, L.recover_react(a, react));
-            ++launches;
+    int n = 0;
+    if (graphs && nsteps > 0 && (h->graph_dirty || !h->graph_exec)) {
+        // the first step runs eagerly (one-time kernel attribute set-up), then
+        // the step is captured
+        eu_status s = step_launches(h, a, L, false, &launches);
+        if (s != EU_OK)
+            return s;
+        n = 1;
+        if ((s = capture_step(h, a, L)) != EU_OK)
+            return s;
+    }
+    for (; n < nsteps; ++n) {
+        if (graphs) {
+            CK(h, cudaGraphLaunch(h->graph_exec, h->stream));
+            launches += h->graph_launches;
+            continue;
         }
-        if (heavy) { // warp-per-cell kinetics of the cells deferred above
-            CK(h, L.react_heavy(a, h->heavy_blocks));
-            ++launches;
-        }
+        eu_status s = step_launches(h, a, L, prof, &launches);
+        if (s != EU_OK)
+            return s;
         if (prof) {
-            CK(h, cudaEventRecord(h->pev[3], h->stream));
             CK(h, cudaEventSynchronize(h->pev[3]));
             for (int q = 0; q < 3; ++q) {
                 float ms = 0;
@@ -814,6 +900,11 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
     CK(h, cudaEventRecord(h->ev1, h->stream));
     unsigned long long cnt[kCntCount];
     CK(h, cudaMemcpyAsync(cnt, h->st.counters, sizeof cnt, cudaMemcpyDeviceToHost, h->stream));
+    int queued = 0, model_err = 0;
+    if (learned && nsteps > 0) {
+        CK(h, cudaMemcpyAsync(&queued, h->lp.counts, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaMemcpyAsync(&model_err, mlp_error_flag(h->model), sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    }
     CK(h, cudaStreamSynchronize(h->stream));
     float ms = 0;
     CK(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1));
@@ -821,13 +912,17 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
     stats->steps = nsteps;
     stats->max_nchem = int(cnt[kCntMaxNchem]);
     stats->sum_nchem = (long long)cnt[kCntSumNchem];
-    stats->reacting = react ? (long long)h->ni * h->nj * h->nk : reacting;
+    stats->reacting = react ? (long long)h->ni * h->nj * h->nk : queued;
     stats->learned = (long long)cnt[kCntLearned];
     stats->fallback = (long long)cnt[kCntFallback];
     stats->nonfinite = (long long)cnt[kCntNonfinite];
     stats->device_ms = ms;
     stats->launches = launches;
     for (int q = 0; q < 4; ++q) stats->phase_ms[q] = phase[q];
+    if (model_err) {
+        CK(h, cudaMemsetAsync(mlp_error_flag(h->model), 0, sizeof(int), h->stream));
+        return fail(h, EU_ERR_TIMEOUT, "a tensor-core pipeline wait of the learned model gave up");
+    }
     if (cnt[kCntNonfinite])
         return fail(h, EU_ERR_NONFINITE, "%llu cells with non-finite density or temperature", cnt[kCntNonfinite]);
     if (cnt[kCntBadNchem])

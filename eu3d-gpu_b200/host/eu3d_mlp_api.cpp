@@ -54,6 +54,12 @@ struct eu_mlp {
     int *rows = nullptr;
     long long adam_t = 0;
     std::vector<void *> allocs;
+    // inference in one persistent kernel (eu3d_mlp_fused.cuh): the bf16 weights
+    // repacked into K-slabs whenever they change
+    bool fused = false;
+    void *slabs = nullptr;
+    long long slab_off[eu3d::kFusedMaxMembers][eu3d::kFusedMaxLayers] = {};
+    int sms = 0;
 };
 
 namespace {
@@ -172,8 +178,13 @@ eu_status backward(eu_mlp *m, int e, int n)
 
 eu_status refresh(eu_mlp *m, int e)
 {
-    for (Layer &L : m->net[e])
+    for (size_t l = 0; l < m->net[e].size(); ++l) {
+        Layer &L = m->net[e][l];
         MCK(m, eu3d::refresh_weights(L.W, L.out_pad, L.in_pad, L.out_pad, L.in_pad, L.Wb, L.Wt, m->stream));
+        if (m->fused)
+            MCK(m, eu3d::pack_slabs(L.Wb, L.out_pad, L.in_pad,
+                                    static_cast<uint16_t *>(m->slabs) + m->slab_off[e][l], m->stream));
+    }
     return EU_OK;
 }
 
@@ -229,6 +240,49 @@ bool mlp_layer_view(const eu_mlp *m, int member, int layer, MlpLayerView *v)
 
 eu_status mlp_fail(eu_mlp *m, eu_status s, const char *msg) { return mfail(m, s, "%s", msg); }
 
+bool mlp_fused_params(const eu_mlp *m, FusedMlpParams *p)
+{
+    if (!m || !m->ready || !m->fused || !p)
+        return false;
+    *p = FusedMlpParams{};
+    p->members = m->members;
+    p->layers = m->hidden + 1;
+    p->n_in = m->n_in;
+    p->in_pad = m->in_pad;
+    p->width = m->width;
+    p->out_pad = m->out_pad;
+    p->n_out = m->n_out;
+    p->slabs = m->slabs;
+    for (int e = 0; e < m->members; ++e)
+        for (int l = 0; l <= m->hidden; ++l) {
+            p->off[e][l] = m->slab_off[e][l];
+            p->bias[e][l] = m->net[e][l].b;
+        }
+    p->in_shift = m->in_shift;
+    p->in_scale = m->in_scale;
+    p->out_shift = m->out_shift;
+    p->out_scale = m->out_scale;
+    return true;
+}
+
+eu_status mlp_predict_queue(eu_mlp *m, const float *feat, const int *count_dev, int max_rows, float *out,
+                            long long s_row, long long s_mem, cudaStream_t s)
+{
+    FusedMlpParams p;
+    if (!mlp_fused_params(m, &p))
+        return mfail(m, EU_ERR_UNSUPPORTED, "the model's shape has no fused inference kernel");
+    const int tiles = (max_rows + 127) / 128;
+    const int grid = tiles < m->sms ? tiles : m->sms;
+    MCK(m, eu3d::mlp_fused(p, feat, m->n_in, 0, count_dev, max_rows, out, s_row, s_mem, m->d_err, grid, s));
+    return EU_OK;
+}
+
+bool mlp_has_fused(const eu_mlp *m) { return m && m->ready && m->fused; }
+
+int *mlp_error_flag(eu_mlp *m) { return m ? m->d_err : nullptr; }
+
+cudaStream_t mlp_stream(const eu_mlp *m) { return m ? m->stream : nullptr; }
+
 eu_status mlp_predict_stream(eu_mlp *m, const float *X, long long n, float *out, cudaStream_t s)
 {
     for (long long r0 = 0; r0 < n; r0 += m->max_batch) {
@@ -262,6 +316,7 @@ eu_status eu_mlp_create(int device, eu_mlp **out)
         return EU_ERR_OUT_OF_MEMORY;
     m->device = device;
     if (cudaSetDevice(device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&m->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&m->d_err, sizeof(int)) != cudaSuccess || cudaMemset(m->d_err, 0, sizeof(int)) != cudaSuccess) {
         eu_mlp_destroy(m);
@@ -396,6 +451,16 @@ eu_status eu_mlp_init(eu_mlp *m, int n_in, int width, int hidden_layers, int n_o
     MCK(m, malloc_zero(m, &m->T2, size_t(B) * tw * 2));
     MCK(m, malloc_zero(m, &m->loss, 4 * sizeof(float)));
     MCK(m, malloc_zero(m, &m->rows, size_t(B) * sizeof(int)));
+    m->fused = eu3d::fused_supported(m->in_pad, width, m->out_pad, members, hidden_layers + 1);
+    if (m->fused) {
+        long long n = 0;
+        for (int e = 0; e < members; ++e)
+            for (int l = 0; l <= hidden_layers; ++l) {
+                m->slab_off[e][l] = n;
+                n += (long long)m->net[e][l].out_pad * m->net[e][l].in_pad;
+            }
+        MCK(m, malloc_zero(m, &m->slabs, size_t(n) * 2));
+    }
     for (int e = 0; e < members; ++e) {
         eu_status s = refresh(m, e);
         if (s != EU_OK)
@@ -565,6 +630,24 @@ eu_status eu_mlp_train(eu_mlp *m, const float *X, const float *T, long long n, i
     if (mean_loss)
         for (int e = 0; e < m->members; ++e) mean_loss[e] = float(total[e]);
     return EU_OK;
+}
+
+eu_status eu_mlp_predict_fused(eu_mlp *m, const float *X, long long n, float *out)
+{
+    if (!m || !X || !out || n < 0 || n > 0x7fffffffLL)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!m->ready)
+        return mfail(m, EU_ERR_NOT_READY, "eu_mlp_init first");
+    if (!m->fused)
+        return mfail(m, EU_ERR_UNSUPPORTED, "the model's shape has no fused inference kernel");
+    cudaSetDevice(m->device);
+    eu3d::FusedMlpParams p;
+    eu3d::mlp_fused_params(m, &p);
+    const long long tiles = (n + 127) / 128;
+    const int grid = int(tiles < m->sms ? tiles : m->sms);
+    MCK(m, eu3d::mlp_fused(p, X, m->n_in, int(n), nullptr, int(n), out, m->n_out, n * m->n_out, m->d_err, grid,
+                           m->stream));
+    return check_err(m);
 }
 
 eu_status eu_mlp_predict(eu_mlp *m, const float *X, long long n, float *out)

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include "eu3d.h"
+#include "eu3d_mlp_kernels.hpp"
 
 namespace eu3d {
 // Model shape; false when the model is not initialised.
@@ -33,4 +34,16 @@ bool mlp_view(const eu_mlp *m, MlpView *v);
 bool mlp_layer_view(const eu_mlp *m, int member, int layer, MlpLayerView *v);
 // Records msg as the model's last error and returns s.
 eu_status mlp_fail(eu_mlp *m, eu_status s, const char *msg);
+// The fused inference kernel: whether the model's shape has one, its launch
+// parameters, and predictions for the rows of a device-side queue whose length
+// the kernel reads from count_dev (at most max_rows): out[row * s_row + member *
+// s_mem + o]. One launch of one CTA per SM, so it can be captured in a graph.
+bool mlp_has_fused(const eu_mlp *m);
+bool mlp_fused_params(const eu_mlp *m, FusedMlpParams *p);
+eu_status mlp_predict_queue(eu_mlp *m, const float *feat, const int *count_dev, int max_rows, float *out,
+                            long long s_row, long long s_mem, cudaStream_t s);
+// Device flag the tensor-core kernels set when a bounded wait gives up.
+int *mlp_error_flag(eu_mlp *m);
+// The model's own stream (weight updates and repacking run there).
+cudaStream_t mlp_stream(const eu_mlp *m);
 } // namespace eu3d

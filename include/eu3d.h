@@ -83,6 +83,8 @@ typedef struct {
     int max_substeps;                 /* Nchem cap; 0 selects 1 << 20 */
     int record_sources;               /* nonzero: keep per-cell mass sources (CMS) */
     int profile;                      /* nonzero: time each kernel phase with CUDA events */
+    int eager;                        /* nonzero: launch each step's kernels one by one instead of
+                                         replaying the step's captured CUDA graph */
 } eu_config;
 
 /* Mechanism and thermo tables in the reference's layouts (src/Reaction.cpp:156-327). */
@@ -252,6 +254,13 @@ eu_status eu_mlp_train(eu_mlp *m, const float *X, const float *T, long long n, i
                        unsigned seed, float *mean_loss);
 /* Physical outputs of every member: out[member][row][n_out] (device fp32). */
 eu_status eu_mlp_predict(eu_mlp *m, const float *X, long long n, float *out);
+/* The same outputs from one persistent tensor-core kernel that runs every
+ * member's whole network per 128-row tile with the activations in shared
+ * memory and the accumulators in tensor memory (the form the learned timestep
+ * uses). Needs width <= 256 (multiple of 16), n_in <= 64, n_out <= width;
+ * other shapes return EU_ERR_UNSUPPORTED. No counterpart in the reference
+ * (its DNN scheme runs no model, src/Euler.cpp:1473-1480). */
+eu_status eu_mlp_predict_fused(eu_mlp *m, const float *X, long long n, float *out);
 
 /* eu_mlp_predict without any device allocation, for callers that cannot call
  * cudaMalloc while they run: a solver that gives all free device memory to its

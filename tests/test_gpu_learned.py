@@ -126,3 +126,36 @@ def test_trained_model_replaces_stiff_substeps(gpu):
     assert np.allclose(yb.sum(axis=0), 1.0, atol=1e-12)
     print(f"stiff substeps {sa['sum_nchem']}, learned path {sb['sum_nchem']}; learned cells {sb['learned']} of {n}; "
           f"species L1 mean {l1.mean():.2e} max {l1.max():.2e}")
+
+
+@pytest.mark.parametrize("chemistry,precision", [("stiff", "fp64"), ("stiff", "mixed"), ("learned", "mixed"),
+                                                 ("learned", "fp64")])
+def test_graph_replay_equals_eager_launches(gpu, chemistry, precision):
+    """A timestep replayed from its captured CUDA graph is the same launches as
+    the eager path: bitwise the same state, the same statistics. Covers the
+    learned phase (device-side queue lengths, the fused model kernel) and a
+    change of the gate's tau between calls, which recaptures the graph."""
+    import learned
+    out = {}
+    for graphs in (False, True):
+        ni, nj, nk = 24, 8, 8
+        ext = (0.0, 0.024, 0.0, 0.008, 0.0, 0.008)
+        mech = gpu.parse_mechanism(cases.MECH_JA919, cases.THERMO)
+        prim = cases.hot_reacting_block(ni + 4, nj + 4, nk + 4, mech["mw"], mech["ns"])
+        s = gpu.Solver(ni, nj, nk, ext, chemistry=chemistry, precision=precision, arith="fast", graphs=graphs)
+        s.set_mechanism(mech)
+        s.set_primitive(*prim)
+        stats = []
+        if chemistry == "learned":
+            model, gate = learned.load()
+            learned.attach(s, model, gate)
+        stats.append(s.step(3, 2e-8))
+        if chemistry == "learned":
+            learned.attach(s, model, dict(gate, tau=gate["tau"] * 3))
+        stats.append(s.step(2, 2e-8))
+        keep = ("max_nchem", "sum_nchem", "reacting", "learned", "fallback", "launches")
+        out[graphs] = ([{k: st[k] for k in keep} for st in stats], s.get("CS"), s.get("T"), s.get("Yi"))
+        s.close()
+    assert out[False][0] == out[True][0]
+    for a, b in zip(out[False][1:], out[True][1:]):
+        assert n_unequal(a, b) == 0

@@ -93,3 +93,28 @@ def test_training_fits_a_smooth_map(gpu):
     m.train(Xd, Td, batch=512, steps=400, lr=1e-3, seed=7)
     l1 = np.array([m.loss_grad(e, Xd[:1024], Td[:1024])[0] for e in range(MEMBERS)])
     assert (l1 < l0 / 20).all(), (l0, l1)
+
+
+@pytest.mark.parametrize("shape", [(N_IN, WIDTH, HIDDEN, N_OUT, MEMBERS), (5, 64, 2, 3, 2), (20, 96, 1, 40, 1)])
+def test_fused_inference_matches_layerwise(gpu, shape):
+    """The one-kernel inference (every member's network per 128-row tile, the
+    activations in shared memory, the accumulators in tensor memory, weights
+    streamed by bulk copies) gives the layer-wise GEMM path's outputs bit for
+    bit: the same K=16 MMA sequence, epilogues and scalings. Row counts cover
+    partial, exact and many tiles (more tiles than SMs); an empty queue is the
+    learned timestep's common case and is covered there."""
+    import torch
+    n_in, width, hidden, n_out, members = shape
+    m = gpu.Mlp()
+    m.init(n_in, width, hidden, n_out, members, max_batch=1024, seed=7)
+    rng = np.random.default_rng(11)
+    m.set_scaling(rng.normal(size=n_in), rng.uniform(0.5, 2, n_in), rng.normal(size=n_out), rng.uniform(0.5, 2, n_out))
+    m.set_params(rng.normal(scale=0.08, size=m.num_params()).astype(np.float32))
+    for n in (1, 127, 128, 129, 3000, 40000):
+        X = torch.from_numpy(rng.normal(size=(n, n_in)).astype(np.float32)).cuda()
+        a = torch.full((members, n, n_out), float("nan"), device="cuda")
+        b = torch.full((members, n, n_out), float("nan"), device="cuda")
+        m.predict(X, a)
+        m.predict_fused(X, b)
+        torch.cuda.synchronize()
+        assert torch.equal(a, b), (shape, n, (a - b).abs().max().item())
