@@ -316,6 +316,88 @@ def reacting_block(args, model, gate, local, dt=2e-8):
             "dt": dt, "after_steps": args.warmup + args.steps}
 
 
+BATCH_SIZES = ((64, 64, 64), (128, 64, 64), (192, 96, 96))
+
+
+def batch_specs(count=32, seed=5):
+    """The uneven batch: `count` shock-bubble instances with grids drawn from
+    BATCH_SIZES, shock Mach U[1.8, 3.5] and bubble radius U[4, 10] mm
+    (numpy.random.default_rng(seed)). Domains: 64 x 32 x 32 mm for the
+    elongated grids, 32 mm cubes for 64^3; the radius is scaled by
+    min(1, 0.3 L_y / 10 mm) so every bubble fits its domain."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        grid = BATCH_SIZES[int(rng.integers(len(BATCH_SIZES)))]
+        mach = float(rng.uniform(1.8, 3.5))
+        radius = float(rng.uniform(4e-3, 10e-3))
+        ext = (0.0, 0.032, 0.0, 0.032, 0.0, 0.032) if grid[0] == grid[1] else (0.0, 0.064, 0.0, 0.032, 0.0, 0.032)
+        out.append((grid, mach, radius * min(1.0, 0.3 * ext[3] / 10e-3), ext))
+    return out
+
+
+def batch_instances(args, model, gate, local, mech, count=32):
+    """The batched uneven shock-bubble workload: the instances of batch_specs,
+    learned chemistry + mixed precision, advanced together by one graph
+    launch per step (eu_batch), against running them one by one on the plain
+    FP64 stiff path. Aggregate cell-steps per device second of each, and each
+    instance's own step time one by one."""
+    import torch
+    import learned
+    built = []
+    for q, (grid, mach, radius, ext) in enumerate(batch_specs(count)):
+        x, y, z = (cases.node_coordinates(n, ext[2 * a], ext[2 * a + 1]) for a, n in enumerate(grid))
+        center_x = 0.55 * ext[1]
+        prim = cases.shock_bubble(x, y, z, mech["mw"], mech["ns"], mach=mach, radius=radius,
+                                  shock_x=center_x - radius - 2e-3, standoff=radius + 2e-3, seed=100 + q, band=0.5)
+        p, cs, T, E = eu3d.initial_state(mech, *grid, *prim)
+        dt = cases.cfl_dt(x, y, p[0], p[1], p[2], p[3], p[6], CFL)
+        built.append((grid, ext, state_dict((p, cs, T, E)), dt))
+    cells = [g[0] * g[1] * g[2] for g, _, _, _ in built]
+    total = sum(cells)
+
+    def solver(grid, ext, st, chem, prec):
+        s = eu3d.Solver(*grid, ext, precision=prec, chemistry=chem, arith="fast", device=local)
+        s.set_mechanism(mech)
+        s.set_state(st)
+        if chem == "learned":
+            learned.attach(s, model, gate)
+        return s
+
+    # one by one, plain FP64 stiff: each instance's own step time
+    single_ms = []
+    for (grid, ext, st, dt) in built:
+        s = solver(grid, ext, st, "stiff", "fp64")
+        s.step(args.warmup, dt)
+        r = s.step(args.steps, dt)
+        single_ms.append(r["device_ms"] / args.steps)
+        s.close()
+    torch.cuda.synchronize()
+    # together: learned + mixed, one graph launch per step
+    solvers = [solver(grid, ext, st, "learned", "mixed") for (grid, ext, st, _) in built]
+    dts = [dt for (_, _, _, dt) in built]
+    b = eu3d.Batch(solvers)
+    b.step(args.warmup, dts)
+    stats, ms = b.step(args.steps, dts)
+    b.close()
+    for s in solvers:
+        s.close()
+    one_by_one = total * args.steps / (sum(single_ms) * args.steps / 1e3) / 1e6
+    together = total * args.steps / (ms / 1e3) / 1e6
+    return {"instances": count, "cells": total, "grids": {f"{g[0]}x{g[1]}x{g[2]}": sum(1 for b_ in built if b_[0] == g)
+                                                           for g in BATCH_SIZES},
+            "learned_mixed_batch": {"value": round(together, 3), "ms_per_step": round(ms / args.steps, 4),
+                                    "launches_per_step": 1,
+                                    "learned_cells_last_step": int(sum(st_["learned"] for st_ in stats)),
+                                    "max_nchem": int(max(st_["max_nchem"] for st_ in stats))},
+            "plain_fp64_one_by_one": {"value": round(one_by_one, 3), "ms_per_step": round(sum(single_ms), 4),
+                                      "instance_ms_per_step": {"min": round(min(single_ms), 4),
+                                                               "median": round(float(np.median(single_ms)), 4),
+                                                               "max": round(max(single_ms), 4)}},
+            "speedup": round(together / one_by_one, 3), "steps": args.steps, "warmup": args.warmup,
+            "seed": 5, "unit": "Mcell-steps/s"}
+
+
 def our_arm(args):
     import torch
     world, rank, local, dist = dist_setup(args)
@@ -392,6 +474,11 @@ def our_arm(args):
     # -- reacting gas: the chemistry phase the learned model replaces ---------------------------
     block = reacting_block(args, model, gate, local) if args.chem == "learned" else None
 
+    # -- uneven instances advanced together (one graph launch per step) ----------------------
+    batch = None
+    if args.chem == "learned" and not args.no_batch:
+        batch = batch_instances(args, model, gate, local, mech)
+
     # -- per-kernel times (same stream, CUDA events around each kernel phase) -----------------
     sp = make_solver(args.chem, args.precision, args.arith, profile=True)
     sp.step(args.warmup, dt)
@@ -450,6 +537,7 @@ def our_arm(args):
                            "l2": f"inputs larger than L2: {sd['CS'].nbytes * 3 // 2**20} MiB state > 126 MiB"},
                 "plain_fp64": plain,
                 "reacting_block": block,
+                "batch_instances": batch,
                 "roofline": roofline, "kernels_ms_per_step": per_kernel,
                 "max_nchem": stats["max_nchem"], "reacting_cells": stats["reacting"],
                 "learned_cells": stats["learned"], "fallback_cells": stats["fallback"],
@@ -475,6 +563,7 @@ def main():
     ap.add_argument("--arith", choices=["strict", "fast"], default="fast")
     ap.add_argument("--grid", type=int, nargs=3, default=list(GRID))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-instance workload")
     args = ap.parse_args()
     if args.chem == "learned":
         sys.path.insert(0, os.path.join(ROOT, "eu3d-gpu_b200"))

@@ -114,6 +114,13 @@ def library():
         lib.eu_mlp_train.argtypes = [_P, _P, _P, ctypes.c_longlong, _I, _I, ctypes.c_float, ctypes.c_uint, _P]
         lib.eu_mlp_predict.argtypes = [_P, _P, ctypes.c_longlong, _P]
         lib.eu_mlp_predict_noalloc.argtypes = [_P, _P, ctypes.c_longlong, _P]
+        lib.eu_batch_create.argtypes = [ctypes.POINTER(_P), _I, ctypes.POINTER(_P)]
+        lib.eu_batch_step.argtypes = [_P, _I, ctypes.POINTER(_D), _P, ctypes.POINTER(_D)]
+        lib.eu_batch_destroy.argtypes = [_P]
+        lib.eu_batch_last_error.argtypes = [_P]
+        lib.eu_batch_last_error.restype = ctypes.c_char_p
+        for fn in ("eu_batch_create", "eu_batch_step", "eu_batch_destroy"):
+            getattr(lib, fn).restype = _I
         lib.eu_mlp_predict_fused.argtypes = [_P, _P, ctypes.c_longlong, _P]
         lib.eu_mlp_predict_fused.restype = _I
         lib.eu_mlp_predict_noalloc.restype = _I
@@ -318,6 +325,43 @@ class Solver:
         nbytes = ctypes.c_size_t()
         self._check(library().eu_device_info(self.h, ctypes.byref(stream), ctypes.byref(nbytes)))
         return stream.value, nbytes.value
+
+
+class Batch:
+    """eu_batch: independent solvers on one device advanced by one graph launch
+    per step (the instances' captured timesteps as parallel branches)."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+        arr = (_P * len(self.solvers))(*[s.h for s in self.solvers])
+        h = _P()
+        st = library().eu_batch_create(arr, len(self.solvers), ctypes.byref(h))
+        if st:
+            raise EU3DError(st, "eu_batch_create")
+        self.h = h
+
+    def step(self, nsteps, dt):
+        """dt: one value or one per instance. Returns (per-instance stats, device ms)."""
+        n = len(self.solvers)
+        dts = [float(dt)] * n if np.isscalar(dt) else [float(v) for v in dt]
+        darr = (_D * n)(*dts)
+        stats = (StepStats * n)()
+        ms = _D()
+        st = library().eu_batch_step(self.h, int(nsteps), darr, ctypes.cast(stats, _P), ctypes.byref(ms))
+        if st:
+            raise EU3DError(st, library().eu_batch_last_error(self.h).decode())
+        return [s.as_dict() for s in stats], ms.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            library().eu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Mlp:

@@ -57,6 +57,7 @@ struct eu_handle {
     cudaGraphExec_t graph_exec = nullptr;
     int graph_launches = 0;
     bool graph_dirty = true;
+    unsigned graph_gen = 0; // captures so far (batches rebuild when it changes)
     std::string err;
 };
 
@@ -732,6 +733,7 @@ eu_status capture_step(eu_handle *h, const LaunchArgs &a, const Launchers &L)
     CK(h, cudaGraphInstantiate(&h->graph_exec, g, 0));
     h->graph_launches = launches;
     h->graph_dirty = false;
+    ++h->graph_gen;
     return EU_OK;
 }
 
@@ -1177,6 +1179,210 @@ eu_status eu_device_info(const eu_handle *h, void **stream, size_t *device_bytes
     if (stream) *stream = h->stream;
     if (device_bytes) *device_bytes = h->bytes;
     return EU_OK;
+}
+
+} // extern "C"
+
+// ------------------------------------------------------------ instance batches
+// Several handles on one device advanced together: one CUDA graph whose
+// independent branches are the instances' captured timesteps, launched once
+// per step on the batch's own stream, so the kernels of different instances
+// overlap on the GPU. Each instance keeps its own buffers, queues and
+// statistics.
+struct eu_batch {
+    std::vector<eu_handle *> hs;
+    std::vector<unsigned> gens;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> joins; // one per instance
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::string err;
+};
+
+namespace {
+
+eu_status bfail(eu_batch *b, eu_status s, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    b->err = buf;
+    return s;
+}
+
+#define BCK(b, call)                                                                               \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return bfail((b), e_ == cudaErrorMemoryAllocation ? EU_ERR_OUT_OF_MEMORY : EU_ERR_CUDA, "%s: %s", #call, \
+                         cudaGetErrorString(e_));                                                  \
+    } while (0)
+
+void drop_batch_graph(eu_batch *b)
+{
+    if (b->exec)
+        cudaGraphExecDestroy(b->exec);
+    if (b->graph)
+        cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+} // namespace
+
+extern "C" {
+
+eu_status eu_batch_create(eu_handle *const *handles, int count, eu_batch **out)
+{
+    if (!handles || count < 1 || !out)
+        return EU_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    for (int i = 0; i < count; ++i) {
+        if (!handles[i] || handles[i]->cfg.device != handles[0]->cfg.device)
+            return EU_ERR_INVALID_ARGUMENT;
+        for (int j = 0; j < i; ++j)
+            if (handles[j] == handles[i])
+                return EU_ERR_INVALID_ARGUMENT;
+    }
+    eu_batch *b = new (std::nothrow) eu_batch;
+    if (!b)
+        return EU_ERR_OUT_OF_MEMORY;
+    b->hs.assign(handles, handles + count);
+    b->gens.assign(count, 0);
+    b->device = handles[0]->cfg.device;
+    b->joins.assign(count, nullptr);
+    bool ok = cudaSetDevice(b->device) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreate(&b->ev0) == cudaSuccess && cudaEventCreate(&b->ev1) == cudaSuccess;
+    for (int i = 0; ok && i < count; ++i)
+        ok = cudaEventCreateWithFlags(&b->joins[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        eu_batch_destroy(b);
+        return EU_ERR_CUDA;
+    }
+    *out = b;
+    return EU_OK;
+}
+
+eu_status eu_batch_destroy(eu_batch *b)
+{
+    if (!b)
+        return EU_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(b->device);
+    if (b->stream)
+        cudaStreamSynchronize(b->stream);
+    drop_batch_graph(b);
+    for (cudaEvent_t e : b->joins)
+        if (e) cudaEventDestroy(e);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return EU_OK;
+}
+
+const char *eu_batch_last_error(const eu_batch *b) { return b ? b->err.c_str() : kNoHandle; }
+
+eu_status eu_batch_step(eu_batch *b, int nsteps, const double *dt, eu_step_stats *stats, double *device_ms)
+{
+    if (!b || !dt || nsteps < 0)
+        return EU_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(b->device);
+    const int n = int(b->hs.size());
+    bool rebuild = !b->exec;
+    for (int i = 0; i < n; ++i) {
+        eu_handle *h = b->hs[i];
+        if (!(dt[i] > 0))
+            return bfail(b, EU_ERR_INVALID_ARGUMENT, "instance %d: dt must be > 0", i);
+        if (!h->has_mech || !h->has_state)
+            return bfail(b, EU_ERR_NOT_READY, "instance %d: mechanism and state must be set", i);
+        if (h->cfg.chemistry == EU_CHEM_LEARNED && (!h->model || !mlp_has_fused(h->model)))
+            return bfail(b, EU_ERR_UNSUPPORTED, "instance %d: learned chemistry needs a model with the fused kernel", i);
+        if (h->graph_dirty || !h->graph_exec) {
+            const eu_status s = capture_step(h, launch_args(h), flavour(h));
+            if (s != EU_OK)
+                return bfail(b, s, "instance %d: %s", i, h->err.c_str());
+        }
+        rebuild |= b->gens[i] != h->graph_gen;
+    }
+    if (rebuild) {
+        drop_batch_graph(b);
+        BCK(b, cudaGraphCreate(&b->graph, 0));
+        for (int i = 0; i < n; ++i) {
+            cudaGraphNode_t node;
+            BCK(b, cudaGraphAddChildGraphNode(&node, b->graph, nullptr, 0, b->hs[i]->graph));
+            b->gens[i] = b->hs[i]->graph_gen;
+        }
+        BCK(b, cudaGraphInstantiate(&b->exec, b->graph, 0));
+    }
+    // order after each instance's earlier work, set its dt and call counters
+    for (int i = 0; i < n; ++i) {
+        eu_handle *h = b->hs[i];
+        BCK(b, cudaEventRecord(b->joins[i], h->stream));
+        BCK(b, cudaStreamWaitEvent(b->stream, b->joins[i], 0));
+        BCK(b, cudaMemsetAsync(h->st.counters, 0, kCntCount * sizeof(unsigned long long), b->stream));
+        BCK(b, strict::launch_set_value(h->d_dt, dt[i], b->stream));
+        if (h->st.prim32 && nsteps > 0)
+            h->prim_stale = true;
+    }
+    BCK(b, cudaEventRecord(b->ev0, b->stream));
+    for (int q = 0; q < nsteps; ++q) BCK(b, cudaGraphLaunch(b->exec, b->stream));
+    BCK(b, cudaEventRecord(b->ev1, b->stream));
+    // later work on each instance's stream follows the batch
+    for (int i = 0; i < n; ++i) BCK(b, cudaStreamWaitEvent(b->hs[i]->stream, b->ev1, 0));
+    if (!stats && !device_ms)
+        return EU_OK;
+    std::vector<unsigned long long> cnt(size_t(n) * kCntCount);
+    std::vector<int> queued(n, 0), model_err(n, 0);
+    for (int i = 0; i < n; ++i) {
+        eu_handle *h = b->hs[i];
+        BCK(b, cudaMemcpyAsync(&cnt[size_t(i) * kCntCount], h->st.counters, kCntCount * sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, b->stream));
+        if (h->cfg.chemistry == EU_CHEM_LEARNED && nsteps > 0) {
+            BCK(b, cudaMemcpyAsync(&queued[i], h->lp.counts, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+            BCK(b, cudaMemcpyAsync(&model_err[i], mlp_error_flag(h->model), sizeof(int), cudaMemcpyDeviceToHost,
+                                   b->stream));
+        }
+    }
+    BCK(b, cudaStreamSynchronize(b->stream));
+    float ms = 0;
+    BCK(b, cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    if (device_ms)
+        *device_ms = ms;
+    eu_status worst = EU_OK;
+    for (int i = 0; i < n; ++i) {
+        eu_handle *h = b->hs[i];
+        const unsigned long long *c = &cnt[size_t(i) * kCntCount];
+        if (stats) {
+            eu_step_stats &st = stats[i];
+            std::memset(&st, 0, sizeof st);
+            st.steps = nsteps;
+            st.max_nchem = int(c[kCntMaxNchem]);
+            st.sum_nchem = (long long)c[kCntSumNchem];
+            st.reacting = h->cfg.chemistry == EU_CHEM_STIFF ? (long long)h->ni * h->nj * h->nk : queued[i];
+            st.learned = (long long)c[kCntLearned];
+            st.fallback = (long long)c[kCntFallback];
+            st.nonfinite = (long long)c[kCntNonfinite];
+            st.device_ms = ms;
+            st.launches = nsteps * h->graph_launches;
+        }
+        eu_status s = EU_OK;
+        if (model_err[i])
+            s = fail(h, EU_ERR_TIMEOUT, "a tensor-core pipeline wait of the learned model gave up");
+        else if (c[kCntNonfinite])
+            s = fail(h, EU_ERR_NONFINITE, "%llu cells with non-finite density or temperature", c[kCntNonfinite]);
+        else if (c[kCntBadNchem])
+            s = fail(h, EU_ERR_NCHEM, "%llu cells predicted Nchem <= 0 or above max_substeps", c[kCntBadNchem]);
+        if (s != EU_OK && worst == EU_OK) {
+            worst = s;
+            bfail(b, s, "instance %d: %s", i, h->err.c_str());
+        }
+    }
+    return worst;
 }
 
 } // extern "C"

@@ -307,6 +307,22 @@ typedef struct {
 
 eu_status eu_set_learned(eu_handle *h, eu_mlp *model, const eu_learned_config *cfg);
 
+/* Batches of independent instances (any grid sizes, any modes) on one device,
+ * advanced together: each step is one launch of a CUDA graph whose branches
+ * are the instances' captured timesteps, so small and uneven instances share
+ * the GPU instead of running one after another. No counterpart in the
+ * reference (one grid per run; its multi-block runs are MPI ranks).
+ * eu_batch_step: dt[count] per instance; stats[count] (or NULL) per instance;
+ * device_ms (or NULL) the device time of the whole call. The handles stay
+ * usable on their own between batch calls (the batch orders itself after
+ * their earlier work and their later work after it). Learned instances need a
+ * model with the fused inference kernel. Destroy the batch before its handles. */
+typedef struct eu_batch eu_batch;
+eu_status eu_batch_create(eu_handle *const *handles, int count, eu_batch **out);
+eu_status eu_batch_step(eu_batch *b, int nsteps, const double *dt, eu_step_stats *stats, double *device_ms);
+const char *eu_batch_last_error(const eu_batch *b);
+eu_status eu_batch_destroy(eu_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -159,3 +159,45 @@ def test_graph_replay_equals_eager_launches(gpu, chemistry, precision):
     assert out[False][0] == out[True][0]
     for a, b in zip(out[False][1:], out[True][1:]):
         assert n_unequal(a, b) == 0
+
+
+def test_batch_of_uneven_instances_equals_one_by_one(gpu):
+    """A batch of instances of different sizes and modes (stiff FP64, learned +
+    mixed, frozen) advanced by one graph launch per step gives each instance
+    bitwise the state and statistics it reaches stepping alone, and the
+    handles stay usable on their own between batch calls."""
+    import learned
+    model, gate = learned.load()
+    mech = gpu.parse_mechanism(cases.MECH_JA919, cases.THERMO)
+    specs = [((24, 8, 8), "stiff", "fp64", 2e-8), ((16, 12, 8), "learned", "mixed", 3e-8),
+             ((20, 6, 10), "frozen", "mixed", 2e-8), ((8, 8, 8), "learned", "fp64", 1e-8)]
+
+    def make():
+        out = []
+        for (ni, nj, nk), chem, prec, _ in specs:
+            s = gpu.Solver(ni, nj, nk, (0.0, ni * 1e-3, 0.0, nj * 1e-3, 0.0, nk * 1e-3), chemistry=chem,
+                           precision=prec, arith="fast")
+            s.set_mechanism(mech)
+            s.set_primitive(*cases.hot_reacting_block(ni + 4, nj + 4, nk + 4, mech["mw"], mech["ns"]))
+            if chem == "learned":
+                learned.attach(s, model, gate)
+            out.append(s)
+        return out
+
+    alone = make()
+    ref_stats = [s.step(3, spec[3]) for s, spec in zip(alone, specs)]
+    for s, spec in zip(alone, specs):
+        s.step(1, spec[3])
+    together = make()
+    b = gpu.Batch(together)
+    stats, ms = b.step(3, [spec[3] for spec in specs])
+    assert ms > 0
+    for s, spec in zip(together, specs):  # on their own between batch calls
+        s.step(1, spec[3])
+    keep = ("max_nchem", "sum_nchem", "learned", "fallback")
+    for got, want in zip(stats, ref_stats):
+        assert {k: got[k] for k in keep} == {k: want[k] for k in keep}
+    for a, c in zip(alone, together):
+        for f in ("CS", "T", "Yi"):
+            assert n_unequal(a.get(f), c.get(f)) == 0, f
+    b.close()
