@@ -128,12 +128,13 @@ __device__ __forceinline__ void face_flux(const R *__restrict__ prim, long long 
 // then CS += RHS, src/Flowfield.cpp:1350-1354) with every face flux formed once.
 //
 // A block owns a kFluxTJ x kFluxTK tile of (j, k) columns and marches along x
-// over kFluxCI nodes. The x-face flux at i-1/2 stays in registers from the
+// over ci nodes (a launch parameter the autotuner picks). The x-face flux at
+// i-1/2 stays in registers from the
 // previous node; the y- and z-face fluxes of the current plane go through
 // shared memory (row 0 / column 0 hold the faces below the tile, computed by
 // warp 0 and by eight lanes of warp 1). RHS keeps the reference's order
 // -dt/dx (F+ - F-) - dt/dy (G+ - G-) - dt/dz (Q+ - Q-), accumulated in FP64.
-constexpr int kFluxTK = 32, kFluxTJ = 8, kFluxCI = 16;
+constexpr int kFluxTK = 32, kFluxTJ = 8;
 
 template <int NS, typename R>
 constexpr size_t flux_smem_bytes()
@@ -143,7 +144,8 @@ constexpr size_t flux_smem_bytes()
 
 template <int NS, typename R, bool kStrict>
 __global__ void __launch_bounds__(kFluxTK *kFluxTJ, 1)
-    k_flux_update(const DevGrid g, const DevState st, const R *__restrict__ prim, const double *__restrict__ dt_dev)
+    k_flux_update(const DevGrid g, const DevState st, const R *__restrict__ prim, const double *__restrict__ dt_dev,
+                  int ci)
 {
     constexpr int NV = NS + 4;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -155,8 +157,8 @@ __global__ void __launch_bounds__(kFluxTK *kFluxTJ, 1)
     const int k0 = blockIdx.x * kFluxTK, j0 = blockIdx.y * kFluxTJ;
     const int k = g.bc + k0 + tx, j = g.bc + j0 + ty;
     const bool valid = (k0 + tx < g.nk) && (j0 + ty < g.nj);
-    const int i_begin = g.bc + blockIdx.z * kFluxCI;
-    const int i_end = min(i_begin + kFluxCI, g.bc + g.ni);
+    const int i_begin = g.bc + blockIdx.z * ci;
+    const int i_end = min(i_begin + ci, g.bc + g.ni);
     const long long n3 = g.n3, sx = (long long)g.ny * g.nz, sy = g.nz;
     const double dt = *dt_dev;
     const double cy = valid ? dt / (g.y[j] - g.y[j - 1]) : 0.0;
@@ -229,7 +231,7 @@ __global__ void __launch_bounds__(kFluxTK *kFluxTJ, 1)
 // is the y face below tile row r (r = kTileJ: above the last row), sQ[q][r][c]
 // the z face left of column c. Partial tiles: the faces of the valid
 // rows/columns are formed, including the one past the last valid row/column.
-constexpr int kTileK = 32, kTileJ = 8, kTileCI = 16;
+constexpr int kTileK = 32, kTileJ = 8;
 constexpr int kTileRows = kTileJ + 4, kTileCols = kTileK + 4;
 constexpr int kTileHalo = 4 * kTileCols + 4 * kTileJ; // two rows above, two below, two columns each side
 
@@ -256,7 +258,8 @@ __device__ __forceinline__ void window_face_flux(const R (&w)[4][7 + NS], R (&F)
 
 template <int NS, typename R, bool kStrict>
 __global__ void __launch_bounds__(kTileK *kTileJ, 2)
-    k_flux_update_tiled(const DevGrid g, const DevState st, const R *__restrict__ prim, const double *__restrict__ dt_dev)
+    k_flux_update_tiled(const DevGrid g, const DevState st, const R *__restrict__ prim, const double *__restrict__ dt_dev,
+                        int ci)
 {
     constexpr int NP = 7 + NS, NV = NS + 4;
     using Plane = R[NP][kTileRows][kTileCols];
@@ -299,8 +302,8 @@ __global__ void __launch_bounds__(kTileK *kTileJ, 2)
     const double dt = *dt_dev;
     const double cy = valid ? dt / (g.y[j] - g.y[j - 1]) : 0.0;
     const double cz = valid ? dt / (g.z[k] - g.z[k - 1]) : 0.0;
-    const int i_begin = g.bc + blockIdx.z * kTileCI;
-    const int i_end = min(i_begin + kTileCI, g.bc + g.ni);
+    const int i_begin = g.bc + blockIdx.z * ci;
+    const int i_end = min(i_begin + ci, g.bc + g.ni);
     const long long col = resident ? cell_index(g, 0, j, k) : 0;
     const long long hcol = halo ? cell_index(g, 0, hj, hk) : 0;
 

@@ -42,9 +42,9 @@ cudaError_t flux_launch(const LaunchArgs &a, const R *prim)
         configured = true;
     }
     const dim3 block(kFluxTK, kFluxTJ);
-    const dim3 grid((g.nk + kFluxTK - 1) / kFluxTK, (g.nj + kFluxTJ - 1) / kFluxTJ,
-                    (g.ni + kFluxCI - 1) / kFluxCI);
-    k_flux_update<NS, R, kStrict><<<grid, block, smem, a.stream>>>(g, a.st, prim, a.dt_dev);
+    const int ci = a.flux_ci > 0 ? a.flux_ci : 16;
+    const dim3 grid((g.nk + kFluxTK - 1) / kFluxTK, (g.nj + kFluxTJ - 1) / kFluxTJ, (g.ni + ci - 1) / ci);
+    k_flux_update<NS, R, kStrict><<<grid, block, smem, a.stream>>>(g, a.st, prim, a.dt_dev, ci);
     return cudaGetLastError();
 }
 
@@ -62,8 +62,9 @@ cudaError_t tiled_flux_launch(const LaunchArgs &a, const R *prim)
         configured = true;
     }
     const dim3 block(kTileK, kTileJ);
-    const dim3 grid((g.nk + kTileK - 1) / kTileK, (g.nj + kTileJ - 1) / kTileJ, (g.ni + kTileCI - 1) / kTileCI);
-    k_flux_update_tiled<NS, R, kStrict><<<grid, block, smem, a.stream>>>(g, a.st, prim, a.dt_dev);
+    const int ci = a.flux_ci > 0 ? a.flux_ci : 16;
+    const dim3 grid((g.nk + kTileK - 1) / kTileK, (g.nj + kTileJ - 1) / kTileJ, (g.ni + ci - 1) / ci);
+    k_flux_update_tiled<NS, R, kStrict><<<grid, block, smem, a.stream>>>(g, a.st, prim, a.dt_dev, ci);
     return cudaGetLastError();
 }
 
@@ -82,7 +83,7 @@ cudaError_t react_t(const LaunchArgs &a, bool react)
 {
     const DevGrid &g = a.g;
     const long long n = (long long)g.ni * g.nj * g.nk;
-    const int threads = 128;
+    const int threads = a.recover_block > 0 ? a.recover_block : 128;
     const long long blocks = (n + threads - 1) / threads;
     const dim3 grid((unsigned)blocks);
     if (!react)
@@ -119,7 +120,9 @@ template <int NS, int NR>
 cudaError_t classify_t(const LaunchArgs &a, const LearnedParams &lp)
 {
     const long long n = (long long)a.g.ni * a.g.nj * a.g.nk;
-    k_recover_classify<NS><<<dim3(unsigned((n + 127) / 128)), 128, 0, a.stream>>>(*a.mech, a.g, a.st, lp);
+    const int threads = a.recover_block > 0 ? a.recover_block : 128;
+    k_recover_classify<NS><<<dim3(unsigned((n + threads - 1) / threads)), threads, 0, a.stream>>>(*a.mech, a.g, a.st,
+                                                                                                  lp);
     return cudaGetLastError();
 }
 

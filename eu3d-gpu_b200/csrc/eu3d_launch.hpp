@@ -19,6 +19,8 @@ struct LaunchArgs {
     int chemistry; // eu_chemistry
     int spec;      // 1: tables are bitwise H2_JA919, use the generated rate code
     int sms;       // multiprocessors of the device (fixed grids of the queue kernels)
+    int flux_ci;   // nodes each flux block marches along x (autotuned; 0: 16)
+    int recover_block; // threads per block of the recovery kernels, 32..128 (autotuned; 0: 128)
     cudaStream_t stream;
 };
 

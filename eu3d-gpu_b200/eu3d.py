@@ -50,6 +50,18 @@ class LearnedConfig(ctypes.Structure):
                 ("box_hi", _P), ("out_scale", _P), ("out_eps", _P), ("out_bound", _P)]
 
 
+class TuneReport(ctypes.Structure):
+    _fields_ = [("flux_candidates", _I), ("flux_ci", _I * 16), ("flux_ms", ctypes.c_float * 16),
+                ("recover_candidates", _I), ("recover_block", _I * 8), ("recover_ms", ctypes.c_float * 8),
+                ("chosen_flux_ci", _I), ("chosen_recover_block", _I)]
+
+    def as_dict(self):
+        nf, nr = self.flux_candidates, self.recover_candidates
+        return {"flux_ms": {int(self.flux_ci[q]): round(float(self.flux_ms[q]), 4) for q in range(nf)},
+                "recover_ms": {int(self.recover_block[q]): round(float(self.recover_ms[q]), 4) for q in range(nr)},
+                "flux_ci": self.chosen_flux_ci, "recover_block": self.chosen_recover_block}
+
+
 class StepStats(ctypes.Structure):
     _fields_ = [("steps", _I), ("max_nchem", _I), ("sum_nchem", ctypes.c_longlong),
                 ("reacting", ctypes.c_longlong), ("learned", ctypes.c_longlong), ("fallback", ctypes.c_longlong),
@@ -114,6 +126,8 @@ def library():
         lib.eu_mlp_train.argtypes = [_P, _P, _P, ctypes.c_longlong, _I, _I, ctypes.c_float, ctypes.c_uint, _P]
         lib.eu_mlp_predict.argtypes = [_P, _P, ctypes.c_longlong, _P]
         lib.eu_mlp_predict_noalloc.argtypes = [_P, _P, ctypes.c_longlong, _P]
+        lib.eu_autotune.argtypes = [_P, _I, _P]
+        lib.eu_autotune.restype = _I
         lib.eu_batch_create.argtypes = [ctypes.POINTER(_P), _I, ctypes.POINTER(_P)]
         lib.eu_batch_step.argtypes = [_P, _I, ctypes.POINTER(_D), _P, ctypes.POINTER(_D)]
         lib.eu_batch_destroy.argtypes = [_P]
@@ -307,6 +321,13 @@ class Solver:
                             *[None if v is None else v.ctypes.data for v in keep])
         self._model = model
         self._check(library().eu_set_learned(self.h, model.h, ctypes.byref(cfg)), "set_learned")
+
+    def autotune(self, reps=10):
+        """eu_autotune: pick the flux march length and recovery block size by
+        timing them on the current state (restored afterwards)."""
+        rep = TuneReport()
+        self._check(library().eu_autotune(self.h, int(reps), ctypes.cast(ctypes.byref(rep), _P)), "autotune")
+        return rep.as_dict()
 
     def write_state(self, path, iteration=0, num=0, final_time=0.0, dt=0.0):
         """EU3D_STATE_V1_LE dump of the current state (the reference's format)."""

@@ -8,7 +8,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -58,6 +61,8 @@ struct eu_handle {
     int graph_launches = 0;
     bool graph_dirty = true;
     unsigned graph_gen = 0; // captures so far (batches rebuild when it changes)
+    // launch shapes picked by eu_autotune (0: defaults)
+    int flux_ci = 0, recover_block = 0;
     std::string err;
 };
 
@@ -217,8 +222,19 @@ LaunchArgs launch_args(eu_handle *h)
     a.chemistry = h->cfg.chemistry;
     a.spec = h->spec;
     a.sms = h->sms;
+    a.flux_ci = h->flux_ci;
+    a.recover_block = h->recover_block;
     a.stream = h->stream;
     return a;
+}
+
+using TuneKey = std::tuple<int, int, int, int, int, int, int>;
+std::mutex g_tune_mutex;                            // guards g_tuned
+std::map<TuneKey, std::pair<int, int>> g_tuned;     // (flux_ci, recover_block) per grid and mode
+
+TuneKey tune_key(const eu_handle *h)
+{
+    return TuneKey(h->ni, h->nj, h->nk, h->cfg.precision, h->cfg.arith, h->cfg.chemistry, h->cfg.device);
 }
 
 void drop_graph(eu_handle *h)
@@ -421,6 +437,14 @@ eu_status eu_create(const eu_config *cfg, eu_handle **out)
     h->g.x = h->d_xyz;
     h->g.y = h->d_xyz + h->nx;
     h->g.z = h->d_xyz + h->nx + h->ny;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tuned.find(tune_key(h));
+        if (it != g_tuned.end()) {
+            h->flux_ci = it->second.first;
+            h->recover_block = it->second.second;
+        }
+    }
     *out = h;
     return EU_OK;
 }
@@ -1383,6 +1407,139 @@ eu_status eu_batch_step(eu_batch *b, int nsteps, const double *dt, eu_step_stats
         }
     }
     return worst;
+}
+
+} // extern "C"
+
+// ------------------------------------------------------------------ autotuner
+// Launch shapes that change no arithmetic (every candidate gives bitwise the
+// same state), timed on the handle's own state, which is restored afterwards:
+// the x-march length of the flux kernels (the block count's fit to the SMs
+// against each block's prologue of four planes) and the block size of the
+// recovery kernels. Choices are kept per grid and mode for the process, so
+// later handles of the same shape start from them.
+extern "C" {
+
+eu_status eu_autotune(eu_handle *h, int reps, eu_tune_report *report)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (reps < 1 || reps > 1000)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "reps must be 1..1000");
+    if (!h->has_mech || !h->has_state)
+        return fail(h, EU_ERR_NOT_READY, "mechanism and state must be set before tuning");
+    if (h->cfg.chemistry == EU_CHEM_LEARNED && !h->model)
+        return fail(h, EU_ERR_NOT_READY, "learned chemistry needs eu_set_learned first");
+    cudaSetDevice(h->cfg.device);
+    CK(h, cudaStreamSynchronize(h->stream));
+    const long long n3 = h->n3;
+    const int ns = h->mech.ns;
+    // snapshot of everything a flux or recovery launch writes
+    struct Part { void *p; size_t bytes; };
+    std::vector<Part> parts = {{h->st.cs, size_t(ns + 4) * n3 * 8}, {h->st.T, size_t(n3) * 8},
+                               {h->st.E, size_t(n3) * 8}, {h->st.prim, size_t(7 + ns) * n3 * 8},
+                               {h->st.nchem, size_t(n3) * 4}};
+    if (h->st.prim32)
+        parts.push_back({h->st.prim32, size_t(7 + ns) * n3 * 4});
+    size_t total = 0;
+    for (const Part &q : parts) total += q.bytes;
+    unsigned char *snap = nullptr;
+    CK(h, cudaMalloc(&snap, total));
+    size_t off = 0;
+    cudaError_t e = cudaSuccess;
+    for (const Part &q : parts) {
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(snap + off, q.p, q.bytes, cudaMemcpyDeviceToDevice, h->stream);
+        off += q.bytes;
+    }
+    const int ci_cand[] = {8, 12, 16, 20, 24, 29, 32, 43, 64};
+    const int rb_cand[] = {64, 96, 128};
+    eu_tune_report rep;
+    std::memset(&rep, 0, sizeof rep);
+    LaunchArgs a = launch_args(h);
+    const Launchers &L = flavour(h);
+    const bool learned = h->cfg.chemistry == EU_CHEM_LEARNED;
+    auto time_it = [&](auto &&launch, float *ms) -> cudaError_t {
+        cudaError_t r = launch(); // warm-up
+        if (r == cudaSuccess) r = cudaEventRecord(h->ev0, h->stream);
+        for (int q = 0; q < reps && r == cudaSuccess; ++q) r = launch();
+        if (r == cudaSuccess) r = cudaEventRecord(h->ev1, h->stream);
+        if (r == cudaSuccess) r = cudaEventSynchronize(h->ev1);
+        if (r == cudaSuccess) r = cudaEventElapsedTime(ms, h->ev0, h->ev1);
+        *ms /= reps;
+        return r;
+    };
+    int best_ci = 16, best_rb = 128;
+    float best = 1e30f;
+    for (int ci : ci_cand) {
+        if (e != cudaSuccess || ci > h->ni + 15)
+            continue;
+        a.flux_ci = ci;
+        float ms = 0;
+        e = time_it([&] { return L.flux_update(a); }, &ms);
+        if (rep.flux_candidates < 16) {
+            rep.flux_ci[rep.flux_candidates] = ci;
+            rep.flux_ms[rep.flux_candidates++] = ms;
+        }
+        if (ms < best) {
+            best = ms;
+            best_ci = ci;
+        }
+    }
+    a.flux_ci = best_ci;
+    // the flux launches moved the conserved state: back to the snapshot
+    // before timing the recovery on it
+    auto restore = [&] {
+        size_t o = 0;
+        for (const Part &q : parts) {
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(q.p, snap + o, q.bytes, cudaMemcpyDeviceToDevice, h->stream);
+            o += q.bytes;
+        }
+    };
+    restore();
+    best = 1e30f;
+    for (int rb : rb_cand) {
+        if (e != cudaSuccess)
+            break;
+        a.recover_block = rb;
+        float ms = 0;
+        e = time_it(
+            [&] {
+                if (learned) {
+                    cudaError_t r = cudaMemsetAsync(h->lp.counts, 0, 3 * sizeof(int), h->stream);
+                    return r == cudaSuccess ? L.recover_classify(a, h->lp) : r;
+                }
+                return L.recover_react(a, false);
+            },
+            &ms);
+        if (rep.recover_candidates < 8) {
+            rep.recover_block[rep.recover_candidates] = rb;
+            rep.recover_ms[rep.recover_candidates++] = ms;
+        }
+        if (ms < best) {
+            best = ms;
+            best_rb = rb;
+        }
+    }
+    restore();
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(h->stream);
+    cudaFree(snap);
+    if (e != cudaSuccess)
+        return cuda_fail(h, e, "autotune");
+    h->flux_ci = best_ci;
+    h->recover_block = best_rb;
+    h->graph_dirty = true;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tuned[tune_key(h)] = {best_ci, best_rb};
+    }
+    rep.chosen_flux_ci = best_ci;
+    rep.chosen_recover_block = best_rb;
+    if (report)
+        *report = rep;
+    return EU_OK;
 }
 
 } // extern "C"

@@ -307,6 +307,25 @@ typedef struct {
 
 eu_status eu_set_learned(eu_handle *h, eu_mlp *model, const eu_learned_config *cfg);
 
+/* Autotuner: times the launch shapes that change no arithmetic (every
+ * candidate gives bitwise the same state) on the handle's current state, which
+ * it restores: the x-march length of the flux kernels and the block size of
+ * the recovery kernels. The choice applies to this handle and to handles
+ * created later in the process with the same grid and mode. reps: timed
+ * launches per candidate. report (or NULL) receives the candidates' times.
+ * Allocates a temporary copy of the state. No counterpart in the reference. */
+typedef struct {
+    int flux_candidates;
+    int flux_ci[16];
+    float flux_ms[16];
+    int recover_candidates;
+    int recover_block[8];
+    float recover_ms[8];
+    int chosen_flux_ci;
+    int chosen_recover_block;
+} eu_tune_report;
+eu_status eu_autotune(eu_handle *h, int reps, eu_tune_report *report);
+
 /* Batches of independent instances (any grid sizes, any modes) on one device,
  * advanced together: each step is one launch of a CUDA graph whose branches
  * are the instances' captured timesteps, so small and uneven instances share

@@ -185,3 +185,31 @@ def test_mixed_stiff_heavy_cells_match_fp64(gpu):
     l1 = np.abs(out["mixed"][0] - out["fp64"][0]).sum(axis=0)
     terr = np.abs(out["mixed"][1] - out["fp64"][1]) / out["fp64"][1]
     assert l1.mean() <= 1e-4 and terr.max() <= 1e-4, (l1.mean(), l1.max(), terr.max(), peak)
+
+
+@pytest.mark.parametrize("precision,arith", [("mixed", "fast"), ("fp64", "strict")])
+def test_autotuned_launch_shapes_change_no_bits(gpu, precision, arith):
+    """Every launch shape the autotuner may pick gives bitwise the same state:
+    steps after tuning equal steps with the default shapes, and tuning leaves
+    the state it timed on unchanged (ragged grid: 40 x 21 x 45 nodes)."""
+    ni, nj, nk = 40, 21, 45
+    ext = (0.0, 0.02, 0.0, 0.01, 0.0, 0.012)
+    x, y, z = (cases.node_coordinates(n, a, b) for n, a, b in ((ni, 0, 0.02), (nj, 0, 0.01), (nk, 0, 0.012)))
+    mech = gpu.parse_mechanism(cases.MECH_JA919, cases.THERMO)
+    prim = cases.shock_bubble(x, y, z, mech["mw"], mech["ns"], radius=3e-3, shock_x=3e-3, standoff=5e-3, seed=5)
+    out = []
+    for tune in (False, True):
+        s = gpu.Solver(ni, nj, nk, ext, precision=precision, arith=arith)
+        s.set_mechanism(mech)
+        s.set_primitive(*prim)
+        s.step(1, 2e-8)
+        before = s.get("CS")
+        if tune:
+            rep = s.autotune(reps=2)
+            assert len(rep["flux_ms"]) >= 5 and rep["flux_ci"] in rep["flux_ms"], rep
+            assert n_unequal(s.get("CS"), before) == 0
+        s.step(4, 2e-8)
+        out.append((s.get("CS"), s.get("T")))
+        s.close()
+    for a, b in zip(*out):
+        assert n_unequal(a, b) == 0
