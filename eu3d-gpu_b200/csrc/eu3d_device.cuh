@@ -20,6 +20,22 @@ __device__ __forceinline__ long long cell_index(const DevGrid &g, int i, int j, 
     return ((long long)i * g.ny + j) * g.nz + k;
 }
 
+// floor(n / f.d) for n < 2^31 (see FastDiv)
+__device__ __forceinline__ int fdiv(long long n, const FastDiv &f)
+{
+    return int((static_cast<unsigned long long>(n) * f.m) >> (32 + f.s));
+}
+
+// Interior node (i, j, k) of flat interior index t (k fastest), ghosts offset.
+__device__ __forceinline__ void interior_node(const DevGrid &g, long long t, int &i, int &j, int &k)
+{
+    const int ij = fdiv(t, g.d_nk);
+    i = fdiv(t, g.d_njnk);
+    k = g.bc + int(t - (long long)ij * g.nk);
+    j = g.bc + (ij - i * g.nj);
+    i += g.bc;
+}
+
 // Reciprocal of a nonzero, non-denormal double by the hardware approximation
 // (rcp.approx.ftz.f64) refined with two Newton-Raphson steps
 // y <- y + y (1 - a y); relative error near one unit in the last place.

@@ -39,18 +39,18 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
     double sv = 1, sw = 1;
     bool rebuild = false;
     if (t < nxf) {
-        const int k = bc + int(t % nk);
-        const int j = bc + int((t / nk) % nj);
-        const int q = int(t / ((long long)nk * nj)); // 0 .. 2bc-1
+        const int jk = fdiv(t, g.d_nk), q = fdiv(t, g.d_njnk); // q: 0 .. 2bc-1
+        const int k = bc + int(t - (long long)jk * nk);
+        const int j = bc + (jk - q * nj);
         const int i = q < bc ? q : ni + q;           // ghost index
         const int si = q < bc ? 2 * bc - 1 - i : 2 * (ni + bc) - 1 - i;
         dst = cell_index(g, i, j, k);
         src = cell_index(g, si, j, k);
     } else if (t < nxf + nyf) {
         t -= nxf;
-        const int k = bc + int(t % nk);
-        const int i = bc + int((t / nk) % ni);
-        const int q = int(t / ((long long)nk * ni));
+        const int ik = fdiv(t, g.d_nk), q = fdiv(t, g.d_nink);
+        const int k = bc + int(t - (long long)ik * nk);
+        const int i = bc + (ik - q * ni);
         const int j = q < bc ? q : nj + q;
         const int sj = q < bc ? 2 * bc - 1 - j : 2 * (nj + bc) - 1 - j;
         dst = cell_index(g, i, j, k);
@@ -63,9 +63,10 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
         // the ghost index runs fastest: the 2 bc ghosts of one (i, j) row sit in
         // two contiguous pairs, so a warp touches 16 pairs instead of 32 rows
         t -= nxf + nyf;
-        const int q = int(t % (2 * bc));
-        const int j = bc + int((t / (2 * bc)) % nj);
-        const int i = bc + int(t / (2LL * bc * nj));
+        const int jq = fdiv(t, g.d_ghost), ii = fdiv(t, g.d_ghost_nj);
+        const int q = int(t - (long long)jq * (2 * bc));
+        const int j = bc + (jq - ii * nj);
+        const int i = bc + ii;
         const int k = q < bc ? q : nk + q;
         const int sk = q < bc ? 2 * bc - 1 - k : 2 * (nk + bc) - 1 - k;
         dst = cell_index(g, i, j, k);
@@ -635,7 +636,8 @@ __global__ void __launch_bounds__(128) k_materialize(const __grid_constant__ Dev
     if (c >= g.n3)
         return;
     const long long n3 = g.n3;
-    const int k = int(c % g.nz), j = int((c / g.nz) % g.ny), i = int(c / ((long long)g.nz * g.ny));
+    const int jk = fdiv(c, g.d_nz), i = fdiv(c, g.d_nynz);
+    const int k = int(c - (long long)jk * g.nz), j = jk - i * g.ny;
     const bool interior = i >= g.bc && i < g.bc + g.ni && j >= g.bc && j < g.bc + g.nj && k >= g.bc &&
                           k < g.bc + g.nk;
     if (!interior) {
@@ -673,9 +675,8 @@ __global__ void __launch_bounds__(128) k_recover_react(const __grid_constant__ D
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ncell)
         return;
-    const int k = g.bc + int(t % g.nk);
-    const int j = g.bc + int((t / g.nk) % g.nj);
-    const int i = g.bc + int(t / ((long long)g.nk * g.nj));
+    int i, j, k;
+    interior_node(g, t, i, j, k);
     const long long n3 = g.n3;
     const long long c = cell_index(g, i, j, k);
     CellState<NS> cell;
@@ -704,9 +705,8 @@ __global__ void __launch_bounds__(128, 5) k_recover_classify(const __grid_consta
     bool active = false;
     long long c = 0;
     if (t < ncell) {
-        const int k = g.bc + int(t % g.nk);
-        const int j = g.bc + int((t / g.nk) % g.nj);
-        const int i = g.bc + int(t / ((long long)g.nk * g.nj));
+        int i, j, k;
+        interior_node(g, t, i, j, k);
         const long long n3 = g.n3;
         c = cell_index(g, i, j, k);
         CellState<NS> cell;

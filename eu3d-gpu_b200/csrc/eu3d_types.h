@@ -30,11 +30,29 @@ struct DevMech {
     int has_tb[kMaxR];
 };
 
+// Division of an index n < 2^31 by a fixed divisor d >= 1 without a divide
+// instruction: q = (n m) >> (32 + s) with s = ceil(log2 d), m = 2^(32+s) / d + 1.
+// For n < 2^32 <= 2^(32+s)/d the rounding error n (m - 2^(32+s)/d) / 2^(32+s) stays
+// below 1/d, so q = floor(n / d); n m < 2^31 2^33 fits 64 bits.
+struct FastDiv {
+    unsigned long long m;
+    unsigned d;
+    int s;
+};
+inline FastDiv make_fastdiv(unsigned d)
+{
+    int s = 0;
+    while ((1ull << s) < d) ++s;
+    return FastDiv{(1ull << (32 + s)) / d + 1, d, s};
+}
+
 // Grid and field pointers of one handle (all device memory).
 struct DevGrid {
     int ni, nj, nk, bc, nx, ny, nz;
     long long n3;
     const double *x, *y, *z; // node coordinates with ghosts
+    // index decompositions of the kernels' flat thread indices
+    FastDiv d_nk, d_njnk, d_nink, d_ghost, d_ghost_nj, d_nz, d_nynz;
 };
 
 // Primitive planes the stencils read, in this order (haloed, FP64).

@@ -369,6 +369,9 @@ eu_status eu_create(const eu_config *cfg, eu_handle **out)
     *out = nullptr;
     if (cfg->bc != 2 || cfg->total_ni < 2 || cfg->total_nj < 2 || cfg->total_nk < 2)
         return EU_ERR_INVALID_ARGUMENT;
+    // the kernels' flat node indices stay below 2^31
+    if ((long long)(cfg->total_ni + 4) * (cfg->total_nj + 4) * (cfg->total_nk + 4) >= (1LL << 31))
+        return EU_ERR_INVALID_ARGUMENT;
     if (cfg->precision != EU_PREC_FP64 && cfg->precision != EU_PREC_MIXED)
         return EU_ERR_INVALID_ARGUMENT;
     if (cfg->chemistry != EU_CHEM_STIFF && cfg->chemistry != EU_CHEM_FROZEN && cfg->chemistry != EU_CHEM_LEARNED)
@@ -437,6 +440,13 @@ eu_status eu_create(const eu_config *cfg, eu_handle **out)
     h->g.x = h->d_xyz;
     h->g.y = h->d_xyz + h->nx;
     h->g.z = h->d_xyz + h->nx + h->ny;
+    h->g.d_nk = make_fastdiv(unsigned(h->nk));
+    h->g.d_njnk = make_fastdiv(unsigned(h->nj) * unsigned(h->nk));
+    h->g.d_nink = make_fastdiv(unsigned(h->ni) * unsigned(h->nk));
+    h->g.d_ghost = make_fastdiv(unsigned(2 * h->bc));
+    h->g.d_ghost_nj = make_fastdiv(unsigned(2 * h->bc) * unsigned(h->nj));
+    h->g.d_nz = make_fastdiv(unsigned(h->nz));
+    h->g.d_nynz = make_fastdiv(unsigned(h->ny) * unsigned(h->nz));
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tuned.find(tune_key(h));
