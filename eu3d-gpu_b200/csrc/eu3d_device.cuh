@@ -169,16 +169,36 @@ struct MixPoly {
     double h3, h4, h5, h6;                 // a3/2, a4/3, a5/4, a6/5
 };
 
-template <int NS>
-__device__ __forceinline__ void mix_poly(const DevMech &m, const double (&Y)[NS], bool low, MixPoly<NS> &c)
+// The coefficients of one range, read from the kernel's constant parameter:
+// with the range fixed at compile time every coefficient is an operand of the
+// constant bank; with a per-thread choice each is a load whose address differs
+// between threads. The range is the same across a warp almost everywhere (it
+// changes only at the 1000 K isotherm), so the warp takes a fixed-range form
+// whenever all its active threads agree; the sums are the same either way.
+template <int NS, int kRange>
+__device__ __forceinline__ void mix_sums(const DevMech &m, const double (&Y)[NS], bool low, double (&a)[8])
 {
-    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
         const double w = Y[s] * m.ri[s];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) a[q] = fma(w, low ? m.clo[q][s] : m.chi[q][s], a[q]);
+        for (int q = 0; q < 8; ++q)
+            a[q] = fma(w, kRange == 1 ? m.clo[q][s] : (kRange == 2 ? m.chi[q][s] : (low ? m.clo[q][s] : m.chi[q][s])),
+                       a[q]);
     }
+}
+
+template <int NS>
+__device__ __forceinline__ void mix_poly(const DevMech &m, const double (&Y)[NS], bool low, MixPoly<NS> &c)
+{
+    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const unsigned active = __activemask();
+    if (__all_sync(active, low))
+        mix_sums<NS, 1>(m, Y, low, a);
+    else if (__all_sync(active, !low))
+        mix_sums<NS, 2>(m, Y, low, a);
+    else
+        mix_sums<NS, 0>(m, Y, low, a);
     c.a0 = a[0];
     c.a1 = a[1];
     c.a2 = a[2];
