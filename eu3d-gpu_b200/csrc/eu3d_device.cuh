@@ -9,6 +9,8 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
+
 #include <cuda_runtime.h>
 
 #include "eu3d_types.h"
@@ -82,29 +84,53 @@ __device__ __forceinline__ TPow make_tpow(double T, bool need_log)
     return p;
 }
 
-template <int NS>
+// Coefficient k of species s in the range of p. kRange 1 / 2: the low / high
+// range fixed at compile time, so the value is an operand of the kernel's
+// constant bank; 0: chosen per thread, a load whose address differs between
+// threads (those loads throttle the memory pipe). by_range() picks the form.
+template <int NS, int kRange = 0>
 __device__ __forceinline__ double coeff(const DevMech &m, const TPow &p, int k, int s)
 {
+    if (kRange == 1)
+        return m.clo[k][s];
+    if (kRange == 2)
+        return m.chi[k][s];
     return p.low ? m.clo[k][s] : m.chi[k][s];
 }
 
+// Runs f(std::integral_constant<int, R>) with R = 1 when every active thread of
+// the warp is on the low NASA range, 2 when all are on the high one, 0
+// otherwise. The range changes only at the 1000 K isotherm, so nearly every
+// warp takes a fixed-range form; the arithmetic is the same in all three.
+template <class F>
+__device__ __forceinline__ void by_range(bool low, F &&f)
+{
+    const unsigned active = __activemask();
+    if (__all_sync(active, low))
+        f(std::integral_constant<int, 1>{});
+    else if (__all_sync(active, !low))
+        f(std::integral_constant<int, 2>{});
+    else
+        f(std::integral_constant<int, 0>{});
+}
+
 // Reaction::GetCpi: R*(a1 T^-2 + a2 T^-1 + a3 + a4 T + a5 T^2 + a6 T^3 + a7 T^4)
-template <int NS>
+template <int NS, int kRange = 0>
 __device__ __forceinline__ double cp_species(const DevMech &m, const TPow &p, double R, int s)
 {
-    const double a0 = coeff<NS>(m, p, 0, s), a1 = coeff<NS>(m, p, 1, s), a2 = coeff<NS>(m, p, 2, s),
-                 a3 = coeff<NS>(m, p, 3, s), a4 = coeff<NS>(m, p, 4, s), a5 = coeff<NS>(m, p, 5, s),
-                 a6 = coeff<NS>(m, p, 6, s);
+    const double a0 = coeff<NS, kRange>(m, p, 0, s), a1 = coeff<NS, kRange>(m, p, 1, s), a2 = coeff<NS, kRange>(m, p, 2, s),
+                 a3 = coeff<NS, kRange>(m, p, 3, s), a4 = coeff<NS, kRange>(m, p, 4, s), a5 = coeff<NS, kRange>(m, p, 5, s),
+                 a6 = coeff<NS, kRange>(m, p, 6, s);
     return R * (a0 * p.inv2 + a1 * p.inv + a2 + a3 * p.T + a4 * p.t2 + a5 * p.t3 + a6 * p.t4);
 }
 
 // Reaction::GetHi: R*(-a1/T + a2 lnT + a3 T + a4 T^2/2 + a5 T^3/3 + a6 T^4/4 + a7 T^5/5 + b1)
-template <int NS>
+template <int NS, int kRange = 0>
 __device__ __forceinline__ double h_species(const DevMech &m, const TPow &p, double R, int s)
 {
-    const double a0 = coeff<NS>(m, p, 0, s), a1 = coeff<NS>(m, p, 1, s), a2 = coeff<NS>(m, p, 2, s),
-                 a3 = coeff<NS>(m, p, 3, s), a4 = coeff<NS>(m, p, 4, s), a5 = coeff<NS>(m, p, 5, s),
-                 a6 = coeff<NS>(m, p, 6, s), a7 = coeff<NS>(m, p, 7, s);
+    const double a0 = coeff<NS, kRange>(m, p, 0, s), a1 = coeff<NS, kRange>(m, p, 1, s), a2 = coeff<NS, kRange>(m, p, 2, s),
+                 a3 = coeff<NS, kRange>(m, p, 3, s), a4 = coeff<NS, kRange>(m, p, 4, s), a5 = coeff<NS, kRange>(m, p, 5, s),
+                 a6 = coeff<NS, kRange>(m, p, 6, s), a7 = coeff<NS, kRange>(m, p, 7, s);
 #ifdef EU_EXACT_CHEM
     return R * (-a0 * p.inv + a1 * p.lnT + a2 * p.T + a3 * p.t2 / 2 + a4 * p.t3 / 3 + a5 * p.t4 / 4 +
                 a6 * p.t5 / 5 + a7);
@@ -115,12 +141,12 @@ __device__ __forceinline__ double h_species(const DevMech &m, const TPow &p, dou
 }
 
 // Reaction::GetSi: R*(-a1 T^-2/2 - a2/T + a3 lnT + a4 T + a5 T^2/2 + a6 T^3/3 + a7 T^4/4 + b2)
-template <int NS>
+template <int NS, int kRange = 0>
 __device__ __forceinline__ double s_species(const DevMech &m, const TPow &p, double R, int s)
 {
-    const double a0 = coeff<NS>(m, p, 0, s), a1 = coeff<NS>(m, p, 1, s), a2 = coeff<NS>(m, p, 2, s),
-                 a3 = coeff<NS>(m, p, 3, s), a4 = coeff<NS>(m, p, 4, s), a5 = coeff<NS>(m, p, 5, s),
-                 a6 = coeff<NS>(m, p, 6, s), a8 = coeff<NS>(m, p, 8, s);
+    const double a0 = coeff<NS, kRange>(m, p, 0, s), a1 = coeff<NS, kRange>(m, p, 1, s), a2 = coeff<NS, kRange>(m, p, 2, s),
+                 a3 = coeff<NS, kRange>(m, p, 3, s), a4 = coeff<NS, kRange>(m, p, 4, s), a5 = coeff<NS, kRange>(m, p, 5, s),
+                 a6 = coeff<NS, kRange>(m, p, 6, s), a8 = coeff<NS, kRange>(m, p, 8, s);
 #ifdef EU_EXACT_CHEM
     return R * (-a0 * p.inv2 / 2 - a1 * p.inv + a2 * p.lnT + a3 * p.T + a4 * p.t2 / 2 + a5 * p.t3 / 3 +
                 a6 * p.t4 / 4 + a8);
@@ -128,6 +154,18 @@ __device__ __forceinline__ double s_species(const DevMech &m, const TPow &p, dou
     return R * (-a0 * p.inv2 * 0.5 - a1 * p.inv + a2 * p.lnT + a3 * p.T + a4 * p.t2 * 0.5 +
                 a5 * p.t3 * (1.0 / 3.0) + a6 * p.t4 * 0.25 + a8);
 #endif
+}
+
+// G_s = H_s - S_s T of every species (src/Reaction.cpp:597-600), the
+// reference's per-species expression.
+template <int NS>
+__device__ __forceinline__ void gibbs_all(const DevMech &m, const TPow &p, double T, double (&G)[NS])
+{
+    by_range(p.low, [&](auto range) {
+        constexpr int kR = decltype(range)::value;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) G[s] = h_species<NS, kR>(m, p, kRUniv, s) - s_species<NS, kR>(m, p, kRUniv, s) * T;
+    });
 }
 
 // --------------------------------------------------------- state recovery
@@ -148,10 +186,13 @@ __device__ __forceinline__ double newton_temperature(const DevMech &m, double T,
         const double T0 = T_temp;
         const TPow p = make_tpow(T0, true);
         double hsum = 0, cpsum = 0;
+        by_range(p.low, [&](auto range) {
+            constexpr int kR = decltype(range)::value;
 #pragma unroll
-        for (int s = 0; s < NS; ++s) hsum += Y[s] * h_species<NS>(m, p, m.ri[s], s);
+            for (int s = 0; s < NS; ++s) hsum += Y[s] * h_species<NS, kR>(m, p, m.ri[s], s);
 #pragma unroll
-        for (int s = 0; s < NS; ++s) cpsum += Y[s] * cp_species<NS>(m, p, m.ri[s], s);
+            for (int s = 0; s < NS; ++s) cpsum += Y[s] * cp_species<NS, kR>(m, p, m.ri[s], s);
+        });
         const double temp1 = (hsum - e_scaled) - rsum * T0;
         const double temp2 = cpsum - rsum;
         T_temp = T0 - temp1 / temp2;
@@ -301,8 +342,11 @@ __device__ __forceinline__ void finish_primitives(const DevMech &m, const CellSt
     H = P / c.D + c.E;
     const TPow p = make_tpow(c.T, false);
     double cp = 0;
+    by_range(p.low, [&](auto range) {
+        constexpr int kR = decltype(range)::value;
 #pragma unroll
-    for (int s = 0; s < NS; ++s) cp += cp_species<NS>(m, p, m.ri[s], s) * c.Y[s];
+        for (int s = 0; s < NS; ++s) cp += cp_species<NS, kR>(m, p, m.ri[s], s) * c.Y[s];
+    });
     const double Cp = cp * 1000;
     G = Cp / (Cp - kRUniv * inv_w * 1000);
 #else
@@ -363,12 +407,7 @@ __device__ __forceinline__ void eval_rates(const DevMech &m, double T, const dou
     double Gi[NS];
     {
         const TPow p = make_tpow(T, true);
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            const double hi = h_species<NS>(m, p, kRUniv, s);
-            const double si = s_species<NS>(m, p, kRUniv, s);
-            Gi[s] = hi - si * T;
-        }
+        gibbs_all<NS>(m, p, T, Gi);
     }
     const bool nu_int = m.nu_int != 0;
     const double RT = kRUniv * T;
@@ -422,12 +461,13 @@ __device__ __forceinline__ void eval_rates(const DevMech &m, double T, const dou
 template <int NS, int NR>
 __device__ __forceinline__ void eval_rates(const DevMech &m, double T, const double (&mc)[NS], SpeciesRates<NS> &k)
 {
-    double eg[NS], ieg[NS];
+    double eg[NS], ieg[NS], Gs[NS];
     const TPow p = make_tpow(T, true);
     const double invRT = 1.0 / (kRUniv * T);
+    gibbs_all<NS>(m, p, T, Gs);
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-        const double g = (h_species<NS>(m, p, kRUniv, s) - s_species<NS>(m, p, kRUniv, s) * T) * invRT;
+        const double g = Gs[s] * invRT;
         eg[s] = exp(g);
         ieg[s] = rcp_nr(eg[s]);
     }

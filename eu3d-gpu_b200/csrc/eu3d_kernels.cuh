@@ -85,11 +85,14 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
         const TPow p = make_tpow(T, true);
         double rg = 0, cp = 0, h = 0, e = 0;
         double Cpi[NS], Hi[NS];
+        by_range(p.low, [&](auto range) {
+            constexpr int kR = decltype(range)::value;
 #pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            Cpi[s] = cp_species<NS>(m, p, m.ri[s], s);
-            Hi[s] = h_species<NS>(m, p, m.ri[s], s);
-        }
+            for (int s = 0; s < NS; ++s) {
+                Cpi[s] = cp_species<NS, kR>(m, p, m.ri[s], s);
+                Hi[s] = h_species<NS, kR>(m, p, m.ri[s], s);
+            }
+        });
 #pragma unroll
         for (int s = 0; s < NS; ++s) rg += v[kY0 + s] * m.ri[s];
         const double Rgas = rg * 1000;

@@ -51,9 +51,7 @@ void emit_strict(std::ostream &o, const MechanismTables &m)
     o << "    double Gi[" << ns << "];\n"
       << "    {\n"
       << "        const TPow p = make_tpow(T, true);\n"
-      << "#pragma unroll\n"
-      << "        for (int s = 0; s < " << ns << "; ++s)\n"
-      << "            Gi[s] = h_species<" << ns << ">(m, p, kRUniv, s) - s_species<" << ns << ">(m, p, kRUniv, s) * T;\n"
+      << "        gibbs_all<" << ns << ">(m, p, T, Gi);\n"
       << "    }\n"
       << "    const double RT = kRUniv * T;\n"
       << "    const double RuT = kRuCal * T;\n"
@@ -121,13 +119,13 @@ void emit_strict(std::ostream &o, const MechanismTables &m)
 void emit_fast(std::ostream &o, const MechanismTables &m)
 {
     const int ns = m.ns, nr = m.nr;
-    o << "    double eg[" << ns << "], ieg[" << ns << "];\n"
+    o << "    double eg[" << ns << "], ieg[" << ns << "], Gs[" << ns << "];\n"
       << "    const TPow p = make_tpow(T, true);\n"
       << "    const double invRT = 1.0 / (kRUniv * T);\n"
+      << "    gibbs_all<" << ns << ">(m, p, T, Gs);\n"
       << "#pragma unroll\n"
       << "    for (int s = 0; s < " << ns << "; ++s) {\n"
-      << "        const double g = (h_species<" << ns << ">(m, p, kRUniv, s) - s_species<" << ns
-      << ">(m, p, kRUniv, s) * T) * invRT;\n"
+      << "        const double g = Gs[s] * invRT;\n"
       << "        eg[s] = exp(g);\n"
       << "        ieg[s] = exp(-g);\n"
       << "    }\n"
