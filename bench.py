@@ -310,10 +310,43 @@ def reacting_block(args, model, gate, local, dt=2e-8):
         ys[name] = s.get("Yi")
         s.close()
     l1 = np.abs(ys["learned_mixed"] - ys["stiff_fp64"])[:, 2:-2, 2:-2, 2:-2].sum(axis=0)
+    shift = cases.front_shift(ys["learned_mixed"], ys["stiff_fp64"])
     return {"grid": list(grid), "cells": ncell, **out,
             "speedup": round(out["learned_mixed"]["value"] / out["stiff_fp64"]["value"], 3),
             "species_l1_mean": float(l1.mean()), "species_l1_max": float(l1.max()),
-            "dt": dt, "after_steps": args.warmup + args.steps}
+            "front_shift_cells_max": shift, "dt": dt, "after_steps": args.warmup + args.steps}
+
+
+def znd_case(args, local, steps=1000, cells=4000, dx=25e-6):
+    """The 1-D ZND initiation: 4000 cells of 25 um (4001 x 2 x 2 nodes over
+    0.1 m), 2H2+O2+7Ar at 6.67 kPa / 298 K, a 1 MPa / 3000 K driver on the 40
+    nodes at the reflecting wall (data/input-1dZND.txt; its edge a 2-cell tanh
+    profile, see eu3d_cases.znd), outflow at the far end,
+    plain FP64 stiff chemistry, each step's dt from the CFL rule at 0.5 on the
+    device, 1000 steps. Reports the device throughput, the time advanced and
+    where the leading shock (the largest x with p > 2 x the quiescent
+    pressure) is at the end."""
+    ni = cells + 1
+    ext = (0.0, cells * dx, 0.0, dx, 0.0, dx)
+    x = cases.node_coordinates(ni, ext[0], ext[1])
+    y = cases.node_coordinates(2, ext[2], ext[3])
+    mech = eu3d.parse_mechanism(cases.MECH_JA919_AR, cases.THERMO_AR)
+    prim = cases.znd(x, y, y, mech["mw"], mech["ns"])
+    p, cs, T, E = eu3d.initial_state(mech, ni, 2, 2, *prim)
+    s = eu3d.Solver(ni, 2, 2, ext, precision="fp64", chemistry="stiff", arith="fast", device=local, boundary="znd")
+    s.set_mechanism(mech)
+    s.set_state(state_dict((p, cs, T, E)))
+    st, t_adv = s.step_cfl(steps, CFL)
+    pr = s.get("P")[0, 2:-2, 2, 2]
+    t_end = s.get("T")[0, 2:-2, 2, 2]
+    s.close()
+    p0 = eu3d.read_value(cases.INPUT_ZND, "P")
+    front = int(np.nonzero(pr > 2 * p0)[0].max()) if (pr > 2 * p0).any() else 0
+    return {"grid": [ni, 2, 2], "steps": steps, "time_advanced_s": t_adv,
+            "value": round(ni * 4 * steps / (st["device_ms"] / 1e3) / 1e6, 3), "unit": "Mcell-steps/s",
+            "ms_per_step": round(st["device_ms"] / steps, 4), "max_nchem_last_step": st["max_nchem"],
+            "shock_node": front, "shock_x_m": round(front * dx, 6), "peak_T_K": round(float(t_end.max()), 1),
+            "peak_p_Pa": round(float(pr.max()), 1)}
 
 
 BATCH_SIZES = ((64, 64, 64), (128, 64, 64), (192, 96, 96))
@@ -480,6 +513,12 @@ def our_arm(args):
     batch = None
     if args.chem == "learned" and not args.no_batch:
         batch = batch_instances(args, model, gate, local, mech)
+    znd = None
+    if not args.no_batch:
+        try:
+            znd = znd_case(args, local)
+        except eu3d.EU3DError as e:  # reported, not fatal to the headline measurement
+            znd = {"error": str(e)}
 
     # -- per-kernel times (same stream, CUDA events around each kernel phase) -----------------
     sp = make_solver(args.chem, args.precision, args.arith, profile=True)
@@ -506,6 +545,7 @@ def our_arm(args):
         t = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)
         t.numpy()[...] = v
         pinned[k] = t.numpy()
+    cs_host = torch.empty(sd["CS"].shape, dtype=torch.float64, pin_memory=True).numpy()
     se = make_solver(args.chem, args.precision, args.arith, state=pinned)
     se.step(args.warmup, dt)
     barrier(dist, device)
@@ -514,7 +554,7 @@ def our_arm(args):
     se.set_state(pinned)
     for _ in range(args.steps):
         se.step(1, dt)  # synchronous: reads the step's health counters back
-    cs = se.get("CS")
+    cs = se.get("CS", out=cs_host)
     torch.cuda.synchronize()
     e2e_s = reduce_max(dist, time.perf_counter() - t0, device)
     e2e_value = ncell * args.steps * world / e2e_s / 1e6
@@ -540,6 +580,7 @@ def our_arm(args):
                 "plain_fp64": plain,
                 "reacting_block": block,
                 "batch_instances": batch,
+                "znd_1d": znd,
                 "roofline": roofline, "kernels_ms_per_step": per_kernel,
                 "max_nchem": stats["max_nchem"], "reacting_cells": stats["reacting"],
                 "learned_cells": stats["learned"], "fallback_cells": stats["fallback"],

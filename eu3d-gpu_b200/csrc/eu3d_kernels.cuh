@@ -25,6 +25,10 @@ namespace EU3D_NS {
 //   y low: symmetry, V reflected, rho/H/Gamma rebuilt from mirrored T, p, Y (:647-679)
 //   y high: zero-gradient mirror copy          (:684-705)
 //   z low/high: mirror copy with W reflected   (:710-802)
+// With g.bc_kind == 1 the x faces follow Flowfield::FieldBoundary_1dZND
+// (src/Flowfield.cpp:317-411, commented out in the reference): x low a
+// reflecting wall (mirror copy, U reflected), x high outflow (mirror copy of
+// U, V, p, T, Y with rho/H/Gamma rebuilt as on the y-low face).
 template <int NS>
 __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMech m, const DevGrid g,
                                                   const DevState st)
@@ -36,7 +40,7 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
         return;
     const long long n3 = g.n3;
     long long dst, src;
-    double sv = 1, sw = 1;
+    double su = 1, sv = 1, sw = 1;
     bool rebuild = false;
     if (t < nxf) {
         const int jk = fdiv(t, g.d_nk), q = fdiv(t, g.d_njnk); // q: 0 .. 2bc-1
@@ -46,6 +50,10 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
         const int si = q < bc ? 2 * bc - 1 - i : 2 * (ni + bc) - 1 - i;
         dst = cell_index(g, i, j, k);
         src = cell_index(g, si, j, k);
+        if (g.bc_kind == 1) {
+            su = q < bc ? -1 : 1;
+            rebuild = q >= bc;
+        }
     } else if (t < nxf + nyf) {
         t -= nxf;
         const int ik = fdiv(t, g.d_nk), q = fdiv(t, g.d_nink);
@@ -78,6 +86,7 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
     double v[7 + NS];
 #pragma unroll
     for (int f = 0; f < 7 + NS; ++f) v[f] = st.prim32 ? double(st.prim32[f * n3 + src]) : st.prim[f * n3 + src];
+    v[kU] = su * v[kU];
     v[kV] = sv * v[kV];
     v[kW] = sw * v[kW];
     const double T = st.T[src];
@@ -1135,6 +1144,71 @@ __global__ void k_derived(const __grid_constant__ DevMech m, const DevGrid g, co
 // Writes a scalar (the timestep) into device memory from a kernel argument, so
 // the value is captured at launch and the caller's copy may go away.
 __global__ void k_set_value(double *dst, double v) { *dst = v; }
+
+// Flowfield::CFLcondition (src/Flowfield.cpp:275-304): the smallest
+// min(dx / (|u| + c), dy / (|v| + c)) over the interior nodes, c = sqrt(gamma p
+// / rho), from the primitive planes the next flux step reads (FP32 in mixed
+// precision). The spacings are the interior ones (the reference takes them
+// from its first two ghost nodes, the same on a uniform grid with three or
+// more nodes per axis). Positive doubles order as their bit patterns, so the
+// block minima combine with an integer atomicMin into *slot (non-finite values
+// map to the largest key and never win).
+__global__ void __launch_bounds__(256) k_cfl_min(const DevGrid g, const DevState st, unsigned long long *slot)
+{
+    const long long ncell = (long long)g.ni * g.nj * g.nk;
+    const double dx = g.x[g.bc + 1] - g.x[g.bc], dy = g.y[g.bc + 1] - g.y[g.bc];
+    const long long n3 = g.n3;
+    double m = __longlong_as_double(0x7ff0000000000000LL);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < ncell;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        interior_node(g, t, i, j, k);
+        const long long c = cell_index(g, i, j, k);
+        double P, D, U, V, G;
+        if (st.prim32) {
+            P = st.prim32[kP * n3 + c];
+            D = st.prim32[kD * n3 + c];
+            U = st.prim32[kU * n3 + c];
+            V = st.prim32[kV * n3 + c];
+            G = st.prim32[kG * n3 + c];
+        } else {
+            P = st.prim[kP * n3 + c];
+            D = st.prim[kD * n3 + c];
+            U = st.prim[kU * n3 + c];
+            V = st.prim[kV * n3 + c];
+            G = st.prim[kG * n3 + c];
+        }
+        const double C = sqrt(G * P / D);
+        const double q = fmin(dx / (fabs(U) + C), dy / (fabs(V) + C));
+        m = (q < m || !(q == q)) ? q : m; // a NaN sticks
+    }
+    unsigned long long b = (unsigned long long)__double_as_longlong(m);
+    if (!(m >= 0.0)) // NaN (or a negative spacing): the largest key
+        b = ~0ULL;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long v = __shfl_xor_sync(0xffffffffu, b, o);
+        b = v < b ? v : b;
+    }
+    __shared__ unsigned long long wmin[8];
+    if ((threadIdx.x & 31) == 0)
+        wmin[threadIdx.x >> 5] = b;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) b = wmin[w] < b ? wmin[w] : b;
+        atomicMin(slot, b);
+    }
+}
+
+// dt = cfl * the minimum; the step's kernels read *dt_dev; *time accumulates
+// the steps' dt; the slot is reset for the next step.
+__global__ void k_cfl_finish(unsigned long long *slot, double cfl, double *dt_dev, double *time)
+{
+    const double dt = cfl * __longlong_as_double((long long)*slot);
+    *dt_dev = dt;
+    *time += dt;
+    *slot = 0x7ff0000000000000ULL;
+}
 
 } // namespace EU3D_NS
 } // namespace eu3d

@@ -237,6 +237,15 @@ cudaError_t launch_chem_samples(const LaunchArgs &a, long long n, double *cs, do
 
 cudaError_t launch_react_heavy(const LaunchArgs &a, int blocks) { EU3D_DISPATCH(heavy_t, a, blocks) }
 
+cudaError_t launch_cfl(const LaunchArgs &a, double cfl, unsigned long long *slot, double *time)
+{
+    const long long n = (long long)a.g.ni * a.g.nj * a.g.nk;
+    const unsigned blocks = unsigned(std::min<long long>((n + 255) / 256, (long long)(a.sms > 0 ? a.sms : 148) * 8));
+    k_cfl_min<<<blocks, 256, 0, a.stream>>>(a.g, a.st, slot);
+    k_cfl_finish<<<1, 1, 0, a.stream>>>(slot, cfl, const_cast<double *>(a.dt_dev), time);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_set_value(double *dst, double v, cudaStream_t s)
 {
     k_set_value<<<1, 1, 0, s>>>(dst, v);

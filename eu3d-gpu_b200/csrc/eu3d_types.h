@@ -53,6 +53,7 @@ struct DevGrid {
     const double *x, *y, *z; // node coordinates with ghosts
     // index decompositions of the kernels' flat thread indices
     FastDiv d_nk, d_njnk, d_nink, d_ghost, d_ghost_nj, d_nz, d_nynz;
+    int bc_kind; // eu_boundary
 };
 
 // Primitive planes the stencils read, in this order (haloed, FP64).

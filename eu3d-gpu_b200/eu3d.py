@@ -24,6 +24,7 @@ STATUS = {0: "EU_OK", 1: "EU_ERR_INVALID_ARGUMENT", 2: "EU_ERR_CUDA", 3: "EU_ERR
 PRECISION = {"fp64": 0, "mixed": 1}
 CHEMISTRY = {"stiff": 0, "frozen": 1, "learned": 2}
 ARITH = {"strict": 0, "fast": 1}
+BOUNDARY = {"rsbi": 0, "znd": 1}
 
 
 class EU3DError(RuntimeError):
@@ -37,7 +38,7 @@ class Config(ctypes.Structure):
     _fields_ = [("total_ni", _I), ("total_nj", _I), ("total_nk", _I),
                 ("xa", _D), ("xb", _D), ("ya", _D), ("yb", _D), ("za", _D), ("zb", _D),
                 ("bc", _I), ("device", _I), ("precision", _I), ("chemistry", _I), ("arith", _I),
-                ("max_substeps", _I), ("record_sources", _I), ("profile", _I), ("eager", _I)]
+                ("max_substeps", _I), ("record_sources", _I), ("profile", _I), ("eager", _I), ("boundary", _I)]
 
 
 class MechanismC(ctypes.Structure):
@@ -85,6 +86,8 @@ def library():
         lib = ctypes.CDLL(LIB_PATH)
         lib.eu_abi_version.restype = _I
         lib.eu_read_grid.argtypes = [ctypes.c_char_p, ctypes.POINTER(Config)]
+        lib.eu_read_value.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_D)]
+        lib.eu_read_value.restype = _I
         lib.eu_parse_mechanism.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_I), ctypes.POINTER(_I)] + [_P] * 9
         lib.eu_initial_state.argtypes = [ctypes.POINTER(MechanismC), _I, _I, _I, _I] + [_P] * 10
         lib.eu_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(_P)]
@@ -98,6 +101,8 @@ def library():
         lib.eu_set_primitive.argtypes = [_P] * 7
         lib.eu_set_state.argtypes = [_P] * 12
         lib.eu_step.argtypes = [_P, _I, _D, ctypes.POINTER(StepStats)]
+        lib.eu_step_cfl.argtypes = [_P, _I, _D, ctypes.POINTER(StepStats), ctypes.POINTER(_D)]
+        lib.eu_step_cfl.restype = _I
         lib.eu_get_field.argtypes = [_P, ctypes.c_char_p, _P]
         lib.eu_sync.argtypes = [_P]
         lib.eu_device_info.argtypes = [_P, ctypes.POINTER(_P), ctypes.POINTER(ctypes.c_size_t)]
@@ -174,6 +179,17 @@ def parse_mechanism(mech_path, thermo_path):
     return out
 
 
+def read_value(path, key, default=None):
+    """A numeric value of a reference-format key/value file (input-*.txt)."""
+    v = _D()
+    st = library().eu_read_value(str(path).encode(), key.encode(), ctypes.byref(v))
+    if st == 1 and default is not None:
+        return default
+    if st:
+        raise EU3DError(st, f"{key} in {path}")
+    return v.value
+
+
 def mechanism_struct(m):
     """eu_mechanism from an object/dict with the table attributes; returns (struct, keepalive)."""
     get = (lambda k: m[k]) if isinstance(m, dict) else (lambda k: getattr(m, k))
@@ -204,11 +220,11 @@ class Solver:
     """One eu_handle: a haloed node grid, a mechanism and the device state."""
 
     def __init__(self, total_ni, total_nj, total_nk, extent, precision="fp64", chemistry="stiff", arith="strict",
-                 device=0, max_substeps=0, record_sources=False, profile=False, bc=2, graphs=True):
+                 device=0, max_substeps=0, record_sources=False, profile=False, bc=2, graphs=True, boundary="rsbi"):
         lib = library()
         self.cfg = Config(int(total_ni), int(total_nj), int(total_nk), *[float(v) for v in extent], int(bc),
                           int(device), PRECISION[precision], CHEMISTRY[chemistry], ARITH[arith], int(max_substeps),
-                          int(bool(record_sources)), int(bool(profile)), int(not graphs))
+                          int(bool(record_sources)), int(bool(profile)), int(not graphs), BOUNDARY[boundary])
         h = _P()
         st = lib.eu_create(ctypes.byref(self.cfg), ctypes.byref(h))
         if st:
@@ -292,9 +308,23 @@ class Solver:
         self._check(st, "step")
         return s.as_dict() if stats else None
 
-    def get(self, name):
+    def step_cfl(self, nsteps, cfl):
+        """eu_step_cfl: each step's dt from the CFL rule on the device.
+        Returns (stats, time advanced)."""
+        s = StepStats()
+        t = _D()
+        self._check(library().eu_step_cfl(self.h, int(nsteps), float(cfl), ctypes.byref(s), ctypes.byref(t)),
+                    "step_cfl")
+        return s.as_dict(), t.value
+
+    def get(self, name, out=None):
+        """A field as (planes, nx, ny, nz) float64. out: a caller's C-contiguous
+        float64 array of that size (pinned host memory makes the copy faster)."""
         planes = {"Yi": self.ns, "Di": self.ns, "Mc": self.ns, "CMS": self.ns, "CS": self.ns + 4}.get(name, 1)
-        out = np.empty(planes * self.n3)
+        if out is None:
+            out = np.empty(planes * self.n3)
+        if out.dtype != np.float64 or not out.flags.c_contiguous or out.size != planes * self.n3:
+            raise ValueError(f"out must be C-contiguous float64 with {planes * self.n3} elements")
         self._check(library().eu_get_field(self.h, name.encode(), out.ctypes.data), f"get {name}")
         return out.reshape(planes, *self.shape)
 

@@ -4,6 +4,11 @@
   air): Flowfield::FieldInitial (src/Flowfield.cpp:193-225) for p, T, u and
   Reaction::ReactionInitial (src/Reaction.cpp:412-471) for the composition,
   over every node including ghosts, as the reference fills them.
+* ``znd`` — the 1-D ZND detonation initiation: a hot high-pressure driver at
+  a reflecting wall next to quiescent 2H2+O2+7Ar, parameters from an
+  input-1dZND.txt in the reference's key/value format (P_bound, T_bound, P, T,
+  and driver_nodes, this build's addition). The reference's ZND case is dead
+  code (its boundary is commented out and its initialiser hard-codes RSBI).
 * ``shock_bubble`` — the 3-D reacting shock-bubble workload: a planar shock
   in N2 hitting a sphere of stoichiometric 2H2+O2 with a tanh interface and a
   seeded spherical-harmonic surface perturbation (l = 1..8, RMS amplitude 2 % of
@@ -25,9 +30,14 @@ DATA = os.path.join(HERE, "data")
 MECH_JA919 = os.path.join(DATA, "H2_JA919.txt")
 MECH_JA1119 = os.path.join(DATA, "H2_JA1119.txt")
 THERMO = os.path.join(DATA, "thermo.dat")
+# the same mechanism with Ar as the ninth (inert) species and the thermo file
+# whose ninth block is AR (thermo.dat is read by position)
+MECH_JA919_AR = os.path.join(DATA, "H2_JA919_Ar.txt")
+THERMO_AR = os.path.join(DATA, "thermo_Ar.dat")
+INPUT_ZND = os.path.join(DATA, "input-1dZND.txt")
 
 # species slots of H2_JA919 (H O H2O OH O2 H2 H2O2 HO2 N2)
-S_O2, S_H2, S_N2 = 4, 5, 8
+S_H2O, S_O2, S_H2, S_N2 = 2, 4, 5, 8
 
 
 def node_coordinates(n, a, b, bc=2):
@@ -207,5 +217,61 @@ def hot_reacting_block(nx, ny, nz, mw, ns, t_range=(1300.0, 2600.0), p_range=(1e
     Y[S_H2] = (1 - n2) * y_h2
     Y[S_O2] = (1 - n2) * (1 - y_h2)
     Y[S_N2] = n2
+    Z = np.zeros((nx, ny, nz))
+    return P, T, Z, Z.copy(), Z.copy(), Y
+
+
+def front_shift(y, y_ref, product=S_H2O, min_product=1e-2, bc=2):
+    """Reaction-front position error in cells between two runs' species fields
+    (ns, nx, ny, nz): per (j, k) column the front is the first node along x
+    whose product mass fraction reaches half the reference run's column
+    maximum; returns the largest |difference| over the columns whose reference
+    maximum reaches min_product (before that there is no front, only trace
+    product whose half-maximum point is noise; a front missing in one run
+    counts as the column length)."""
+    a = y[product, bc:-bc, bc:-bc, bc:-bc]
+    b = y_ref[product, bc:-bc, bc:-bc, bc:-bc]
+    thr = 0.5 * b.max(axis=0)
+    ok = 2 * thr >= min_product
+    fa, fb = a >= thr, b >= thr
+    ia = np.where(fa.any(axis=0), fa.argmax(axis=0), a.shape[0])
+    ib = np.where(fb.any(axis=0), fb.argmax(axis=0), b.shape[0])
+    return int(np.abs(ia - ib)[ok].max()) if ok.any() else 0
+
+
+def znd(x, y, z, mw, ns, input_path=INPUT_ZND, mole=None, bc=2, interface_cells=2.0):
+    """ZND initiation: driver (P_bound, T_bound) on the first driver_nodes
+    interior nodes along x and the ghosts left of them, quiescent gas (P, T)
+    elsewhere, at rest, one composition everywhere (default stoichiometric
+    2H2 + O2 + 7 Ar on the Ar variant of the mechanism, Ar in slot 8).
+
+    The driver edge is a tanh profile interface_cells wide (f = (1 - tanh((i -
+    i_edge) / w)) / 2, ln p and T blended by f); 0 gives the sharp jump. The
+    sharp 150:1 jump does not run with the reference's scheme: in the first
+    step both sides are at rest, so the AUSM+ flux at the edge carries no mass
+    and no energy, only the pressure force, which accelerates the first
+    quiescent node while its total energy stays put; its internal energy, and
+    with it T, falls below the NASA range (60 K after 2 ns, non-finite after
+    12 ns)."""
+    import eu3d
+    p_drv = eu3d.read_value(input_path, "P_bound")
+    t_drv = eu3d.read_value(input_path, "T_bound")
+    p0 = eu3d.read_value(input_path, "P")
+    t0 = eu3d.read_value(input_path, "T")
+    n_drv = int(eu3d.read_value(input_path, "driver_nodes", 40))
+    nx, ny, nz = len(x), len(y), len(z)
+    if mole is None:
+        mole = {S_H2: 2.0, S_O2: 1.0, S_N2: 7.0}
+    tot = sum(v * mw[s] for s, v in mole.items())
+    Y = np.zeros((ns, nx, ny, nz))
+    for s, v in mole.items():
+        Y[s] = v * mw[s] / tot
+    i = np.arange(nx, dtype=np.float64)[:, None, None] * np.ones((1, ny, nz))
+    if interface_cells > 0:
+        f = 0.5 * (1 - np.tanh((i - (bc + n_drv - 0.5)) / interface_cells))
+    else:
+        f = (i < bc + n_drv).astype(np.float64)
+    P = np.exp(np.log(p0) + f * (np.log(p_drv) - np.log(p0)))
+    T = t0 + f * (t_drv - t0)
     Z = np.zeros((nx, ny, nz))
     return P, T, Z, Z.copy(), Z.copy(), Y

@@ -38,6 +38,8 @@ struct eu_handle {
     DevState st{};
     double *d_xyz = nullptr;
     double *d_dt = nullptr;
+    unsigned long long *d_cfl_slot = nullptr; // CFL minimum of the step being set up
+    double *d_time = nullptr;                 // time advanced by the CFL-driven steps of a call
     double *d_scratch = nullptr;
     std::vector<void *> allocs;
     size_t bytes = 0;
@@ -60,6 +62,7 @@ struct eu_handle {
     cudaGraphExec_t graph_exec = nullptr;
     int graph_launches = 0;
     bool graph_dirty = true;
+    double graph_cfl = 0;   // the CFL number the captured step sets its dt from (0: a fixed dt)
     unsigned graph_gen = 0; // captures so far (batches rebuild when it changes)
     // launch shapes picked by eu_autotune (0: defaults)
     int flux_ci = 0, recover_block = 0;
@@ -271,6 +274,19 @@ extern "C" {
 
 int eu_abi_version(void) { return EU3D_ABI_VERSION; }
 
+eu_status eu_read_value(const char *path, const char *key, double *value)
+{
+    if (!path || !key || !value)
+        return EU_ERR_INVALID_ARGUMENT;
+    KeyValueFile f;
+    if (!f.read(path))
+        return EU_ERR_IO;
+    if (!f.has(key))
+        return EU_ERR_INVALID_ARGUMENT;
+    *value = f.get_double(key);
+    return EU_OK;
+}
+
 eu_status eu_read_grid(const char *grid_path, eu_config *cfg)
 {
     if (!grid_path || !cfg)
@@ -376,6 +392,8 @@ eu_status eu_create(const eu_config *cfg, eu_handle **out)
         return EU_ERR_INVALID_ARGUMENT;
     if (cfg->chemistry != EU_CHEM_STIFF && cfg->chemistry != EU_CHEM_FROZEN && cfg->chemistry != EU_CHEM_LEARNED)
         return EU_ERR_INVALID_ARGUMENT;
+    if (cfg->boundary != EU_BC_RSBI && cfg->boundary != EU_BC_ZND)
+        return EU_ERR_INVALID_ARGUMENT;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return EU_ERR_CUDA;
@@ -417,9 +435,17 @@ eu_status eu_create(const eu_config *cfg, eu_handle **out)
     h->sms = sms;
     eu_status s;
     if ((s = dalloc(h, &h->d_xyz, size_t(h->nx + h->ny + h->nz))) != EU_OK ||
-        (s = dalloc(h, &h->d_dt, size_t(1))) != EU_OK) {
+        (s = dalloc(h, &h->d_dt, size_t(1))) != EU_OK || (s = dalloc(h, &h->d_time, size_t(1))) != EU_OK ||
+        (s = dalloc(h, &h->d_cfl_slot, size_t(1))) != EU_OK) {
         eu_destroy(h);
         return s;
+    }
+    {
+        const unsigned long long inf_bits = 0x7ff0000000000000ULL; // +inf: no minimum yet
+        if (cudaMemcpy(h->d_cfl_slot, &inf_bits, sizeof inf_bits, cudaMemcpyHostToDevice) != cudaSuccess) {
+            eu_destroy(h);
+            return EU_ERR_CUDA;
+        }
     }
     std::vector<double> xyz;
     xyz.insert(xyz.end(), h->x.begin(), h->x.end());
@@ -447,6 +473,7 @@ eu_status eu_create(const eu_config *cfg, eu_handle **out)
     h->g.d_ghost_nj = make_fastdiv(unsigned(2 * h->bc) * unsigned(h->nj));
     h->g.d_nz = make_fastdiv(unsigned(h->nz));
     h->g.d_nynz = make_fastdiv(unsigned(h->ny) * unsigned(h->nz));
+    h->g.bc_kind = cfg->boundary;
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tuned.find(tune_key(h));
@@ -716,10 +743,15 @@ eu_status learned_chemistry(eu_handle *h, const LaunchArgs &a, const Launchers &
 
 // The launches of one timestep on h->stream (run eagerly or recorded into the
 // step's graph). phase (profile mode) receives per-phase event times.
-eu_status step_launches(eu_handle *h, const LaunchArgs &a, const Launchers &L, bool prof, int *launches)
+eu_status step_launches(eu_handle *h, const LaunchArgs &a, const Launchers &L, bool prof, int *launches,
+                        double cfl = 0)
 {
     const bool react = h->cfg.chemistry == EU_CHEM_STIFF;
     const bool learned = h->cfg.chemistry == EU_CHEM_LEARNED;
+    if (cfl > 0) { // this step's dt from the current state (Flowfield::CFLcondition)
+        CK(h, strict::launch_cfl(a, cfl, h->d_cfl_slot, h->d_time));
+        *launches += 2;
+    }
     CK(h, cudaMemsetAsync(h->st.counters, 0, kCntPerStep * sizeof(unsigned long long), h->stream));
     if (prof) CK(h, cudaEventRecord(h->pev[0], h->stream));
     CK(h, L.boundary(a));
@@ -748,12 +780,12 @@ eu_status step_launches(eu_handle *h, const LaunchArgs &a, const Launchers &L, b
 }
 
 // Records one timestep into h->graph and instantiates it.
-eu_status capture_step(eu_handle *h, const LaunchArgs &a, const Launchers &L)
+eu_status capture_step(eu_handle *h, const LaunchArgs &a, const Launchers &L, double cfl = 0)
 {
     drop_graph(h);
     int launches = 0;
     CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    eu_status s = step_launches(h, a, L, false, &launches);
+    eu_status s = step_launches(h, a, L, false, &launches, cfl);
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     if (s != EU_OK) {
@@ -767,6 +799,7 @@ eu_status capture_step(eu_handle *h, const LaunchArgs &a, const Launchers &L)
     CK(h, cudaGraphInstantiate(&h->graph_exec, g, 0));
     h->graph_launches = launches;
     h->graph_dirty = false;
+    h->graph_cfl = cfl;
     ++h->graph_gen;
     return EU_OK;
 }
@@ -873,12 +906,33 @@ eu_status eu_set_learned(eu_handle *h, eu_mlp *model, const eu_learned_config *l
     return EU_OK;
 }
 
+namespace {
+// nsteps timesteps: with cfl == 0 of the fixed dt, else each of dt = cfl x the
+// CFL minimum of its own starting state (the time advanced goes to *time).
+eu_status step_impl(eu_handle *h, int nsteps, double dt, double cfl, eu_step_stats *stats, double *time);
+} // namespace
+
 eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
 {
     if (!h)
         return EU_ERR_INVALID_ARGUMENT;
     if (nsteps < 0 || !(dt > 0))
         return fail(h, EU_ERR_INVALID_ARGUMENT, "nsteps must be >= 0 and dt > 0");
+    return step_impl(h, nsteps, dt, 0.0, stats, nullptr);
+}
+
+eu_status eu_step_cfl(eu_handle *h, int nsteps, double cfl, eu_step_stats *stats, double *time_advanced)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (nsteps < 0 || !(cfl > 0) || !(cfl <= 10))
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "nsteps must be >= 0 and 0 < cfl <= 10");
+    return step_impl(h, nsteps, 0.0, cfl, stats, time_advanced);
+}
+
+namespace {
+eu_status step_impl(eu_handle *h, int nsteps, double dt, double cfl, eu_step_stats *stats, double *time)
+{
     if (!h->has_mech || !h->has_state)
         return fail(h, EU_ERR_NOT_READY, "mechanism and state must be set before stepping");
     cudaSetDevice(h->cfg.device);
@@ -898,19 +952,23 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
     if (stats)
         CK(h, cudaEventRecord(h->ev0, h->stream));
     CK(h, cudaMemsetAsync(h->st.counters, 0, kCntCount * sizeof(unsigned long long), h->stream));
-    CK(h, strict::launch_set_value(h->d_dt, dt, h->stream));
-    ++launches;
+    if (cfl > 0) {
+        CK(h, cudaMemsetAsync(h->d_time, 0, sizeof(double), h->stream));
+    } else {
+        CK(h, strict::launch_set_value(h->d_dt, dt, h->stream));
+        ++launches;
+    }
     if (h->st.prim32 && nsteps > 0)
         h->prim_stale = true;
     int n = 0;
-    if (graphs && nsteps > 0 && (h->graph_dirty || !h->graph_exec)) {
+    if (graphs && nsteps > 0 && (h->graph_dirty || !h->graph_exec || h->graph_cfl != cfl)) {
         // the first step runs eagerly (one-time kernel attribute set-up), then
         // the step is captured
-        eu_status s = step_launches(h, a, L, false, &launches);
+        eu_status s = step_launches(h, a, L, false, &launches, cfl);
         if (s != EU_OK)
             return s;
         n = 1;
-        if ((s = capture_step(h, a, L)) != EU_OK)
+        if ((s = capture_step(h, a, L, cfl)) != EU_OK)
             return s;
     }
     for (; n < nsteps; ++n) {
@@ -919,7 +977,7 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
             launches += h->graph_launches;
             continue;
         }
-        eu_status s = step_launches(h, a, L, prof, &launches);
+        eu_status s = step_launches(h, a, L, prof, &launches, cfl);
         if (s != EU_OK)
             return s;
         if (prof) {
@@ -929,6 +987,14 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
                 CK(h, cudaEventElapsedTime(&ms, h->pev[q], h->pev[q + 1]));
                 phase[q] += ms;
             }
+        }
+    }
+    if (time) {
+        if (cfl > 0) {
+            CK(h, cudaMemcpyAsync(time, h->d_time, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            CK(h, cudaStreamSynchronize(h->stream));
+        } else {
+            *time = dt * nsteps;
         }
     }
     if (!stats)
@@ -965,6 +1031,7 @@ eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
         return fail(h, EU_ERR_NCHEM, "%llu cells predicted Nchem <= 0 or above max_substeps", cnt[kCntBadNchem]);
     return EU_OK;
 }
+} // namespace
 
 eu_status eu_get_field(eu_handle *h, const char *name, double *out)
 {
@@ -1336,7 +1403,7 @@ eu_status eu_batch_step(eu_batch *b, int nsteps, const double *dt, eu_step_stats
             return bfail(b, EU_ERR_NOT_READY, "instance %d: mechanism and state must be set", i);
         if (h->cfg.chemistry == EU_CHEM_LEARNED && (!h->model || !mlp_has_fused(h->model)))
             return bfail(b, EU_ERR_UNSUPPORTED, "instance %d: learned chemistry needs a model with the fused kernel", i);
-        if (h->graph_dirty || !h->graph_exec) {
+        if (h->graph_dirty || !h->graph_exec || h->graph_cfl != 0) {
             const eu_status s = capture_step(h, launch_args(h), flavour(h));
             if (s != EU_OK)
                 return bfail(b, s, "instance %d: %s", i, h->err.c_str());

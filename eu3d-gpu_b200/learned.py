@@ -233,3 +233,44 @@ def attach(solver, model, gate):
     solver.set_learned(model, gate["tau"], gate["box_lo"], gate["box_hi"], gate["out_scale"],
                        frozen_y=gate["frozen_y"], frozen_T=gate["frozen_T"], frozen_radical=gate["frozen_radical"],
                        out_eps=gate["out_eps"], out_bound=gate["out_bound"])
+
+
+def front_check(model, gate, steps=20, dt=2e-8, grid=(40, 16, 16), device=0):
+    """Largest reaction-front shift (cells, eu3d_cases.front_shift) of the
+    learned + mixed step against the plain FP64 stiff step over `steps` steps
+    of an igniting validation block (1300-2500 K along x, 0.1-0.8 MPa along y,
+    0-50 % N2 along z: not the benchmark's block), with the given gate."""
+    import eu3d_cases as cases
+    mech = eu3d.parse_mechanism(cases.MECH_JA919, cases.THERMO)
+    ext = (0.0, grid[0] * 2.5e-4, 0.0, grid[1] * 2.5e-4, 0.0, grid[2] * 2.5e-4)
+    prim = cases.hot_reacting_block(grid[0] + 4, grid[1] + 4, grid[2] + 4, mech["mw"], mech["ns"],
+                                    t_range=(1300.0, 2500.0), p_range=(1e5, 8e5), n2_max=0.5)
+    ys = {}
+    for name, chem, prec in (("stiff", "stiff", "fp64"), ("learned", "learned", "mixed")):
+        s = eu3d.Solver(*grid, ext, precision=prec, chemistry=chem, arith="fast", device=device)
+        s.set_mechanism(mech)
+        s.set_primitive(*prim)
+        if chem == "learned":
+            attach(s, model, gate)
+        ys[name] = []
+        for _ in range(steps):
+            s.step(1, dt)
+            ys[name].append(s.get("Yi"))
+        s.close()
+    return max(cases.front_shift(a, b) for a, b in zip(ys["learned"], ys["stiff"]))
+
+
+def tighten_for_front(model, gate, max_shift=1, tries=5, log=print):
+    """Halve the gate's tau until the validation block's reaction front stays
+    within max_shift cells of the stiff run at every step."""
+    g = dict(gate)
+    g.setdefault("frozen_y", FROZEN_Y)
+    g.setdefault("frozen_T", FROZEN_T)
+    g.setdefault("frozen_radical", FROZEN_RADICAL)
+    for _ in range(tries):
+        shift = front_check(model, g)
+        log(f"tau {g['tau']:.4g}: front shift {shift} cells")
+        if shift <= max_shift:
+            return g, shift
+        g["tau"] *= 0.5
+    return g, shift

@@ -72,6 +72,14 @@ typedef enum {
     EU_ARITH_FAST = 1    /* FMA contraction allowed */
 } eu_arith;
 
+/* Ghost fill of the case (the reference wires one per case). */
+typedef enum {
+    EU_BC_RSBI = 0, /* Flowfield::FieldBoundary_3dRSBI (src/Flowfield.cpp:593-807) */
+    EU_BC_ZND = 1   /* Flowfield::FieldBoundary_1dZND (src/Flowfield.cpp:317-411, commented out in the
+                       reference): reflecting wall at x low, outflow with the thermo rebuilt at x high;
+                       y and z faces as RSBI */
+} eu_boundary;
+
 typedef struct {
     int total_ni, total_nj, total_nk; /* nodes per axis (grid file total_ni, ...) */
     double xa, xb, ya, yb, za, zb;    /* domain extents (grid file xa, xb, ...) */
@@ -85,6 +93,7 @@ typedef struct {
     int profile;                      /* nonzero: time each kernel phase with CUDA events */
     int eager;                        /* nonzero: launch each step's kernels one by one instead of
                                          replaying the step's captured CUDA graph */
+    int boundary;                     /* eu_boundary: which case's ghost fill */
 } eu_config;
 
 /* Mechanism and thermo tables in the reference's layouts (src/Reaction.cpp:156-327). */
@@ -121,6 +130,13 @@ int eu_abi_version(void);
 /* Parse a grid file in the reference's format (input/grid-*.txt) into cfg's
  * grid members; other members are left as they are. */
 eu_status eu_read_grid(const char *grid_path, eu_config *cfg);
+
+/* One numeric value of a key/value file in the reference's format (ctrl.txt,
+ * input-*.txt), read as FileReader::getdoubleParameter reads it
+ * (src/FileReader.cpp:53-84); EU_ERR_INVALID_ARGUMENT when the key is absent.
+ * The case initialisers take their parameters (P_bound, T_bound, P, T, ...)
+ * from these files. */
+eu_status eu_read_value(const char *path, const char *key, double *value);
 
 /* Parse a mechanism file and thermo.dat (reference formats) without a device.
  * Replaces Reaction::ReactionRead (src/Reaction.cpp:156-327). Pass NULL arrays
@@ -172,6 +188,15 @@ eu_status eu_set_state(eu_handle *h, const double *cs, const double *T, const do
 /* Advance nsteps timesteps of fixed dt. Asynchronous on the handle's stream
  * unless stats is non-NULL (then it synchronises and fills stats). */
 eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats);
+
+/* Advance nsteps timesteps, each of dt = cfl x min over the interior nodes of
+ * min(dx / (|u| + c), dy / (|v| + c)) on its own starting state, the reduction
+ * done on the device (Flowfield::CFLcondition, src/Flowfield.cpp:275-304, with
+ * the interior node spacings; the reference takes its spacings from the first
+ * two ghost nodes, which is the same for three or more nodes per axis).
+ * time_advanced (or NULL) receives the sum of the steps' dt (the call then
+ * synchronises). */
+eu_status eu_step_cfl(eu_handle *h, int nsteps, double cfl, eu_step_stats *stats, double *time_advanced);
 
 /* Copy a named field to host (haloed SoA planes). Names: P D T U V W H E Gamma
  * C Ma Wav Rgas Cp (1 plane); Yi Di Mc CMS (ns planes); CS (ns+4 planes); Nchem

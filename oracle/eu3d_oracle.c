@@ -41,6 +41,7 @@ struct eo_state {
     int *nchem;
     double dt;
     int bad_nchem;
+    int bc_kind; /* 0: RSBI ghost fill, 1: ZND */
 };
 
 #define IDX(st, i, j, k) (((long)(i) * (st)->ny + (j)) * (st)->nz + (k))
@@ -385,48 +386,64 @@ static void copy_cell(eo_state *st, long dst, long src, double su, double sv, do
     for (int s = 0; s < st->ns; s++) st->Y[s * n3 + dst] = st->Y[s * n3 + src];
 }
 
+/* Ghost node d from node s0 with the thermo recomputed from the mirrored T,
+ * p, Y (src/Flowfield.cpp:647-679; the same rebuild closes the ZND outflow,
+ * :340-366); sv flips the y velocity. */
+static void rebuild_cell(eo_state *st, long d, long s0, double sv)
+{
+    const int ns = st->ns;
+    const long n3 = st->n3;
+    st->U[d] = st->U[s0];
+    st->V[d] = sv * st->V[s0];
+    st->W[d] = st->W[s0];
+    st->P[d] = st->P[s0];
+    st->T[d] = st->T[s0];
+    const double T = st->T[d];
+    double rg = 0, cp = 0, h = 0, e = 0;
+    double Y[EO_MAXS], Cpi[EO_MAXS], Hi[EO_MAXS], Ei[EO_MAXS];
+    for (int s = 0; s < ns; s++) {
+        Y[s] = st->Y[s * n3 + s0];
+        st->Y[s * n3 + d] = Y[s];
+        Cpi[s] = get_cpi(st, T, st->ri[s], s);
+        Hi[s] = get_hi(st, T, st->ri[s], s);
+        Ei[s] = Hi[s] - st->ri[s] * T;
+    }
+    for (int s = 0; s < ns; s++) rg += Y[s] * st->ri[s];
+    const double Rgas = rg * 1000;
+    st->D[d] = st->P[d] / (T * Rgas);
+    for (int s = 0; s < ns; s++) cp += Cpi[s] * Y[s];
+    for (int s = 0; s < ns; s++) h += Y[s] * Hi[s];
+    for (int s = 0; s < ns; s++) e += Y[s] * Ei[s];
+    const double Cp = cp * 1000;
+    st->H[d] = h * 1000;
+    st->E[d] = e * 1000;
+    st->G[d] = Cp / (Cp - Rgas);
+}
+
 static void boundary_fill(eo_state *st)
 {
-    const int ni = st->ni, nj = st->nj, nk = st->nk, bc = st->bc, ns = st->ns;
-    const long n3 = st->n3;
-    /* x: zero-gradient mirror copy (src/Flowfield.cpp:597-641) */
+    const int ni = st->ni, nj = st->nj, nk = st->nk, bc = st->bc;
+    /* x, RSBI: zero-gradient mirror copy (src/Flowfield.cpp:597-641);
+     * ZND (Flowfield::FieldBoundary_1dZND, :317-366, commented out in the
+     * reference): reflecting wall at x low (U reflected), outflow at x high
+     * with the thermo rebuilt */
     for (int i = 0; i < bc; i++)
         for (int j = bc; j < nj + bc; j++)
             for (int k = bc; k < nk + bc; k++) {
-                copy_cell(st, IDX(st, i, j, k), IDX(st, 2 * bc - 1 - i, j, k), 1, 1, 1);
-                copy_cell(st, IDX(st, ni + bc + i, j, k), IDX(st, 2 * (ni + bc) - 1 - (ni + bc + i), j, k), 1, 1, 1);
+                const long lo = IDX(st, i, j, k), hi = IDX(st, ni + bc + i, j, k);
+                const long slo = IDX(st, 2 * bc - 1 - i, j, k), shi = IDX(st, 2 * (ni + bc) - 1 - (ni + bc + i), j, k);
+                if (st->bc_kind == 1) {
+                    copy_cell(st, lo, slo, -1, 1, 1);
+                    rebuild_cell(st, hi, shi, 1);
+                } else {
+                    copy_cell(st, lo, slo, 1, 1, 1);
+                    copy_cell(st, hi, shi, 1, 1, 1);
+                }
             }
     /* y front: symmetry with thermo recomputed from mirrored T, p, Y (:647-679) */
     for (int i = bc; i < ni + bc; i++)
         for (int j = 0; j < bc; j++)
-            for (int k = bc; k < nk + bc; k++) {
-                const long d = IDX(st, i, j, k), s0 = IDX(st, i, 2 * bc - 1 - j, k);
-                st->U[d] = st->U[s0];
-                st->V[d] = -st->V[s0];
-                st->W[d] = st->W[s0];
-                st->P[d] = st->P[s0];
-                st->T[d] = st->T[s0];
-                const double T = st->T[d];
-                double rg = 0, cp = 0, h = 0, e = 0;
-                double Y[EO_MAXS], Cpi[EO_MAXS], Hi[EO_MAXS], Ei[EO_MAXS];
-                for (int s = 0; s < ns; s++) {
-                    Y[s] = st->Y[s * n3 + s0];
-                    st->Y[s * n3 + d] = Y[s];
-                    Cpi[s] = get_cpi(st, T, st->ri[s], s);
-                    Hi[s] = get_hi(st, T, st->ri[s], s);
-                    Ei[s] = Hi[s] - st->ri[s] * T;
-                }
-                for (int s = 0; s < ns; s++) rg += Y[s] * st->ri[s];
-                const double Rgas = rg * 1000;
-                st->D[d] = st->P[d] / (T * Rgas);
-                for (int s = 0; s < ns; s++) cp += Cpi[s] * Y[s];
-                for (int s = 0; s < ns; s++) h += Y[s] * Hi[s];
-                for (int s = 0; s < ns; s++) e += Y[s] * Ei[s];
-                const double Cp = cp * 1000;
-                st->H[d] = h * 1000;
-                st->E[d] = e * 1000;
-                st->G[d] = Cp / (Cp - Rgas);
-            }
+            for (int k = bc; k < nk + bc; k++) rebuild_cell(st, IDX(st, i, j, k), IDX(st, i, 2 * bc - 1 - j, k), -1);
     /* y back: zero-gradient mirror copy (:684-705) */
     for (int i = bc; i < ni + bc; i++)
         for (int j = nj + bc; j < nj + 2 * bc; j++)
@@ -638,6 +655,8 @@ void eo_set_state(eo_state *st, const double *cs, const double *T, const double 
 }
 
 void eo_boundary(eo_state *st) { boundary_fill(st); }
+
+void eo_set_boundary(eo_state *st, int kind) { st->bc_kind = kind; }
 
 int eo_step(eo_state *st, int nsteps, double dt)
 {

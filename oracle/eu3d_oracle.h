@@ -58,6 +58,10 @@ int eo_step(eo_state *st, int nsteps, double dt);
 
 /* The RSBI ghost fill alone (src/Flowfield.cpp:593-807, face layers). */
 void eo_boundary(eo_state *st);
+/* Ghost fill kind: 0 RSBI (default), 1 ZND (reflecting wall at x low, outflow
+ * with the thermo rebuilt at x high; Flowfield::FieldBoundary_1dZND,
+ * src/Flowfield.cpp:317-411, commented out in the reference). */
+void eo_set_boundary(eo_state *st, int kind);
 
 /* Copy a named field out (SoA, haloed). Names: P D T U V W H E Gamma C Ma Wav
  * Rgas Cp (1 plane); Yi Di Mc CMS (ns planes); CS (ns+4 planes); Nchem (1 plane,

@@ -62,6 +62,13 @@ class Mechanism:
         return cls(int(z["ns"]), int(z["nr"]), z["mw"], z["coeff_lo"], z["coeff_hi"], z["af"], z["bf"],
                    z["eaf"], z["stoi_f"], z["stoi_b"], z["tb"])
 
+    @classmethod
+    def from_dict(cls, d):
+        """From the library parser's dict (eu3d.parse_mechanism): same layouts."""
+        return cls(int(d["ns"]), int(d["nr"]), *[np.asarray(d[k], dtype=np.float64) for k in
+                                                  ("mw", "coeff_lo", "coeff_hi", "af", "bf", "eaf", "stoi_f",
+                                                   "stoi_b", "tb")])
+
     def save_npz(self, path):
         np.savez(path, ns=self.ns, nr=self.nr, mw=self.mw, coeff_lo=self.coeff_lo, coeff_hi=self.coeff_hi,
                  af=self.af, bf=self.bf, eaf=self.eaf, stoi_f=self.stoi_f, stoi_b=self.stoi_b, tb=self.tb)
@@ -233,6 +240,7 @@ class PortOracle:
             lib.eo_step.restype = _I
             lib.eo_step.argtypes = [_P, _I, _D]
             lib.eo_boundary.argtypes = [_P]
+            lib.eo_set_boundary.argtypes = [_P, _I]
             lib.eo_get.restype = _I
             lib.eo_get.argtypes = [_P, ctypes.c_char_p, _P]
             lib.eo_thermo.argtypes = [_P, _D, _D, _I, _P]
@@ -248,7 +256,7 @@ class PortOracle:
                                                 ("mw", "coeff_lo", "coeff_hi", "af", "bf", "eaf",
                                                  "stoi_f", "stoi_b", "tb")]
 
-    def __init__(self, ni, nj, nk, x, y, z, mech: Mechanism, bc=2, nthreads=None):
+    def __init__(self, ni, nj, nk, x, y, z, mech: Mechanism, bc=2, nthreads=None, boundary="rsbi"):
         lib = self.lib()
         self.ni, self.nj, self.nk, self.bc = ni, nj, nk, bc
         self.ns, self.nr = mech.ns, mech.nr
@@ -262,6 +270,7 @@ class PortOracle:
                                ctypes.byref(m), int(nthreads))
         if not self.h:
             raise RuntimeError("eo_create failed")
+        lib.eo_set_boundary(self.h, {"rsbi": 0, "znd": 1}[boundary])
 
     def close(self):
         if self.h:

@@ -99,14 +99,15 @@ def hot_mixture(gpu, chemistry, precision="fp64"):
 
 
 def test_trained_model_replaces_stiff_substeps(gpu):
-    """What the trained network gains over the stiff kinetics alone: on hot
-    reacting gas the committed checkpoint advances a share of the cells itself
-    (the gate is calibrated for a mean species L1 of 5e-6 per step, so it
-    accepts only the cells the ensemble agrees on: about 15 % of this block),
-    and every one of them is a trapezoid substep the stiff kinetics does not
-    run; the rejected cells take the stiff kinetics' own substeps (the same
-    FP64 arithmetic). The species error (mean over cells of sum_s |dY_s|
-    against the stiff step) stays within 1e-4."""
+    """What the trained network gains over the stiff kinetics alone, at the
+    committed gate: every cell the model advances is a trapezoid substep the
+    stiff kinetics does not run, and the rejected cells take the stiff
+    kinetics' own substeps (the same FP64 arithmetic). The gate is tight (tau
+    calibrated for a mean species L1 of 5e-6 per step, then halved so that the
+    reaction front of an igniting validation block stays within one cell), so
+    on this block of hot reacting gas it takes about 1 % of the cells. The
+    species error (mean over cells of sum_s |dY_s| against the stiff step)
+    stays within 1e-4."""
     import learned
     dt = 5e-8
     a = hot_mixture(gpu, "stiff")
@@ -118,7 +119,7 @@ def test_trained_model_replaces_stiff_substeps(gpu):
     n = 24 * 8 * 8
     assert sa["reacting"] == n and sb["reacting"] == n
     assert sb["learned"] + sb["fallback"] == n
-    assert sb["learned"] >= 0.1 * n, sb
+    assert sb["learned"] >= 0.005 * n, sb
     assert sb["sum_nchem"] <= sa["sum_nchem"] - sb["learned"], (sa["sum_nchem"], sb["sum_nchem"], sb["learned"])
     ya, yb = interior(a.get("Yi")), interior(b.get("Yi"))
     l1 = np.abs(ya - yb).sum(axis=0)
@@ -201,3 +202,27 @@ def test_batch_of_uneven_instances_equals_one_by_one(gpu):
         for f in ("CS", "T", "Yi"):
             assert n_unequal(a.get(f), c.get(f)) == 0, f
     b.close()
+
+
+def test_learned_front_within_one_cell(gpu):
+    """Over 10 steps of igniting gas (24 x 8 x 8 block, 1300-2600 K along x,
+    dt 2e-8 s) the learned + mixed step keeps the reaction front (the first
+    node along x where H2O reaches half the stiff run's column maximum, in the
+    columns where it reaches 1e-2) within one cell of the plain FP64 stiff run
+    in every column, at a species L1 (mean over cells of sum_s |dY_s|) within
+    1e-3."""
+    import learned
+    model, gate = learned.load()
+    ys = {}
+    for chem, prec in (("stiff", "fp64"), ("learned", "mixed")):
+        s = hot_mixture(gpu, chem, prec)
+        if chem == "learned":
+            learned.attach(s, model, gate)
+        ys[chem] = []
+        for _ in range(10):
+            s.step(1, 2e-8)
+            ys[chem].append(s.get("Yi"))
+        s.close()
+    assert max(cases.front_shift(a, b) for a, b in zip(ys["learned"], ys["stiff"])) <= 1
+    l1 = np.abs(interior(ys["learned"][-1]) - interior(ys["stiff"][-1])).sum(axis=0)
+    assert l1.mean() <= 1e-3, l1.mean()

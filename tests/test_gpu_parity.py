@@ -213,3 +213,46 @@ def test_autotuned_launch_shapes_change_no_bits(gpu, precision, arith):
         s.close()
     for a, b in zip(*out):
         assert n_unequal(a, b) == 0
+
+
+def test_znd_against_restatement(gpu, port_lib):
+    """The 1-D ZND initiation (2H2+O2+7Ar on the Ar variant of the mechanism,
+    1 MPa / 3000 K driver at a reflecting wall, 6.67 kPa / 298 K gas ahead,
+    parameters from data/input-1dZND.txt, driver edge a 2-cell tanh profile)
+    with the ZND ghost fill, on a
+    401 x 2 x 2 node grid at 25 um spacing, against the pinned C restatement
+    with the same ghost fill: relative L-inf <= 1e-10 per conserved variable
+    after 100 steps (strict arithmetic), Nchem exact. Each step's dt comes from
+    the device-side CFL reduction at 0.5 (eu_step_cfl) and the restatement
+    takes the same dt."""
+    from oracle import Mechanism
+    ni, nj, nk = 401, 2, 2
+    dx = 25e-6
+    ext = (0.0, (ni - 1) * dx, 0.0, dx, 0.0, dx)
+    x = cases.node_coordinates(ni, ext[0], ext[1])
+    y = cases.node_coordinates(nj, ext[2], ext[3])
+    mech = gpu.parse_mechanism(cases.MECH_JA919_AR, cases.THERMO_AR)
+    prim = cases.znd(x, y, y, mech["mw"], mech["ns"])
+    port = port_lib(ni, nj, nk, x, y, y, Mechanism.from_dict(mech), boundary="znd")
+    port.set_primitive(*prim)
+    s = gpu.Solver(ni, nj, nk, ext, record_sources=True, boundary="znd")
+    s.set_mechanism(mech)
+    s.set_primitive(*prim)
+    # the first dt against the host rule on the initial state (interior
+    # spacings: the reference's rule takes dy from its ghost nodes, which a
+    # two-node direction makes negative)
+    p, cs, T, E = gpu.initial_state(mech, ni, nj, nk, *prim)
+    dt0 = cases.cfl_dt(x, x, p[0], p[1], p[2], p[3], p[6], 0.5)
+    peak = 0
+    for n in range(100):
+        st, dt = s.step_cfl(1, 0.5)
+        if n == 0:
+            assert abs(dt - dt0) <= 1e-12 * dt0, (dt, dt0)
+        port.step(1, dt)
+        peak = max(peak, st["max_nchem"])
+    assert peak >= 1
+    assert rel_linf(interior(s.get("CS")), interior(port.get("CS"))).max() <= 1e-10
+    assert n_unequal(interior(s.get("Nchem")), interior(port.get("Nchem"))) == 0
+    # the wall reflects: the ghost velocity mirrors the first nodes' with the sign flipped
+    u = s.get("U")
+    assert np.array_equal(u[0, 0:2, 2, 2], -u[0, 3:1:-1, 2, 2])

@@ -115,3 +115,27 @@ def test_ghost_fill_matches_reference(ref_lib, port_lib):
         r, p = ref.get(f), port.get(f)
         for sl in faces:
             assert n_unequal(p[(slice(None),) + sl], r[(slice(None),) + sl]) == 0, (f, sl)
+
+
+def test_znd_ghost_fill_of_the_restatement(port_lib):
+    """The C restatement's ZND ghost fill (the reference's commented-out
+    Flowfield::FieldBoundary_1dZND, src/Flowfield.cpp:317-411): the x-low
+    ghosts mirror the first nodes with U reflected, the x-high ghosts mirror
+    the last nodes with density rebuilt from the mirrored p, T, Y."""
+    from oracle import Mechanism
+    import eu3d
+    ni, nj, nk = 12, 2, 2
+    dx = 25e-6
+    x = cases.node_coordinates(ni, 0.0, (ni - 1) * dx)
+    y = cases.node_coordinates(nj, 0.0, dx)
+    md = eu3d.parse_mechanism(cases.MECH_JA919_AR, cases.THERMO_AR)
+    P, T, U, V, W, Y = cases.znd(x, y, y, md["mw"], md["ns"])
+    U = U + np.linspace(10.0, 20.0, ni + 4)[:, None, None]
+    o = port_lib(ni, nj, nk, x, y, y, Mechanism.from_dict(md), boundary="znd")
+    o.set_primitive(P, T, U, V, W, Y)
+    o.boundary()
+    u, d, p = o.get("U")[0], o.get("D")[0], o.get("P")[0]
+    assert np.array_equal(u[0:2, 2, 2], -u[3:1:-1, 2, 2])
+    assert np.array_equal(u[ni + 2:ni + 4, 2, 2], u[ni + 1:ni - 1:-1, 2, 2])
+    assert np.array_equal(p[ni + 2:ni + 4, 2, 2], p[ni + 1:ni - 1:-1, 2, 2])
+    assert np.allclose(d[ni + 2:ni + 4, 2, 2], d[ni + 1:ni - 1:-1, 2, 2], rtol=1e-14)
