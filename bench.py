@@ -46,6 +46,13 @@ L2_BYTES = 126 * 2 ** 20
 # Algorithmic bytes per cell-step of the flux + update kernel: 16 primitives
 # read, 13 conserved read and written (FP64); FP32 primitives in mixed mode.
 FLUX_BYTES = {"fp64": (16 + 26) * 8, "mixed": 16 * 4 + 26 * 8}
+# DRAM bytes per cell of one launch of the mixed-precision flux kernel, from the
+# ncu capture summarised in profiles/flux_tiled_and_recover_classify_256x128x64.md
+# (dram__bytes_read.sum + dram__bytes_write.sum at 256 x 128 x 64 nodes, divided by
+# the cells; the traffic scales with the cells, so it is scaled to the grid).
+FLUX_TRAFFIC_PER_CELL = {"mixed": 287.4}
+# FLOPs per row of the learned ensemble (3 members x 2 (12 256 + 256 256 + 256 256 + 256 10)).
+MLP_FLOP_PER_ROW = 820224
 # FP64 flops per cell-substep of the stiff kinetics (rates, trapezoid update,
 # state rebuild with its temperature Newton), counted on the oracle over the
 # thin RSBI case by oracle/flop_count.cpp.
@@ -273,6 +280,34 @@ def species_error(a, b, bc=2):
     l1 = np.abs(ya - yb).sum(axis=0)
     reactive = yb[:8].sum(axis=0) > 1e-9
     return float(l1.mean()), float(l1[reactive].mean()) if reactive.any() else 0.0
+
+
+def mlp_roofline(model, rows=1 << 18, reps=5):
+    """The fused inference kernel (eu_mlp_predict_fused) on `rows` feature rows
+    drawn inside the model's input box: FLOPs of the 3-member ensemble per
+    second, against the measured BF16 dense peak."""
+    import torch
+    z = np.load(__import__("learned").CHECKPOINT)
+    lo, hi = z["box_lo"].astype(np.float32), z["box_hi"].astype(np.float32)
+    g = torch.Generator(device="cuda").manual_seed(7)
+    X = (torch.from_numpy(lo).cuda() + torch.rand(rows, lo.size, device="cuda", generator=g) *
+         torch.from_numpy(hi - lo).cuda()).contiguous()
+    members = int(z["shape"][4])
+    out = torch.empty(members, rows, int(z["shape"][3]), device="cuda")
+    model.predict_fused(X, out)
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(torch.cuda.current_stream())
+    for _ in range(reps):
+        model.predict_fused(X, out)
+    s1.record(torch.cuda.current_stream())
+    torch.cuda.synchronize()
+    ms = s0.elapsed_time(s1) / reps
+    _, bf16, kind = measured_peaks()
+    tf = MLP_FLOP_PER_ROW * rows / (ms / 1e3) / 1e12
+    return {"kernel": "mlp_fused", "bound": "tensor", "rows": rows, "ms": round(ms, 4), "achieved": round(tf, 2),
+            "peak": bf16, "unit": "TFLOP/s", "frac": round(tf / bf16, 4), "peak_source": f"{kind} bf16_tflops",
+            "note": "each call synchronises the model's stream (error check), included"}
 
 
 def reacting_block(args, model, gate, local, dt=2e-8):
@@ -510,6 +545,7 @@ def our_arm(args):
 
     # -- reacting gas: the chemistry phase the learned model replaces ---------------------------
     block = reacting_block(args, model, gate, local) if args.chem == "learned" else None
+    mlp = mlp_roofline(model) if args.chem == "learned" else None
 
     # -- uneven instances advanced together (one graph launch per step) ----------------------
     batch = None
@@ -536,7 +572,10 @@ def our_arm(args):
     flux_gbs = FLUX_BYTES[args.precision] * ncell / (flux_ms / 1e3) / 1e9
     dominant = max(range(3), key=lambda q: phase[q])
     roofline = {"kernel": "flux_update", "bound": "hbm", "achieved": round(flux_gbs, 1), "peak": hbm,
-                "unit": "GB/s", "frac": round(flux_gbs / hbm, 4), "traffic": None,
+                "unit": "GB/s", "frac": round(flux_gbs / hbm, 4),
+                "traffic": (round(FLUX_TRAFFIC_PER_CELL[args.precision] * ncell / 1e9, 4)
+                            if args.precision in FLUX_TRAFFIC_PER_CELL else None),
+                "traffic_unit": "GB per launch (ncu, scaled from 256x128x64)",
                 "algorithmic_bytes_per_cell": FLUX_BYTES[args.precision], "peak_source": f"{peak_kind} hbm_gbs",
                 "dominant_kernel": names[dominant],
                 "dominant_share": round(phase[dominant] / max(sum(phase[:3]), 1e-9), 3)}
@@ -582,6 +621,7 @@ def our_arm(args):
                 "plain_fp64": plain,
                 "reacting_block": block,
                 "batch_instances": batch,
+                "mlp_roofline": mlp,
                 "znd_1d": znd,
                 "roofline": roofline, "kernels_ms_per_step": per_kernel,
                 "max_nchem": stats["max_nchem"], "reacting_cells": stats["reacting"],

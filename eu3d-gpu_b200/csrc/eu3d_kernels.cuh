@@ -969,6 +969,9 @@ __global__ void __launch_bounds__(128, 1) k_react_heavy(const __grid_constant__ 
                                                      int max_substeps)
 {
     __shared__ DevMech ms;
+    const int count = st.heavy[0];
+    if (count == 0) // no deferred cell this step: skip the table copy
+        return;
     {
         const int *src = reinterpret_cast<const int *>(&m);
         int *dst = reinterpret_cast<int *>(&ms);
@@ -976,7 +979,6 @@ __global__ void __launch_bounds__(128, 1) k_react_heavy(const __grid_constant__ 
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    const int count = st.heavy[0];
     const double dtm = *dt_dev;
     const long long n3 = g.n3;
     for (;;) {

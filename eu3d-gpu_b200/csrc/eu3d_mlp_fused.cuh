@@ -2,7 +2,7 @@
 // one persistent tcgen05 kernel (inference only; training uses the layer-wise
 // GEMMs of eu3d_gemm.cuh).
 //
-// One CTA of 128 threads per SM walks the 128-row tiles of the input rows
+// One CTA of 512 threads per SM walks the 128-row tiles of the input rows
 // (tile = blockIdx.x, blockIdx.x + gridDim.x, ...). The row count may be read
 // from device memory when the kernel starts, so a launch needs no host-side
 // count and can sit in a captured CUDA graph. For each tile and member, every
@@ -17,7 +17,8 @@
 // that each slab is one contiguous bulk copy (cp.async.bulk, completion counted
 // on a "full" mbarrier); the MMAs that read a slot commit to its "empty"
 // mbarrier. Thread 0 issues the copies and the MMAs; all threads run the
-// epilogues. Every wait is bounded: on a timeout the CTA records an error,
+// epilogues: warp w reads TMEM lanes 32 (w % 4) (its rows) and the four warp
+// groups take every fourth 32-column chunk of the accumulator. Every wait is bounded: on a timeout the CTA records an error,
 // waits (bounded) for its copies in flight, frees its TMEM and returns.
 //
 // The arithmetic is the layer-wise path's: the same K=16 MMA sequence into an
@@ -33,7 +34,7 @@
 
 namespace eu3d {
 
-constexpr int kFusedStages = 3, kFusedRows = 128, kFusedThreads = 128;
+constexpr int kFusedStages = 3, kFusedRows = 128, kFusedThreads = 512, kFusedGroups = kFusedThreads / 128;
 
 // Bytes of shared memory the kernel needs for a model.
 // At least 116 KB, so that one CTA (and its 256 TMEM columns) fits per SM.
@@ -85,6 +86,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     uint32_t *tslot = reinterpret_cast<uint32_t *>(empty + kFusedStages);
 
     const int tid = threadIdx.x, warp = tid / 32;
+    const int lrow = tid % kFusedRows, wg = tid / kFusedRows; // tile row (TMEM lane), warp group
     int count = count_dev ? *count_dev : count_host;
     count = count < max_rows ? count : max_rows;
     const int ntiles = (count + kFusedRows - 1) / kFusedRows;
@@ -143,10 +145,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     long long g = 0; // slabs consumed so far (all threads track it)
     for (int it = 0; it < mine && ok; ++it) {
         const int tile = int(blockIdx.x) + it * int(gridDim.x);
-        const int row = tile * kFusedRows + tid;
+        const int row = tile * kFusedRows + lrow;
         const bool valid = row < count;
         // features -> fin (core-matrix layout, 8 bf16 per 16-byte chunk)
-        for (int kc = 0; kc < p.in_pad / 8; ++kc) {
+        for (int kc = wg; kc < p.in_pad / 8; kc += kFusedGroups) {
             __align__(16) __nv_bfloat16 v[8];
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
@@ -156,7 +158,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
                     x = (feat[(long long)row * ld_feat + c] - p.in_shift[c]) * p.in_scale[c];
                 v[q] = __float2bfloat16_rn(x);
             }
-            *reinterpret_cast<uint4 *>(fin + (kc * kFusedRows + tid) * 16) = *reinterpret_cast<const uint4 *>(v);
+            *reinterpret_cast<uint4 *>(fin + (kc * kFusedRows + lrow) * 16) = *reinterpret_cast<const uint4 *>(v);
         }
         tc::fence_proxy_async();
         tc::tc_fence_before();
@@ -199,9 +201,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
                     break;
                 tc::tc_fence_after();
                 const float *bias = p.bias[e][l];
-                const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);
+                const uint32_t trow = tmem + (uint32_t((warp % 4) * 32) << 16);
                 if (l < p.layers - 1) {
-                    for (int c0 = 0; c0 < N; c0 += 32) {
+                    for (int c0 = wg * 32; c0 < N; c0 += 32 * kFusedGroups) {
                         float v[32];
                         tc::tmem_ld32(trow + c0, v);
 #pragma unroll
@@ -211,14 +213,14 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
                                 __align__(16) __nv_bfloat16 h[8];
 #pragma unroll
                                 for (int q = 0; q < 8; ++q) h[q] = __float2bfloat16_rn(silu(v[j * 8 + q] + bias[cbase + q]));
-                                *reinterpret_cast<uint4 *>(act + ((cbase / 8) * kFusedRows + tid) * 16) =
+                                *reinterpret_cast<uint4 *>(act + ((cbase / 8) * kFusedRows + lrow) * 16) =
                                     *reinterpret_cast<const uint4 *>(h);
                             }
                         }
                     }
                     tc::fence_proxy_async();
                 } else {
-                    for (int c0 = 0; c0 < N; c0 += 32) {
+                    for (int c0 = wg * 32; c0 < N; c0 += 32 * kFusedGroups) {
                         float v[32];
                         tc::tmem_ld32(trow + c0, v);
                         if (valid) {
