@@ -26,7 +26,12 @@ constexpr int kGemmBM = 128, kGemmBK = 64, kGemmThreads = 128;
 // atomics (split-K partial sums; no bias).
 enum GemmAct { kActNone = 0, kActSilu = 1, kActSiluGrad = 2, kActAccumulate = 3 };
 
-__device__ __forceinline__ float silu(float x) { return x / (1.0f + __expf(-x)); }
+// SiLU with the hardware's approximate division (reciprocal and multiply, about
+// two units in the last place): the activations are rounded to bf16 next, eight
+// bits of mantissa, so the division's last bits rarely survive. For x below
+// about -87 the denominator overflows and the result is 0 (the exact value is
+// below 1e-36 in magnitude).
+__device__ __forceinline__ float silu(float x) { return __fdividef(x, 1.0f + __expf(-x)); }
 __device__ __forceinline__ float silu_grad(float z)
 {
     const float s = 1.0f / (1.0f + __expf(-z));

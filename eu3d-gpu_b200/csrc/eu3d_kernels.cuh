@@ -708,8 +708,10 @@ __global__ void __launch_bounds__(128) k_recover_react(const __grid_constant__ D
 // Post-advection recovery of every cell; cells with chemistry to do are
 // appended to the learned queue (warp-aggregated atomics), the others are
 // final. Every cell's recovered state is stored.
-template <int NS>
-__global__ void __launch_bounds__(128, 5) k_recover_classify(const __grid_constant__ DevMech m, const DevGrid g,
+// MINB: resident blocks per SM the register allocation aims at (the
+// autotuner picks the instantiation; fewer registers, more warps, some spills).
+template <int NS, int MINB = 5>
+__global__ void __launch_bounds__(128, MINB) k_recover_classify(const __grid_constant__ DevMech m, const DevGrid g,
                                                           const DevState st, LearnedParams lp)
 {
     const long long ncell = (long long)g.ni * g.nj * g.nk;

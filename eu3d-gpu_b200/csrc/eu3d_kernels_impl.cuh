@@ -121,8 +121,13 @@ cudaError_t classify_t(const LaunchArgs &a, const LearnedParams &lp)
 {
     const long long n = (long long)a.g.ni * a.g.nj * a.g.nk;
     const int threads = a.recover_block > 0 ? a.recover_block : 128;
-    k_recover_classify<NS><<<dim3(unsigned((n + threads - 1) / threads)), threads, 0, a.stream>>>(*a.mech, a.g, a.st,
-                                                                                                  lp);
+    const dim3 grid(unsigned((n + threads - 1) / threads));
+    switch (a.recover_minb) {
+    case 4: k_recover_classify<NS, 4><<<grid, threads, 0, a.stream>>>(*a.mech, a.g, a.st, lp); break;
+    case 6: k_recover_classify<NS, 6><<<grid, threads, 0, a.stream>>>(*a.mech, a.g, a.st, lp); break;
+    case 8: k_recover_classify<NS, 8><<<grid, threads, 0, a.stream>>>(*a.mech, a.g, a.st, lp); break;
+    default: k_recover_classify<NS, 5><<<grid, threads, 0, a.stream>>>(*a.mech, a.g, a.st, lp); break;
+    }
     return cudaGetLastError();
 }
 

@@ -53,14 +53,17 @@ class LearnedConfig(ctypes.Structure):
 
 class TuneReport(ctypes.Structure):
     _fields_ = [("flux_candidates", _I), ("flux_ci", _I * 16), ("flux_ms", ctypes.c_float * 16),
-                ("recover_candidates", _I), ("recover_block", _I * 8), ("recover_ms", ctypes.c_float * 8),
-                ("chosen_flux_ci", _I), ("chosen_recover_block", _I)]
+                ("recover_candidates", _I), ("recover_block", _I * 16), ("recover_minblocks", _I * 16),
+                ("recover_ms", ctypes.c_float * 16), ("chosen_flux_ci", _I), ("chosen_recover_block", _I),
+                ("chosen_recover_minblocks", _I)]
 
     def as_dict(self):
         nf, nr = self.flux_candidates, self.recover_candidates
         return {"flux_ms": {int(self.flux_ci[q]): round(float(self.flux_ms[q]), 4) for q in range(nf)},
-                "recover_ms": {int(self.recover_block[q]): round(float(self.recover_ms[q]), 4) for q in range(nr)},
-                "flux_ci": self.chosen_flux_ci, "recover_block": self.chosen_recover_block}
+                "recover_ms": {f"{self.recover_block[q]}x{self.recover_minblocks[q]}": round(float(self.recover_ms[q]), 4)
+                               for q in range(nr)},
+                "flux_ci": self.chosen_flux_ci, "recover_block": self.chosen_recover_block,
+                "recover_minblocks": self.chosen_recover_minblocks}
 
 
 class StepStats(ctypes.Structure):

@@ -65,7 +65,7 @@ struct eu_handle {
     double graph_cfl = 0;   // the CFL number the captured step sets its dt from (0: a fixed dt)
     unsigned graph_gen = 0; // captures so far (batches rebuild when it changes)
     // launch shapes picked by eu_autotune (0: defaults)
-    int flux_ci = 0, recover_block = 0;
+    int flux_ci = 0, recover_block = 0, recover_minb = 0;
     std::string err;
 };
 
@@ -227,13 +227,14 @@ LaunchArgs launch_args(eu_handle *h)
     a.sms = h->sms;
     a.flux_ci = h->flux_ci;
     a.recover_block = h->recover_block;
+    a.recover_minb = h->recover_minb;
     a.stream = h->stream;
     return a;
 }
 
 using TuneKey = std::tuple<int, int, int, int, int, int, int>;
 std::mutex g_tune_mutex;                            // guards g_tuned
-std::map<TuneKey, std::pair<int, int>> g_tuned;     // (flux_ci, recover_block) per grid and mode
+std::map<TuneKey, std::array<int, 3>> g_tuned;      // (flux_ci, recover_block, recover_minb) per grid and mode
 
 TuneKey tune_key(const eu_handle *h)
 {
@@ -478,8 +479,9 @@ eu_status eu_create(const eu_config *cfg, eu_handle **out)
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tuned.find(tune_key(h));
         if (it != g_tuned.end()) {
-            h->flux_ci = it->second.first;
-            h->recover_block = it->second.second;
+            h->flux_ci = it->second[0];
+            h->recover_block = it->second[1];
+            h->recover_minb = it->second[2];
         }
     }
     *out = h;
@@ -1576,29 +1578,37 @@ eu_status eu_autotune(eu_handle *h, int reps, eu_tune_report *report)
     };
     restore();
     best = 1e30f;
-    for (int rb : rb_cand) {
-        if (e != cudaSuccess)
-            break;
-        a.recover_block = rb;
-        float ms = 0;
-        e = time_it(
-            [&] {
-                if (learned) {
-                    cudaError_t r = cudaMemsetAsync(h->lp.counts, 0, 3 * sizeof(int), h->stream);
-                    return r == cudaSuccess ? L.recover_classify(a, h->lp) : r;
-                }
-                return L.recover_react(a, false);
-            },
-            &ms);
-        if (rep.recover_candidates < 8) {
-            rep.recover_block[rep.recover_candidates] = rb;
-            rep.recover_ms[rep.recover_candidates++] = ms;
+    int best_minb = 5;
+    const int minb_learned[] = {4, 5, 6, 8}, minb_other[] = {5};
+    const int *minbs = learned ? minb_learned : minb_other;
+    const int n_minb = learned ? 4 : 1;
+    for (int rb : rb_cand)
+        for (int mq = 0; mq < n_minb; ++mq) {
+            if (e != cudaSuccess)
+                break;
+            a.recover_block = rb;
+            a.recover_minb = minbs[mq];
+            float ms = 0;
+            e = time_it(
+                [&] {
+                    if (learned) {
+                        cudaError_t r = cudaMemsetAsync(h->lp.counts, 0, 3 * sizeof(int), h->stream);
+                        return r == cudaSuccess ? L.recover_classify(a, h->lp) : r;
+                    }
+                    return L.recover_react(a, false);
+                },
+                &ms);
+            if (rep.recover_candidates < 16) {
+                rep.recover_block[rep.recover_candidates] = rb;
+                rep.recover_minblocks[rep.recover_candidates] = minbs[mq];
+                rep.recover_ms[rep.recover_candidates++] = ms;
+            }
+            if (ms < best) {
+                best = ms;
+                best_rb = rb;
+                best_minb = minbs[mq];
+            }
         }
-        if (ms < best) {
-            best = ms;
-            best_rb = rb;
-        }
-    }
     restore();
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(h->stream);
@@ -1607,13 +1617,15 @@ eu_status eu_autotune(eu_handle *h, int reps, eu_tune_report *report)
         return cuda_fail(h, e, "autotune");
     h->flux_ci = best_ci;
     h->recover_block = best_rb;
+    h->recover_minb = best_minb;
     h->graph_dirty = true;
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
-        g_tuned[tune_key(h)] = {best_ci, best_rb};
+        g_tuned[tune_key(h)] = {best_ci, best_rb, best_minb};
     }
     rep.chosen_flux_ci = best_ci;
     rep.chosen_recover_block = best_rb;
+    rep.chosen_recover_minblocks = best_minb;
     if (report)
         *report = rep;
     return EU_OK;

@@ -334,8 +334,8 @@ eu_status eu_set_learned(eu_handle *h, eu_mlp *model, const eu_learned_config *c
 
 /* Autotuner: times the launch shapes that change no arithmetic (every
  * candidate gives bitwise the same state) on the handle's current state, which
- * it restores: the x-march length of the flux kernels and the block size of
- * the recovery kernels. The choice applies to this handle and to handles
+ * it restores: the x-march length of the flux kernels, the block size of the
+ * recovery kernels and, in learned mode, the recovery's register target. The choice applies to this handle and to handles
  * created later in the process with the same grid and mode. reps: timed
  * launches per candidate. report (or NULL) receives the candidates' times.
  * Allocates a temporary copy of the state. No counterpart in the reference. */
@@ -344,10 +344,12 @@ typedef struct {
     int flux_ci[16];
     float flux_ms[16];
     int recover_candidates;
-    int recover_block[8];
-    float recover_ms[8];
+    int recover_block[16];      /* threads per block */
+    int recover_minblocks[16];  /* register target: resident blocks per SM (learned mode) */
+    float recover_ms[16];
     int chosen_flux_ci;
     int chosen_recover_block;
+    int chosen_recover_minblocks;
 } eu_tune_report;
 eu_status eu_autotune(eu_handle *h, int reps, eu_tune_report *report);
 
