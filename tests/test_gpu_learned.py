@@ -103,9 +103,9 @@ def test_trained_model_replaces_stiff_substeps(gpu):
     committed gate: every cell the model advances is a trapezoid substep the
     stiff kinetics does not run, and the rejected cells take the stiff
     kinetics' own substeps (the same FP64 arithmetic). The gate is tight (tau
-    calibrated for a mean species L1 of 5e-6 per step, then halved so that the
-    reaction front of an igniting validation block stays within one cell), so
-    on this block of hot reacting gas it takes about 1 % of the cells. The
+    calibrated for a mean species L1 of 5e-6 per step, then halved until the
+    reaction front of an igniting validation block does not move), so on this
+    block of hot reacting gas it takes about 2 % of the cells. The
     species error (mean over cells of sum_s |dY_s| against the stiff step)
     stays within 1e-4."""
     import learned

@@ -187,11 +187,13 @@ def test_mixed_stiff_heavy_cells_match_fp64(gpu):
     assert l1.mean() <= 1e-4 and terr.max() <= 1e-4, (l1.mean(), l1.max(), terr.max(), peak)
 
 
-@pytest.mark.parametrize("precision,arith", [("mixed", "fast"), ("fp64", "strict")])
-def test_autotuned_launch_shapes_change_no_bits(gpu, precision, arith):
+@pytest.mark.parametrize("precision,arith,chemistry", [("mixed", "fast", "stiff"), ("fp64", "strict", "stiff"),
+                                                        ("mixed", "fast", "learned")])
+def test_autotuned_launch_shapes_change_no_bits(gpu, precision, arith, chemistry):
     """Every launch shape the autotuner may pick gives bitwise the same state:
     steps after tuning equal steps with the default shapes, and tuning leaves
-    the state it timed on unchanged (ragged grid: 40 x 21 x 45 nodes)."""
+    the state it timed on unchanged (ragged grid: 40 x 21 x 45 nodes). In
+    learned mode the tuner also picks the recovery's register target."""
     ni, nj, nk = 40, 21, 45
     ext = (0.0, 0.02, 0.0, 0.01, 0.0, 0.012)
     x, y, z = (cases.node_coordinates(n, a, b) for n, a, b in ((ni, 0, 0.02), (nj, 0, 0.01), (nk, 0, 0.012)))
@@ -199,14 +201,19 @@ def test_autotuned_launch_shapes_change_no_bits(gpu, precision, arith):
     prim = cases.shock_bubble(x, y, z, mech["mw"], mech["ns"], radius=3e-3, shock_x=3e-3, standoff=5e-3, seed=5)
     out = []
     for tune in (False, True):
-        s = gpu.Solver(ni, nj, nk, ext, precision=precision, arith=arith)
+        s = gpu.Solver(ni, nj, nk, ext, precision=precision, arith=arith, chemistry=chemistry)
         s.set_mechanism(mech)
         s.set_primitive(*prim)
+        if chemistry == "learned":
+            import learned
+            model, gate = learned.load()
+            learned.attach(s, model, gate)
         s.step(1, 2e-8)
         before = s.get("CS")
         if tune:
             rep = s.autotune(reps=2)
             assert len(rep["flux_ms"]) >= 5 and rep["flux_ci"] in rep["flux_ms"], rep
+            assert len(rep["recover_ms"]) == (12 if chemistry == "learned" else 3), rep
             assert n_unequal(s.get("CS"), before) == 0
         s.step(4, 2e-8)
         out.append((s.get("CS"), s.get("T")))
