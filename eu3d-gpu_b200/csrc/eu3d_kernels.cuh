@@ -234,19 +234,30 @@ __global__ void __launch_bounds__(kFluxTK *kFluxTJ, 1)
 // from HBM once per plane instead of once per stencil point, and the loads of
 // the next plane overlapped with the current plane's arithmetic.
 //
-// A block owns a kTileJ x kTileK tile of (j, k) columns and marches along x.
-// Each thread keeps its column's x-stencil (planes i-1 .. i+2 of every
-// primitive) in registers and loads plane i+3 one node ahead. Plane i of the
-// tile plus a two-node halo in j and k is staged in shared memory, from which
-// the y- and z-face fluxes are formed; two stages alternate, and while plane i
-// is computed the halo of plane i+1 (cp.async) and the conserved values of
-// plane i (cp.async, read by the update) are in flight. Face indices: sG[q][r]
-// is the y face below tile row r (r = kTileJ: above the last row), sQ[q][r][c]
-// the z face left of column c. Partial tiles: the faces of the valid
-// rows/columns are formed, including the one past the last valid row/column.
-constexpr int kTileK = 32, kTileJ = 8;
+// A block owns a kTileJ x kTileK tile of (j, k) columns and marches along x
+// with kTileJ + 1 warps. Warps 0 .. kTileJ-1 own a row of cells each: every
+// thread keeps its column's x-stencil (planes i-1 .. i+2 of every primitive) in
+// registers and loads plane i+3 one node ahead. Plane i of the tile plus a
+// two-node halo in j and k is staged in shared memory, from which the y- and
+// z-face fluxes are formed; two stages alternate, and while plane i is computed
+// the halo of plane i+1 (cp.async) and the conserved values of plane i
+// (cp.async, read by the update) are in flight. Face indices: sG[q][r] is the y
+// face below tile row r (r = kTileJ: above the last row), sQ[q][r][c] the z
+// face left of column c.
+//
+// Each cell warp forms three faces per plane (x, y, z). The edge warp (warp
+// kTileJ) owns the first halo row above the tile, which it stages from its
+// registers, and forms the two faces a full tile has beyond its cells: the y
+// faces above the last row and the z faces right of the last column. No warp
+// forms a fourth face, so no warp waits at the plane's barrier for another's
+// extra face. Partial tiles: the faces of the valid rows/columns are formed,
+// including the one past the last valid row/column.
+constexpr int kTileK = 32, kTileJ = 7, kTileWarps = kTileJ + 1;
 constexpr int kTileRows = kTileJ + 4, kTileCols = kTileK + 4;
-constexpr int kTileHalo = 4 * kTileCols + 4 * kTileJ; // two rows above, two below, two columns each side
+// staged by cp.async: rows 0, 1 and kTileJ + 3 over the full width, and the
+// two columns each side of rows 2 .. kTileJ + 2 (the cell rows and the edge
+// warp's row)
+constexpr int kTileHalo = 3 * kTileCols + 4 * (kTileJ + 1);
 
 template <int NS, typename R>
 constexpr size_t tiled_flux_smem_bytes()
@@ -270,7 +281,7 @@ __device__ __forceinline__ void window_face_flux(const R (&w)[4][7 + NS], R (&F)
 }
 
 template <int NS, typename R, bool kStrict>
-__global__ void __launch_bounds__(kTileK *kTileJ, 2)
+__global__ void __launch_bounds__(kTileK *kTileWarps, 2)
     k_flux_update_tiled(const DevGrid g, const DevState st, const R *__restrict__ prim, const double *__restrict__ dt_dev,
                         int ci)
 {
@@ -290,23 +301,27 @@ __global__ void __launch_bounds__(kTileK *kTileJ, 2)
     const int rows = min(kTileJ, g.nj - j0), cols = min(kTileK, g.nk - k0); // valid rows / columns
     const bool valid = ty < rows && tx < cols;
     const bool resident = j < g.ny && k < g.nz; // inside the haloed arrays: staged for the neighbours
-    // faces this thread forms (see above)
+    // faces this thread forms (see above); the y face above a full tile's
+    // last row is the edge warp's (ty == rows == kTileJ)
     const bool yface = tx < cols && ty <= rows;
-    const bool ytop = ty == 0 && tx < cols && rows == kTileJ;
     const bool zface = ty < rows && tx <= cols;
-    const int zrow = tx; // lanes 0..kTileJ-1 of warp 1: the z face right of the last column
-    const bool zright = ty == 1 && zrow < rows && cols == kTileK;
+    const int zrow = tx; // lanes 0..kTileJ-1 of the edge warp: the z face right of the last column
+    const bool zright = ty == kTileJ && zrow < rows && cols == kTileK;
 
-    // the halo cell this thread stages, if any
+    // the halo cell this thread stages, if any (counted from the last thread,
+    // so the edge warp, which forms fewer faces, takes the first share)
     int hr = -1, hc = 0;
-    if (tid < 4 * kTileCols) {
-        const int band = tid / kTileCols;
-        hr = band < 2 ? band : kTileJ + band;
-        hc = tid % kTileCols;
-    } else if (tid < kTileHalo) {
-        const int h = tid - 4 * kTileCols, side = h % 4;
-        hr = 2 + h / 4;
-        hc = side < 2 ? side : kTileK + side;
+    {
+        const int h = kTileWarps * kTileK - 1 - tid;
+        if (h < 3 * kTileCols) {
+            const int band = h / kTileCols;
+            hr = band < 2 ? band : kTileJ + 3;
+            hc = h % kTileCols;
+        } else if (h < kTileHalo) {
+            const int e = h - 3 * kTileCols, side = e % 4;
+            hr = 2 + e / 4;
+            hc = side < 2 ? side : kTileK + side;
+        }
     }
     const int hj = g.bc + j0 - 2 + hr, hk = g.bc + k0 - 2 + hc;
     const bool halo = hr >= 0 && hj < g.ny && hk < g.nz;
@@ -380,12 +395,6 @@ __global__ void __launch_bounds__(kTileK *kTileJ, 2)
             tile_face_flux<NS, 1, 1, 0, R, kStrict>(stage[s], ty, tx + 2, G);
 #pragma unroll
             for (int q = 0; q < NV; ++q) sG[q][ty][tx] = G[q];
-        }
-        if (ytop) {
-            R G[NV];
-            tile_face_flux<NS, 1, 1, 0, R, kStrict>(stage[s], kTileJ, tx + 2, G);
-#pragma unroll
-            for (int q = 0; q < NV; ++q) sG[q][kTileJ][tx] = G[q];
         }
         if (zface) {
             R Q[NV];

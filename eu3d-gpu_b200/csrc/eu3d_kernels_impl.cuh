@@ -61,7 +61,7 @@ cudaError_t tiled_flux_launch(const LaunchArgs &a, const R *prim)
             return e;
         configured = true;
     }
-    const dim3 block(kTileK, kTileJ);
+    const dim3 block(kTileK, kTileWarps);
     const int ci = a.flux_ci > 0 ? a.flux_ci : 16;
     const dim3 grid((g.nk + kTileK - 1) / kTileK, (g.nj + kTileJ - 1) / kTileJ, (g.ni + ci - 1) / ci);
     k_flux_update_tiled<NS, R, kStrict><<<grid, block, smem, a.stream>>>(g, a.st, prim, a.dt_dev, ci);
