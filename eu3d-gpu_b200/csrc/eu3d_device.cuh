@@ -201,6 +201,11 @@ __device__ __forceinline__ double newton_temperature(const DevMech &m, double T,
     }
     return T_temp;
 }
+
+// The exact forms keep no thermo sums between recovery and the primitives.
+template <int NS>
+struct ThermoCache {
+};
 #else
 // Mixture polynomial of one NASA range: c_k = sum_s Y_s R_s a_k,s, with the
 // enthalpy's divisors folded in (h/R uses a_k T^(k-1)/(k-1) for k >= 3).
@@ -254,15 +259,26 @@ __device__ __forceinline__ void mix_poly(const DevMech &m, const double (&Y)[NS]
     c.h6 = a[6] * 0.2;
 }
 
+// The mixture polynomial of the Newton's last iterate and its range: the
+// primitives that follow the recovery (cp for Gamma) reuse it when the final
+// temperature lies in the same range (the same sums, so the same values).
 template <int NS>
-__device__ __forceinline__ double newton_temperature(const DevMech &m, double T, double E, const double (&Y)[NS])
+struct ThermoCache {
+    MixPoly<NS> c;
+    bool low;
+};
+
+template <int NS>
+__device__ __forceinline__ double newton_temperature(const DevMech &m, double T, double E, const double (&Y)[NS],
+                                                     ThermoCache<NS> &tc)
 {
     double rsum = 0;
 #pragma unroll
     for (int s = 0; s < NS; ++s) rsum += Y[s] * m.ri[s];
     const double e_scaled = E * 1e-3;
-    bool low = T < kThermoSwitch;
-    MixPoly<NS> c;
+    bool &low = tc.low;
+    MixPoly<NS> &c = tc.c;
+    low = T < kThermoSwitch;
     mix_poly<NS>(m, Y, low, c);
     double T_temp = T;
     for (int count = 0; count < 10; ++count) {
@@ -285,6 +301,13 @@ __device__ __forceinline__ double newton_temperature(const DevMech &m, double T,
     }
     return T_temp;
 }
+
+template <int NS>
+__device__ __forceinline__ double newton_temperature(const DevMech &m, double T, double E, const double (&Y)[NS])
+{
+    ThermoCache<NS> tc;
+    return newton_temperature<NS>(m, T, E, Y, tc);
+}
 #endif
 
 // Per-cell flow state kept in registers by the recovery / kinetics kernel.
@@ -299,7 +322,7 @@ struct CellState {
 // cell, up to the point where P, H, Gamma are needed (those are formed by
 // finish_primitives when the cell's primitives are written).
 template <int NS>
-__device__ __forceinline__ void recover_state(const DevMech &m, CellState<NS> &c)
+__device__ __forceinline__ void recover_state(const DevMech &m, CellState<NS> &c, ThermoCache<NS> &tcache)
 {
     double D = 0;
 #pragma unroll
@@ -319,7 +342,7 @@ __device__ __forceinline__ void recover_state(const DevMech &m, CellState<NS> &c
 #pragma unroll
     for (int s = 0; s < NS; ++s) c.Y[s] = c.cs[s] * invD;
     c.D = D;
-    c.T = newton_temperature<NS>(m, c.T, c.E, c.Y);
+    c.T = newton_temperature<NS>(m, c.T, c.E, c.Y, tcache);
     c.U = c.cs[NS + 0] * invD;
     c.V = c.cs[NS + 1] * invD;
     c.W = c.cs[NS + 2] * invD;
@@ -327,10 +350,18 @@ __device__ __forceinline__ void recover_state(const DevMech &m, CellState<NS> &c
 #endif
 }
 
-// P, H, Gamma of Update_after_CS (src/Flowfield.cpp:1606-1614).
 template <int NS>
-__device__ __forceinline__ void finish_primitives(const DevMech &m, const CellState<NS> &c, double &P, double &H,
-                                                  double &G)
+__device__ __forceinline__ void recover_state(const DevMech &m, CellState<NS> &c)
+{
+    ThermoCache<NS> tcache;
+    recover_state<NS>(m, c, tcache);
+}
+
+// P, H, Gamma of Update_after_CS (src/Flowfield.cpp:1606-1614). tcache: the
+// recovery's thermo sums for this state, or null.
+template <int NS>
+__device__ __forceinline__ void finish_primitives(const DevMech &m, const CellState<NS> &c,
+                                                  const ThermoCache<NS> *tcache, double &P, double &H, double &G)
 {
 #ifdef EU_EXACT_CHEM
     double inv_w = 0;
@@ -358,13 +389,24 @@ __device__ __forceinline__ void finish_primitives(const DevMech &m, const CellSt
     P = c.T * c.D * Rgas;
     H = c.T * Rgas + c.E;
     MixPoly<NS> mp;
-    mix_poly<NS>(m, c.Y, c.T < kThermoSwitch, mp);
+    const bool low = c.T < kThermoSwitch;
+    if (tcache && tcache->low == low)
+        mp = tcache->c;
+    else
+        mix_poly<NS>(m, c.Y, low, mp);
     const double T0 = c.T, inv = rcp_nr(T0);
     const double cp = fma(T0, fma(T0, fma(T0, fma(T0, mp.a6, mp.a5), mp.a4), mp.a3), mp.a2) +
                       inv * fma(mp.a0, inv, mp.a1);
     const double Cp = cp * 1000;
     G = div_fast(Cp, Cp - Rgas);
 #endif
+}
+
+template <int NS>
+__device__ __forceinline__ void finish_primitives(const DevMech &m, const CellState<NS> &c, double &P, double &H,
+                                                  double &G)
+{
+    finish_primitives<NS>(m, c, static_cast<const ThermoCache<NS> *>(nullptr), P, H, G);
 }
 
 // ------------------------------------------------------------- kinetics

@@ -451,12 +451,13 @@ __global__ void __launch_bounds__(kTileK *kTileWarps, 2)
 
 // kWriteCs false: the conserved planes are unchanged (recovery alone reads
 // them and changes nothing there), so they are not written back.
+// tcache: the recovery's thermo sums for this state, or null.
 template <int NS, bool kWriteCs = true>
 __device__ __forceinline__ void store_cell(const DevMech &m, const DevState &st, long long n3, long long c,
-                                           const CellState<NS> &cell)
+                                           const CellState<NS> &cell, const ThermoCache<NS> *tcache = nullptr)
 {
     double P, H, G;
-    finish_primitives<NS>(m, cell, P, H, G);
+    finish_primitives<NS>(m, cell, tcache, P, H, G);
     const double v[7] = {P, cell.D, cell.U, cell.V, cell.W, H, G};
     if (st.prim32) { // mixed precision: the FP64 planes are formed on demand (k_materialize)
 #pragma unroll
@@ -702,6 +703,12 @@ __global__ void __launch_bounds__(128) k_recover_react(const __grid_constant__ D
     const long long c = cell_index(g, i, j, k);
     CellState<NS> cell;
     load_cell<NS>(st, n3, c, cell);
+    if (!kReact) {
+        ThermoCache<NS> tcache;
+        recover_state<NS>(m, cell, tcache);
+        store_cell<NS, false>(m, st, n3, c, cell, &tcache);
+        return;
+    }
     recover_state<NS>(m, cell);
     if (kReact) {
         if (!react_or_defer<NS, Rt>(m, st, n3, c, cell, *dt_dev, max_substeps)) {
@@ -734,8 +741,9 @@ __global__ void __launch_bounds__(128, MINB) k_recover_classify(const __grid_con
         c = cell_index(g, i, j, k);
         CellState<NS> cell;
         load_cell<NS>(st, n3, c, cell);
-        recover_state<NS>(m, cell);
-        store_cell<NS, false>(m, st, n3, c, cell);
+        ThermoCache<NS> tcache;
+        recover_state<NS>(m, cell, tcache);
+        store_cell<NS, false>(m, st, n3, c, cell, &tcache);
         double reactive = 0, radical = 0;
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
