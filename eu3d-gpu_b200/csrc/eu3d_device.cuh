@@ -630,6 +630,11 @@ __device__ __forceinline__ R muscl_slope(R a, R A1)
         const R L = A1 / (a + R(1e-12));
         const R L1 = minmod(L), L2 = minmod(R(1.0) / L);
         return R(0.25) * ((R(1.0) - kk) * L1 + (R(1) + kk) * L2 * L) * a;
+    } else if constexpr (std::is_same<R, float>::value) {
+        // min(max(L, 0), 1) is the saturation of the product that forms L
+        // (NaN saturates to 0, as L > 0 fails for it)
+        const R L = __saturatef(div_fast(A1, a + R(1e-12)));
+        return R(0.5) * a * L;
     } else {
         const R L = div_fast(A1, a + R(1e-12));
         return L > R(0) ? R(0.5) * a * fmin(L, R(1)) : R(0);

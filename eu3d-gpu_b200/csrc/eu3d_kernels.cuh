@@ -726,7 +726,7 @@ __global__ void __launch_bounds__(128) k_recover_react(const __grid_constant__ D
 // final. Every cell's recovered state is stored.
 // MINB: resident blocks per SM the register allocation aims at (the
 // autotuner picks the instantiation; fewer registers, more warps, some spills).
-template <int NS, int MINB = 5>
+template <int NS, int MINB = 4>
 __global__ void __launch_bounds__(128, MINB) k_recover_classify(const __grid_constant__ DevMech m, const DevGrid g,
                                                           const DevState st, LearnedParams lp)
 {
@@ -885,6 +885,8 @@ __global__ void __launch_bounds__(128) k_react_queue(const __grid_constant__ Dev
     // A fixed grid drains the queue (its length is read on the device): each
     // warp takes the next 32 cells from count[1] (reset before the launch).
     const int nq = *(volatile int *)count;
+    if (nq == 0) // an empty queue: no warp touches the shared counter
+        return;
     const int lane = threadIdx.x & 31;
     int *next = count + 1;
     for (;;) {

@@ -123,10 +123,10 @@ cudaError_t classify_t(const LaunchArgs &a, const LearnedParams &lp)
     const int threads = a.recover_block > 0 ? a.recover_block : 128;
     const dim3 grid(unsigned((n + threads - 1) / threads));
     switch (a.recover_minb) {
-    case 4: k_recover_classify<NS, 4><<<grid, threads, 0, a.stream>>>(*a.mech, a.g, a.st, lp); break;
-    case 6: k_recover_classify<NS, 6><<<grid, threads, 0, a.stream>>>(*a.mech, a.g, a.st, lp); break;
     case 3: k_recover_classify<NS, 3><<<grid, threads, 0, a.stream>>>(*a.mech, a.g, a.st, lp); break;
-    default: k_recover_classify<NS, 5><<<grid, threads, 0, a.stream>>>(*a.mech, a.g, a.st, lp); break;
+    case 5: k_recover_classify<NS, 5><<<grid, threads, 0, a.stream>>>(*a.mech, a.g, a.st, lp); break;
+    case 6: k_recover_classify<NS, 6><<<grid, threads, 0, a.stream>>>(*a.mech, a.g, a.st, lp); break;
+    default: k_recover_classify<NS, 4><<<grid, threads, 0, a.stream>>>(*a.mech, a.g, a.st, lp); break;
     }
     return cudaGetLastError();
 }

@@ -21,7 +21,7 @@ struct LaunchArgs {
     int sms;       // multiprocessors of the device (fixed grids of the queue kernels)
     int flux_ci;   // nodes each flux block marches along x (autotuned; 0: 16)
     int recover_block; // threads per block of the recovery kernels, 32..128 (autotuned; 0: 128)
-    int recover_minb;  // register target of the learned-mode recovery: 3, 4, 5 or 6 blocks per SM (0: 5)
+    int recover_minb;  // register target of the learned-mode recovery: 3, 4, 5 or 6 blocks per SM (0: 4)
     cudaStream_t stream;
 };
 

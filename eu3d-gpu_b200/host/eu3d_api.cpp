@@ -1578,8 +1578,8 @@ eu_status eu_autotune(eu_handle *h, int reps, eu_tune_report *report)
     };
     restore();
     best = 1e30f;
-    int best_minb = 5;
-    const int minb_learned[] = {3, 4, 5, 6}, minb_other[] = {5};
+    int best_minb = 4;
+    const int minb_learned[] = {3, 4, 5, 6}, minb_other[] = {4};
     const int *minbs = learned ? minb_learned : minb_other;
     const int n_minb = learned ? 4 : 1;
     for (int rb : rb_cand)
