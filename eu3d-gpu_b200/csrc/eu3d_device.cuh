@@ -658,8 +658,17 @@ __device__ __forceinline__ R muscl_upwind(bool up, R fm1, R f0, R f1, R f2)
 {
     const R A1 = f1 - f0;
     const R a = up ? f0 - fm1 : f2 - f1;
-    const R t = muscl_slope<R, kStrict>(a, A1);
-    return up ? f0 + t : f1 - t;
+    if constexpr (!kStrict && std::is_same<R, float>::value) {
+        // f0 + (a/2) L or f1 - (a/2) L as one fused multiply-add on the
+        // selected base: the product's sign is exact, so the value is that of
+        // either side's own fused form
+        const R L = __saturatef(div_fast(A1, a + R(1e-12)));
+        const R h = (up ? R(0.5) : R(-0.5)) * a;
+        return fmaf(h, L, up ? f0 : f1);
+    } else {
+        const R t = muscl_slope<R, kStrict>(a, A1);
+        return up ? f0 + t : f1 - t;
+    }
 }
 
 // MUSCL reconstruction and AUSM+ flux of one face (src/Flowfield.cpp:1794-1930)

@@ -267,11 +267,14 @@ constexpr size_t tiled_flux_smem_bytes()
 }
 
 // Face flux from four consecutive stencil points of the staged plane tile,
-// starting at (r, c) and stepping (DR, DC).
-template <int NS, int DIR, int DR, int DC, typename R, bool kStrict>
-__device__ __forceinline__ void tile_face_flux(const R (*sP)[kTileRows][kTileCols], int r, int c, R (&F)[NS + 4])
+// starting at (r, c) and stepping (DR, DC). own: the values of stencil point 2
+// when that point is the thread's own node (kept in registers), else null.
+template <int NS, int DIR, int DR, int DC, typename R, bool kStrict, bool kOwn>
+__device__ __forceinline__ void tile_face_flux(const R (*sP)[kTileRows][kTileCols], int r, int c, const R *own,
+                                               R (&F)[NS + 4])
 {
-    face_ausm<NS, DIR, R, kStrict, R>([&](int f, int p) { return sP[f][r + p * DR][c + p * DC]; }, F);
+    face_ausm<NS, DIR, R, kStrict, R>(
+        [&](int f, int p) { return (kOwn && p == 2) ? own[f] : sP[f][r + p * DR][c + p * DC]; }, F);
 }
 
 template <int NS, typename R, bool kStrict>
@@ -392,19 +395,19 @@ __global__ void __launch_bounds__(kTileK *kTileWarps, 2)
             window_face_flux<NS, R, kStrict>(w, Fp);
         if (yface) {
             R G[NV];
-            tile_face_flux<NS, 1, 1, 0, R, kStrict>(stage[s], ty, tx + 2, G);
+            tile_face_flux<NS, 1, 1, 0, R, kStrict, true>(stage[s], ty, tx + 2, w[1], G);
 #pragma unroll
             for (int q = 0; q < NV; ++q) sG[q][ty][tx] = G[q];
         }
         if (zface) {
             R Q[NV];
-            tile_face_flux<NS, 2, 0, 1, R, kStrict>(stage[s], ty + 2, tx, Q);
+            tile_face_flux<NS, 2, 0, 1, R, kStrict, true>(stage[s], ty + 2, tx, w[1], Q);
 #pragma unroll
             for (int q = 0; q < NV; ++q) sQ[q][ty][tx] = Q[q];
         }
         if (zright) {
             R Q[NV];
-            tile_face_flux<NS, 2, 0, 1, R, kStrict>(stage[s], zrow + 2, kTileK, Q);
+            tile_face_flux<NS, 2, 0, 1, R, kStrict, false>(stage[s], zrow + 2, kTileK, nullptr, Q);
 #pragma unroll
             for (int q = 0; q < NV; ++q) sQ[q][zrow][kTileK] = Q[q];
         }
