@@ -14,8 +14,11 @@ inversion, Nchem prediction and the adaptive trapezoid kinetics.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One JSON line on rank 0 (see the keys below). Multi-GPU runs (torchrun, one
-rank per GPU) advance independent replicas of the workload: the timestep has
-no exchange between instances, so per-GPU work is fixed ("scaling": "weak").
+rank per GPU) decompose one grid along x, one block of 256 x 128 x 128 nodes
+per rank (the reference's MPI layout: neighbouring blocks share a node, so N
+ranks hold N x 255 + 1 nodes along x over N x 64 mm): every step exchanges the
+blocks' halo planes over NCCL before it runs, dt is the minimum of the blocks'
+CFL steps, and per-GPU work is fixed ("scaling": "weak").
 """
 from __future__ import annotations
 
@@ -468,9 +471,160 @@ def batch_instances(args, model, gate, local, mech, count=32):
             "seed": 5, "unit": "Mcell-steps/s"}
 
 
+def our_arm_blocks(args, world, rank, local, dist):
+    """The workload decomposed along x over the ranks (eu3d-gpu_b200/slab.py),
+    one 256 x 128 x 128-node block per GPU, halo planes exchanged over NCCL
+    every step. The single-GPU side studies (reacting block, batch, ZND, model
+    roofline, CPU baseline) are N = 1 measurements and are not repeated."""
+    import torch
+    import slab
+    device = f"cuda:{local}"
+    ni, nj, nk = args.grid
+    total_ni = world * (ni - 1) + 1
+    ext = (EXTENT[0], EXTENT[0] + (EXTENT[1] - EXTENT[0]) * (total_ni - 1) / (ni - 1), *EXTENT[2:])
+    x = cases.node_coordinates(total_ni, ext[0], ext[1], blocks=world, block=rank)
+    y = cases.node_coordinates(nj, ext[2], ext[3])
+    z = cases.node_coordinates(nk, ext[4], ext[5])
+    mech = eu3d.parse_mechanism(cases.MECH_JA919, cases.THERMO)
+    prim = cases.shock_bubble(x, y, z, mech["mw"], mech["ns"], seed=3)
+    p, cs, T, E = eu3d.initial_state(mech, ni, nj, nk, *prim)
+    sd = state_dict((p, cs, T, E))
+    ncell = ni * nj * nk
+    # dt: the reference's CFL rule at 0.5, minimum over the blocks
+    dt_t = torch.tensor([cases.cfl_dt(x, y, p[0], p[1], p[2], p[3], p[6], CFL)], dtype=torch.float64, device=device)
+    dist.all_reduce(dt_t, op=dist.ReduceOp.MIN)
+    dt = float(dt_t.item())
+    model = gate = None
+    if args.chem == "learned":
+        import learned
+        model, gate = learned.load(device=local)
+
+    def make(chem, precision, arith, profile=False, state=sd):
+        s = slab.SlabSolver(dist, total_ni, nj, nk, ext, device=local, precision=precision, chemistry=chem,
+                            arith=arith, profile=profile)
+        s.set_mechanism(mech)
+        s.set_state(state)
+        if chem == "learned":
+            import learned
+            learned.attach(s.solver, model, gate)
+        return s
+
+    def timed(s, clocks=False):
+        """Device time of args.steps exchanged steps (events on the handle's
+        stream), max over ranks, and the last step's statistics."""
+        s.step(args.warmup, dt, stats=False)
+        s.sync()
+        barrier(dist, device)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clk = ClockSampler(torch.cuda.current_device()) if clocks else None
+        if clk:
+            clk.__enter__()
+        ev0.record(s.stream)
+        st = s.step(args.steps, dt, stats=True)
+        ev1.record(s.stream)
+        ev1.synchronize()
+        if clk:
+            clk.__exit__(None, None, None)
+        barrier(dist, device)
+        return st, reduce_max(dist, ev0.elapsed_time(ev1), device), (clk.summary() if clk else None)
+
+    s = make(args.chem, args.precision, args.arith)
+    tuned = s.autotune(reps=5) if not args.no_autotune else None
+    stats, ms, clocks = timed(s, clocks=True)
+    value = ncell * args.steps * world / (ms / 1e3) / 1e6
+    y_fast = s.get("Yi")
+    halo_bytes = s.halo_bytes()
+    faces = len(s.halo.faces)
+    s.close()
+
+    plain = None
+    if (args.chem, args.precision) != ("stiff", "fp64"):
+        sp_ = make("stiff", "fp64", "fast")
+        _, pms, _ = timed(sp_)
+        y_ref = sp_.get("Yi")
+        sp_.close()
+        err_all, err_reactive = species_error(y_fast, y_ref)
+        pvalue = ncell * args.steps * world / (pms / 1e3) / 1e6
+        plain = {"value": round(pvalue, 3), "ms_per_step": round(pms / args.steps, 4),
+                 "speedup": round(value / pvalue, 3), "species_l1_vs_plain": err_all,
+                 "species_l1_vs_plain_reactive_cells": err_reactive, "after_steps": args.warmup + args.steps,
+                 "note": "rank 0's block"}
+
+    # per-kernel phases of one exchanged step (CUDA events inside the library)
+    sp = make(args.chem, args.precision, args.arith, profile=True)
+    sp.step(args.warmup, dt, stats=False)
+    phase = sp.step(1, dt, stats=True)["phase_ms"]
+    sp.close()
+    names = ["ghost_fill", "flux_update", "recover_kinetics" if args.chem != "learned" else "recover_learned_chem"]
+    per_kernel = {n: round(phase[q], 4) for q, n in enumerate(names)}
+    hbm, bf16, peak_kind = measured_peaks()
+    flux_gbs = FLUX_BYTES[args.precision] * ncell / (phase[1] / 1e3) / 1e9
+    dominant = max(range(3), key=lambda q: phase[q])
+    roofline = {"kernel": "flux_update", "bound": "hbm", "achieved": round(flux_gbs, 1), "peak": hbm,
+                "unit": "GB/s", "frac": round(flux_gbs / hbm, 4),
+                "traffic": (round(FLUX_TRAFFIC_PER_CELL[args.precision] * ncell / 1e9, 4)
+                            if args.precision in FLUX_TRAFFIC_PER_CELL else None),
+                "traffic_unit": "GB per launch (ncu, scaled from 256x128x64)",
+                "algorithmic_bytes_per_cell": FLUX_BYTES[args.precision], "peak_source": f"{peak_kind} hbm_gbs",
+                "dominant_kernel": names[dominant],
+                "dominant_share": round(phase[dominant] / max(sum(phase[:3]), 1e-9), 3)}
+
+    # end to end through the public API with host buffers (state up once, the
+    # exchanged steps each synchronous, the conserved state down at the end)
+    pinned = {}
+    for k, v in sd.items():
+        t = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = v
+        pinned[k] = t.numpy()
+    cs_host = torch.empty(sd["CS"].shape, dtype=torch.float64, pin_memory=True).numpy()
+    se = make(args.chem, args.precision, args.arith, state=pinned)
+    se.step(args.warmup, dt, stats=False)
+    se.sync()
+    barrier(dist, device)
+    t0 = time.perf_counter()
+    se.set_state(pinned)
+    for _ in range(args.steps):
+        se.step(1, dt, stats=True)
+    cs_out = se.get("CS", out=cs_host)
+    e2e_s = reduce_max(dist, time.perf_counter() - t0, device)
+    e2e_value = ncell * args.steps * world / e2e_s / 1e6
+    h2d = sum(v.nbytes for v in pinned.values()) / args.steps + 8
+    d2h = cs_out.nbytes / args.steps + 96
+    se.close()
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 3), "unit": "Mcell-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": f"3-D reacting shock-bubble decomposed along x: {world} blocks of "
+                                       f"{ni}x{nj}x{nk} nodes ({total_ni}x{nj}x{nk} global over "
+                                       f"{ext[1] * 1e3:.0f}x32x32 mm), H2_JA919, Mach 2.83 in N2, seed 3",
+                           "grid": [ni, nj, nk], "global_grid": [total_ni, nj, nk], "dt": dt,
+                           "precision": args.precision, "chemistry": args.chem, "arith": args.arith,
+                           "parallelism": f"x blocks {world}, halo exchange over NCCL every step",
+                           "halo_bytes_per_face": halo_bytes, "autotune": tuned,
+                           "l2": f"inputs larger than L2: {sd['CS'].nbytes * 3 // 2**20} MiB state per GPU > 126 MiB"},
+                "plain_fp64": plain,
+                "roofline": roofline, "kernels_ms_per_step": per_kernel,
+                "max_nchem": stats["max_nchem"], "reacting_cells": stats["reacting"],
+                "learned_cells": stats["learned"], "fallback_cells": stats["fallback"],
+                "clocks": clocks,
+                "e2e": {"value": round(e2e_value, 3), "unit": "Mcell-steps/s",
+                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+                # the step's kernels plus one halo pack and unpack per neighbour face
+                "gpu_launches": (stats["launches"] + 2 * faces) * args.steps,
+                "cpu_baseline": None}
+        print(json.dumps(line), flush=True)
+    dist.destroy_process_group()
+    return 0
+
+
 def our_arm(args):
     import torch
     world, rank, local, dist = dist_setup(args)
+    if world > 1:
+        return our_arm_blocks(args, world, rank, local, dist)
     device = f"cuda:{local}"
     torch.cuda.set_device(local)
     grid = tuple(args.grid)

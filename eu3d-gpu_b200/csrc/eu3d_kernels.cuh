@@ -46,6 +46,8 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
         const int jk = fdiv(t, g.d_nk), q = fdiv(t, g.d_njnk); // q: 0 .. 2bc-1
         const int k = bc + int(t - (long long)jk * nk);
         const int j = bc + (jk - q * nj);
+        if (q < bc ? g.exch_lo : g.exch_hi) // filled by the halo exchange
+            return;
         const int i = q < bc ? q : ni + q;           // ghost index
         const int si = q < bc ? 2 * bc - 1 - i : 2 * (ni + bc) - 1 - i;
         dst = cell_index(g, i, j, k);
@@ -122,6 +124,28 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
             st.prim32[f * n3 + dst] = float(v[f]);
         else
             st.prim[f * n3 + dst] = v[f];
+    }
+}
+
+// Halo messages between x blocks (Flowfield::Mpi_Boundary, src/Flowfield.cpp:809-911):
+// plane p (0 .. bc-1) of field f of a message is node plane src_i(p) of the flux
+// primitives. to_msg: planes -> message (pack), else message -> planes (unpack).
+// Node planes: pack face 0 takes bc+1+p, pack face 1 takes ni+bc-2-p; unpack
+// face 0 fills bc-1-p, unpack face 1 fills ni+bc+p.
+template <typename R>
+__global__ void k_halo_copy(R *planes, R *msg, int nf, int bc, long long n3, long long plane, int first, int step,
+                            bool to_msg)
+{
+    const long long total = (long long)nf * bc * plane;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long fp = t / plane, e = t - fp * plane;
+        const int f = int(fp / bc), p = int(fp - (long long)f * bc);
+        R *node = planes + f * n3 + (long long)(first + step * p) * plane + e;
+        if (to_msg)
+            msg[t] = *node;
+        else
+            *node = msg[t];
     }
 }
 

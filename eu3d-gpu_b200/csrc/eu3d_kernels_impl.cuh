@@ -251,6 +251,30 @@ cudaError_t launch_cfl(const LaunchArgs &a, double cfl, unsigned long long *slot
     return cudaGetLastError();
 }
 
+// face 0: x low, 1: x high; pack: planes -> msg, else msg -> ghost planes.
+cudaError_t launch_halo(const LaunchArgs &a, int nf, int face, bool pack, void *msg)
+{
+    const DevGrid &g = a.g;
+    const long long plane = (long long)g.ny * g.nz;
+    int first, step;
+    if (pack) {
+        first = face == 0 ? g.bc + 1 : g.ni + g.bc - 2;
+        step = face == 0 ? 1 : -1;
+    } else {
+        first = face == 0 ? g.bc - 1 : g.ni + g.bc;
+        step = face == 0 ? -1 : 1;
+    }
+    const long long total = (long long)nf * g.bc * plane;
+    const unsigned blocks = unsigned(std::min<long long>((total + 255) / 256, (long long)(a.sms > 0 ? a.sms : 148) * 8));
+    if (a.st.prim32)
+        k_halo_copy<float><<<blocks, 256, 0, a.stream>>>(a.st.prim32, static_cast<float *>(msg), nf, g.bc, g.n3, plane,
+                                                       first, step, pack);
+    else
+        k_halo_copy<double><<<blocks, 256, 0, a.stream>>>(a.st.prim, static_cast<double *>(msg), nf, g.bc, g.n3, plane,
+                                                        first, step, pack);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_set_value(double *dst, double v, cudaStream_t s)
 {
     k_set_value<<<1, 1, 0, s>>>(dst, v);

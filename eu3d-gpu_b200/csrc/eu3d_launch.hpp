@@ -60,6 +60,7 @@ struct Launchers {
     cudaError_t launch_react_heavy(const LaunchArgs &a, int blocks);                               \
     cudaError_t launch_materialize(const LaunchArgs &a);                                           \
     cudaError_t launch_to_f32(const double *src, float *dst, long long n, cudaStream_t s);          \
+    cudaError_t launch_halo(const LaunchArgs &a, int nf, int face, bool pack, void *msg);           \
     extern const Launchers launchers;                                                              \
     }
 

@@ -54,6 +54,9 @@ struct DevGrid {
     // index decompositions of the kernels' flat thread indices
     FastDiv d_nk, d_njnk, d_nink, d_ghost, d_ghost_nj, d_nz, d_nynz;
     int bc_kind; // eu_boundary
+    // x faces whose ghost nodes come from a neighbouring block (halo exchange)
+    // instead of the boundary condition
+    int exch_lo, exch_hi;
 };
 
 // Primitive planes the stencils read, in this order (haloed, FP64).

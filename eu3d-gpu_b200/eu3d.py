@@ -38,7 +38,8 @@ class Config(ctypes.Structure):
     _fields_ = [("total_ni", _I), ("total_nj", _I), ("total_nk", _I),
                 ("xa", _D), ("xb", _D), ("ya", _D), ("yb", _D), ("za", _D), ("zb", _D),
                 ("bc", _I), ("device", _I), ("precision", _I), ("chemistry", _I), ("arith", _I),
-                ("max_substeps", _I), ("record_sources", _I), ("profile", _I), ("eager", _I), ("boundary", _I)]
+                ("max_substeps", _I), ("record_sources", _I), ("profile", _I), ("eager", _I), ("boundary", _I),
+                ("blocks_x", _I), ("block_x", _I)]
 
 
 class MechanismC(ctypes.Structure):
@@ -143,6 +144,13 @@ def library():
         lib.eu_batch_last_error.restype = ctypes.c_char_p
         for fn in ("eu_batch_create", "eu_batch_step", "eu_batch_destroy"):
             getattr(lib, fn).restype = _I
+        lib.eu_halo_bytes.argtypes = [_P, ctypes.POINTER(ctypes.c_size_t)]
+        lib.eu_halo_pack.argtypes = [_P, _I, _P]
+        lib.eu_halo_unpack.argtypes = [_P, _I, _P]
+        lib.eu_cfl_dt.argtypes = [_P, _D, _P]
+        lib.eu_step_dt_device.argtypes = [_P, _I, _P, ctypes.POINTER(StepStats)]
+        for fn in ("eu_halo_bytes", "eu_halo_pack", "eu_halo_unpack", "eu_cfl_dt", "eu_step_dt_device"):
+            getattr(lib, fn).restype = _I
         lib.eu_mlp_predict_fused.argtypes = [_P, _P, ctypes.c_longlong, _P]
         lib.eu_mlp_predict_fused.restype = _I
         lib.eu_mlp_predict_noalloc.restype = _I
@@ -223,17 +231,22 @@ class Solver:
     """One eu_handle: a haloed node grid, a mechanism and the device state."""
 
     def __init__(self, total_ni, total_nj, total_nk, extent, precision="fp64", chemistry="stiff", arith="strict",
-                 device=0, max_substeps=0, record_sources=False, profile=False, bc=2, graphs=True, boundary="rsbi"):
+                 device=0, max_substeps=0, record_sources=False, profile=False, bc=2, graphs=True, boundary="rsbi",
+                 blocks_x=1, block_x=0):
+        """blocks_x > 1: this handle holds x block `block_x` of the global grid
+        ((total_ni - 1) / blocks_x + 1 nodes, neighbours sharing one node)."""
         lib = library()
         self.cfg = Config(int(total_ni), int(total_nj), int(total_nk), *[float(v) for v in extent], int(bc),
                           int(device), PRECISION[precision], CHEMISTRY[chemistry], ARITH[arith], int(max_substeps),
-                          int(bool(record_sources)), int(bool(profile)), int(not graphs), BOUNDARY[boundary])
+                          int(bool(record_sources)), int(bool(profile)), int(not graphs), BOUNDARY[boundary],
+                          int(blocks_x), int(block_x))
         h = _P()
         st = lib.eu_create(ctypes.byref(self.cfg), ctypes.byref(h))
         if st:
             raise EU3DError(st, "eu_create")
         self.h = h
-        self.ni, self.nj, self.nk, self.bc = int(total_ni), int(total_nj), int(total_nk), int(bc)
+        self.ni = (int(total_ni) - 1) // max(int(blocks_x), 1) + 1
+        self.nj, self.nk, self.bc = int(total_nj), int(total_nk), int(bc)
         self.shape = (self.ni + 2 * bc, self.nj + 2 * bc, self.nk + 2 * bc)
         self.n3 = int(np.prod(self.shape))
         self.ns = None
@@ -373,6 +386,31 @@ class Solver:
         self._check(library().eu_read_state(self.h, str(path).encode(), ctypes.byref(it), ctypes.byref(num),
                                             ctypes.byref(t), ctypes.byref(dt)), "read_state")
         return it.value, num.value, t.value, dt.value
+
+    def halo_bytes(self):
+        """Bytes of one halo message (eu_halo_bytes)."""
+        n = ctypes.c_size_t()
+        self._check(library().eu_halo_bytes(self.h, ctypes.byref(n)), "halo_bytes")
+        return n.value
+
+    def halo_pack(self, face, device_ptr):
+        """Queue the face's outgoing message into device memory (eu_halo_pack)."""
+        self._check(library().eu_halo_pack(self.h, int(face), _P(device_ptr)), "halo_pack")
+
+    def halo_unpack(self, face, device_ptr):
+        """Queue the neighbour's message into the face's ghost planes (eu_halo_unpack)."""
+        self._check(library().eu_halo_unpack(self.h, int(face), _P(device_ptr)), "halo_unpack")
+
+    def cfl_dt(self, cfl, device_ptr):
+        """Queue this block's CFL dt into device memory (eu_cfl_dt)."""
+        self._check(library().eu_cfl_dt(self.h, float(cfl), _P(device_ptr)), "cfl_dt")
+
+    def step_dt_device(self, nsteps, device_ptr, stats=True):
+        """eu_step with dt read from device memory."""
+        s = StepStats()
+        self._check(library().eu_step_dt_device(self.h, int(nsteps), _P(device_ptr), ctypes.byref(s) if stats else None),
+                    "step_dt_device")
+        return s.as_dict() if stats else None
 
     def device_info(self):
         stream = _P()

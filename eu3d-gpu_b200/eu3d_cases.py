@@ -40,12 +40,16 @@ INPUT_ZND = os.path.join(DATA, "input-1dZND.txt")
 S_H2O, S_O2, S_H2, S_N2 = 2, 4, 5, 8
 
 
-def node_coordinates(n, a, b, bc=2):
-    """src/Mesh.cpp:96-142 for one block (ghosts mirrored about the end nodes)."""
-    d = (b - a) / (n - 1)
+def node_coordinates(total_n, a, b, bc=2, blocks=1, block=0):
+    """Node coordinates with ghosts of block `block` of `blocks` along one axis:
+    Mesh::Initial (src/Mesh.cpp:96-119) gives the block (total_n - 1) / blocks + 1
+    nodes at the global spacing, Mesh::Boundary (:131-142) mirrors the ghosts
+    about the block's end nodes."""
+    n = (total_n - 1) // blocks + 1
+    d = (b - a) / (total_n - 1)
     x = np.zeros(n + 2 * bc)
     for i in range(bc, n + bc):
-        x[i] = a + (0 * (n - 1) + i - bc) * d
+        x[i] = a + (block * (n - 1) + i - bc) * d
     for i in range(bc):
         x[i] = 2 * x[bc] - x[2 * bc - i]
         x[n + bc + i] = 2 * x[n + bc - 1] - x[n + bc - 1 - i - 1]

@@ -386,14 +386,22 @@ eu_status eu_create(const eu_config *cfg, eu_handle **out)
     *out = nullptr;
     if (cfg->bc != 2 || cfg->total_ni < 2 || cfg->total_nj < 2 || cfg->total_nk < 2)
         return EU_ERR_INVALID_ARGUMENT;
-    // the kernels' flat node indices stay below 2^31
-    if ((long long)(cfg->total_ni + 4) * (cfg->total_nj + 4) * (cfg->total_nk + 4) >= (1LL << 31))
-        return EU_ERR_INVALID_ARGUMENT;
     if (cfg->precision != EU_PREC_FP64 && cfg->precision != EU_PREC_MIXED)
         return EU_ERR_INVALID_ARGUMENT;
     if (cfg->chemistry != EU_CHEM_STIFF && cfg->chemistry != EU_CHEM_FROZEN && cfg->chemistry != EU_CHEM_LEARNED)
         return EU_ERR_INVALID_ARGUMENT;
     if (cfg->boundary != EU_BC_RSBI && cfg->boundary != EU_BC_ZND)
+        return EU_ERR_INVALID_ARGUMENT;
+    // x blocks: the reference's layout rule (src/Mesh.cpp:64-75) and at least
+    // bc + 2 nodes per block (a message reaches node 2 bc)
+    const int blocks_x = cfg->blocks_x > 1 ? cfg->blocks_x : 1;
+    if (blocks_x > 1 && ((cfg->total_ni - 1) % blocks_x != 0 || cfg->block_x < 0 || cfg->block_x >= blocks_x ||
+                         (cfg->total_ni - 1) / blocks_x + 1 < 2 * cfg->bc + 1))
+        return EU_ERR_INVALID_ARGUMENT;
+    if (blocks_x == 1 && cfg->block_x != 0)
+        return EU_ERR_INVALID_ARGUMENT;
+    // the kernels' flat node indices stay below 2^31
+    if ((long long)((cfg->total_ni - 1) / blocks_x + 1 + 4) * (cfg->total_nj + 4) * (cfg->total_nk + 4) >= (1LL << 31))
         return EU_ERR_INVALID_ARGUMENT;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -408,7 +416,7 @@ eu_status eu_create(const eu_config *cfg, eu_handle **out)
         delete h;
         return EU_ERR_CUDA;
     }
-    h->ni = cfg->total_ni;
+    h->ni = (cfg->total_ni - 1) / blocks_x + 1;
     h->nj = cfg->total_nj;
     h->nk = cfg->total_nk;
     h->bc = cfg->bc;
@@ -416,7 +424,7 @@ eu_status eu_create(const eu_config *cfg, eu_handle **out)
     h->ny = h->nj + 2 * h->bc;
     h->nz = h->nk + 2 * h->bc;
     h->n3 = (long long)h->nx * h->ny * h->nz;
-    h->x = node_coordinates(h->ni, cfg->xa, cfg->xb, h->bc);
+    h->x = node_coordinates(cfg->total_ni, cfg->xa, cfg->xb, h->bc, blocks_x, cfg->block_x);
     h->y = node_coordinates(h->nj, cfg->ya, cfg->yb, h->bc);
     h->z = node_coordinates(h->nk, cfg->za, cfg->zb, h->bc);
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -475,6 +483,8 @@ eu_status eu_create(const eu_config *cfg, eu_handle **out)
     h->g.d_nz = make_fastdiv(unsigned(h->nz));
     h->g.d_nynz = make_fastdiv(unsigned(h->ny) * unsigned(h->nz));
     h->g.bc_kind = cfg->boundary;
+    h->g.exch_lo = blocks_x > 1 && cfg->block_x > 0;
+    h->g.exch_hi = blocks_x > 1 && cfg->block_x < blocks_x - 1;
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tuned.find(tune_key(h));
@@ -911,7 +921,8 @@ eu_status eu_set_learned(eu_handle *h, eu_mlp *model, const eu_learned_config *l
 namespace {
 // nsteps timesteps: with cfl == 0 of the fixed dt, else each of dt = cfl x the
 // CFL minimum of its own starting state (the time advanced goes to *time).
-eu_status step_impl(eu_handle *h, int nsteps, double dt, double cfl, eu_step_stats *stats, double *time);
+eu_status step_impl(eu_handle *h, int nsteps, double dt, double cfl, eu_step_stats *stats, double *time,
+                    const double *dt_src = nullptr);
 } // namespace
 
 eu_status eu_step(eu_handle *h, int nsteps, double dt, eu_step_stats *stats)
@@ -932,8 +943,68 @@ eu_status eu_step_cfl(eu_handle *h, int nsteps, double cfl, eu_step_stats *stats
     return step_impl(h, nsteps, 0.0, cfl, stats, time_advanced);
 }
 
+eu_status eu_step_dt_device(eu_handle *h, int nsteps, const double *device_dt, eu_step_stats *stats)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (nsteps < 0 || !device_dt)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "nsteps must be >= 0 and device_dt non-null");
+    return step_impl(h, nsteps, 0.0, 0.0, stats, nullptr, device_dt);
+}
+
+eu_status eu_cfl_dt(eu_handle *h, double cfl, double *device_dt)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!device_dt || !(cfl > 0) || !(cfl <= 10))
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "device_dt must be non-null and 0 < cfl <= 10");
+    if (!h->has_mech || !h->has_state)
+        return fail(h, EU_ERR_NOT_READY, "mechanism and state must be set first");
+    cudaSetDevice(h->cfg.device);
+    const LaunchArgs a = launch_args(h);
+    // the reduction leaves dt in the handle's slot; d_time is scratch here
+    CK(h, strict::launch_cfl(a, cfl, h->d_cfl_slot, h->d_time));
+    CK(h, cudaMemcpyAsync(device_dt, h->d_dt, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    return EU_OK;
+}
+
+// ------------------------------------------------------------ halo exchange
+
+eu_status eu_halo_bytes(const eu_handle *h, size_t *bytes)
+{
+    if (!h || !bytes)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!h->has_mech)
+        return EU_ERR_NOT_READY;
+    const size_t elem = h->st.prim32 ? sizeof(float) : sizeof(double);
+    *bytes = size_t(7 + h->mech.ns) * h->bc * size_t(h->ny) * h->nz * elem;
+    return EU_OK;
+}
+
 namespace {
-eu_status step_impl(eu_handle *h, int nsteps, double dt, double cfl, eu_step_stats *stats, double *time)
+eu_status halo_copy(eu_handle *h, int face, bool pack, void *buf)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!buf || (face != 0 && face != 1))
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "face must be 0 or 1 and the buffer non-null");
+    if (!h->has_mech || !h->has_state)
+        return fail(h, EU_ERR_NOT_READY, "mechanism and state must be set first");
+    cudaSetDevice(h->cfg.device);
+    CK(h, strict::launch_halo(launch_args(h), 7 + h->mech.ns, face, pack, buf));
+    return EU_OK;
+}
+} // namespace
+
+eu_status eu_halo_pack(eu_handle *h, int face, void *device_buf) { return halo_copy(h, face, true, device_buf); }
+eu_status eu_halo_unpack(eu_handle *h, int face, const void *device_buf)
+{
+    return halo_copy(h, face, false, const_cast<void *>(device_buf));
+}
+
+namespace {
+eu_status step_impl(eu_handle *h, int nsteps, double dt, double cfl, eu_step_stats *stats, double *time,
+                    const double *dt_src)
 {
     if (!h->has_mech || !h->has_state)
         return fail(h, EU_ERR_NOT_READY, "mechanism and state must be set before stepping");
@@ -956,6 +1027,8 @@ eu_status step_impl(eu_handle *h, int nsteps, double dt, double cfl, eu_step_sta
     CK(h, cudaMemsetAsync(h->st.counters, 0, kCntCount * sizeof(unsigned long long), h->stream));
     if (cfl > 0) {
         CK(h, cudaMemsetAsync(h->d_time, 0, sizeof(double), h->stream));
+    } else if (dt_src) {
+        CK(h, cudaMemcpyAsync(h->d_dt, dt_src, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
     } else {
         CK(h, strict::launch_set_value(h->d_dt, dt, h->stream));
         ++launches;
@@ -1104,8 +1177,8 @@ eu_status eu_get_field(eu_handle *h, const char *name, double *out)
 // The reference's EU3D_STATE_V1_LE dump (Euler::Output, src/Euler.cpp:1540-1598):
 // a text header "EU3D_STATE_V1_LE", one line of sizes and times (17 significant
 // digits), one line of column names, then one row of 22 + 5 ns little-endian
-// doubles per interior node in (i, j, k) order, k fastest. Written here as the
-// single rank of a 1 x 1 x 1 decomposition.
+// doubles per interior node in (i, j, k) order, k fastest. Written as block
+// block_x of a blocks_x x 1 x 1 decomposition (one rank per block).
 
 namespace {
 const char *kDumpMagic = "EU3D_STATE_V1_LE";
@@ -1167,10 +1240,12 @@ eu_status eu_write_state(eu_handle *h, const char *path, int iteration, int num,
     std::FILE *f = std::fopen(path, "wb");
     if (!f)
         return fail(h, EU_ERR_IO, "cannot open %s for writing", path);
-    // header: NS, total_n*, local n* (one rank: the same), rank coordinates 0 0 0,
-    // blocks 1 1 1, rank 0 of 1, iteration, output number, time, dt
-    std::fprintf(f, "%s\n%d %d %d %d %d %d %d 0 0 0 1 1 1 0 1 %d %d %.17g %.17g\n%s\n", kDumpMagic, ns, h->ni, h->nj,
-                 h->nk, h->ni, h->nj, h->nk, iteration, num, final_time, dt, dump_columns(ns).c_str());
+    // header: NS, total_n*, local n*, block coordinates (x blocks only), blocks
+    // per axis, rank (the x block) of ranks, iteration, output number, time, dt
+    const int blocks_x = h->cfg.blocks_x > 1 ? h->cfg.blocks_x : 1;
+    std::fprintf(f, "%s\n%d %d %d %d %d %d %d %d 0 0 %d 1 1 %d %d %d %d %.17g %.17g\n%s\n", kDumpMagic, ns,
+                 h->cfg.total_ni, h->nj, h->nk, h->ni, h->nj, h->nk, h->cfg.block_x, blocks_x, h->cfg.block_x, blocks_x,
+                 iteration, num, final_time, dt, dump_columns(ns).c_str());
     const int ncols = 22 + 5 * ns;
     std::vector<double> row(ncols);
     bool ok = true;

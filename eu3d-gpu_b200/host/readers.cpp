@@ -119,11 +119,12 @@ bool read_grid(const std::string &path, GridSpec &g, std::string &err)
     return true;
 }
 
-std::vector<double> node_coordinates(int n, double a, double b, int bc)
+std::vector<double> node_coordinates(int total_n, double a, double b, int bc, int blocks, int block)
 {
+    const int n = (total_n - 1) / blocks + 1;
     std::vector<double> x(n + 2 * bc, 0.0);
-    const double d = (b - a) / (n - 1);
-    for (int i = bc; i < n + bc; i++) x[i] = a + (0 * (n - 1) + i - bc) * d;
+    const double d = (b - a) / (total_n - 1);
+    for (int i = bc; i < n + bc; i++) x[i] = a + (block * (n - 1) + i - bc) * d;
     for (int i = 0; i < bc; i++) {
         x[i] = 2 * x[bc] - x[2 * bc - i];
         x[n + bc + i] = 2 * x[n + bc - 1] - x[n + bc - 1 - i - 1];

@@ -35,8 +35,10 @@ struct GridSpec {
 
 bool read_grid(const std::string &path, GridSpec &out, std::string &err);
 
-// Node coordinates with ghosts for one block (src/Mesh.cpp:96-142).
-std::vector<double> node_coordinates(int total_n, double a, double b, int bc);
+// Node coordinates with ghosts of block `block` of `blocks` along one axis
+// (Mesh::Initial, src/Mesh.cpp:96-119: (total_n - 1) / blocks + 1 nodes from
+// the global spacing; Mesh::Boundary, :131-142: ghosts extrapolated linearly).
+std::vector<double> node_coordinates(int total_n, double a, double b, int bc, int blocks = 1, int block = 0);
 
 struct MechanismTables {
     int ns = 0, nr = 0, tb_count = 0;

@@ -94,6 +94,13 @@ typedef struct {
     int eager;                        /* nonzero: launch each step's kernels one by one instead of
                                          replaying the step's captured CUDA graph */
     int boundary;                     /* eu_boundary: which case's ghost fill */
+    int blocks_x;                     /* domain decomposition along x (the reference's m_block_x): the
+                                         handle holds (total_ni - 1) / blocks_x + 1 nodes of the global
+                                         grid, neighbouring blocks sharing one node (Mesh::Initial,
+                                         src/Mesh.cpp:96-119); 0 or 1: the whole grid */
+    int block_x;                      /* this handle's block, 0 .. blocks_x - 1 (the reference's myid_x);
+                                         x faces between blocks take their ghost nodes from
+                                         eu_halo_unpack instead of the boundary condition */
 } eu_config;
 
 /* Mechanism and thermo tables in the reference's layouts (src/Reaction.cpp:156-327). */
@@ -235,6 +242,32 @@ eu_status eu_chem_advance(eu_handle *h, long long n, double *cs, double *T, doub
 /* Device pointers and the stream of a handle, for callers that keep inputs
  * resident and time kernels themselves. */
 eu_status eu_device_info(const eu_handle *h, void **stream, size_t *device_bytes);
+
+/* ---------------------------------------------------------------------------
+ * Halo exchange between x blocks (Flowfield::Mpi_Boundary, src/Flowfield.cpp:809-911,
+ * the m_block_x > 1 part). A message holds the bc node planes one neighbour needs of
+ * the primitive planes the flux reads (P, D, U, V, W, H, Gamma, Y_0 .. Y_ns-1; FP32 in
+ * EU_PREC_MIXED, FP64 otherwise), laid out [field][plane][j][k] with full haloed planes.
+ * The caller moves messages between ranks (NCCL, MPI) and unpacks them before each step:
+ *   face 0 (x low):  pack = nodes bc+1 .. 2bc (the reference's bc+1+i), sent to block_x-1;
+ *                    unpack fills ghost nodes bc-1-i from the x-low neighbour's face-1 message
+ *   face 1 (x high): pack = nodes ni, ni-1 (the reference's ni-i, bc = 2), sent to block_x+1;
+ *                    unpack fills ghost nodes ni+bc+i from the x-high neighbour's face-0 message
+ * device_buf is device memory of eu_halo_bytes bytes. Both are asynchronous on the
+ * handle's stream (eu_device_info). */
+eu_status eu_halo_bytes(const eu_handle *h, size_t *bytes);
+eu_status eu_halo_pack(eu_handle *h, int face, void *device_buf);
+eu_status eu_halo_unpack(eu_handle *h, int face, const void *device_buf);
+
+/* The CFL timestep of this block's current state, written to device memory on the
+ * handle's stream (the local part of Flowfield::CFLcondition, src/Flowfield.cpp:275-304,
+ * before its MPI_Allreduce(MPI_MIN)); the caller reduces it across blocks and steps with
+ * eu_step_dt_device. */
+eu_status eu_cfl_dt(eu_handle *h, double cfl, double *device_dt);
+
+/* eu_step with dt read from device memory (each step uses the value at *device_dt when
+ * the call is queued; asynchronous unless stats is non-NULL). */
+eu_status eu_step_dt_device(eu_handle *h, int nsteps, const double *device_dt, eu_step_stats *stats);
 
 /* ---------------------------------------------------------------------------
  * Learned chemistry (no counterpart in the reference, which has no learned

@@ -42,6 +42,7 @@ struct eo_state {
     double dt;
     int bad_nchem;
     int bc_kind; /* 0: RSBI ghost fill, 1: ZND */
+    int exch_lo, exch_hi; /* x faces filled by the halo exchange, not the ghost fill */
 };
 
 #define IDX(st, i, j, k) (((long)(i) * (st)->ny + (j)) * (st)->nz + (k))
@@ -433,11 +434,15 @@ static void boundary_fill(eo_state *st)
                 const long lo = IDX(st, i, j, k), hi = IDX(st, ni + bc + i, j, k);
                 const long slo = IDX(st, 2 * bc - 1 - i, j, k), shi = IDX(st, 2 * (ni + bc) - 1 - (ni + bc + i), j, k);
                 if (st->bc_kind == 1) {
-                    copy_cell(st, lo, slo, -1, 1, 1);
-                    rebuild_cell(st, hi, shi, 1);
+                    if (!st->exch_lo)
+                        copy_cell(st, lo, slo, -1, 1, 1);
+                    if (!st->exch_hi)
+                        rebuild_cell(st, hi, shi, 1);
                 } else {
-                    copy_cell(st, lo, slo, 1, 1, 1);
-                    copy_cell(st, hi, shi, 1, 1, 1);
+                    if (!st->exch_lo)
+                        copy_cell(st, lo, slo, 1, 1, 1);
+                    if (!st->exch_hi)
+                        copy_cell(st, hi, shi, 1, 1, 1);
                 }
             }
     /* y front: symmetry with thermo recomputed from mirrored T, p, Y (:647-679) */
@@ -657,6 +662,46 @@ void eo_set_state(eo_state *st, const double *cs, const double *T, const double 
 void eo_boundary(eo_state *st) { boundary_fill(st); }
 
 void eo_set_boundary(eo_state *st, int kind) { st->bc_kind = kind; }
+
+void eo_set_exchange(eo_state *st, int x_low, int x_high)
+{
+    st->exch_lo = x_low != 0;
+    st->exch_hi = x_high != 0;
+}
+
+/* Halo messages between x blocks (Flowfield::Mpi_Boundary, src/Flowfield.cpp:809-911):
+ * [field][plane][j][k] over full haloed planes, fields P D U V W H Gamma Y_0..Y_ns-1.
+ * Pack face 0 takes nodes bc+1+p (the reference's bc+1+i), face 1 nodes ni+bc-2-p
+ * (its ni-i for bc = 2); unpack face 0 fills ghost nodes bc-1-p, face 1 ni+bc+p. */
+static double *halo_field(eo_state *st, int f)
+{
+    double *one[7] = {st->P, st->D, st->U, st->V, st->W, st->H, st->G};
+    return f < 7 ? one[f] : st->Y + (long)(f - 7) * st->n3;
+}
+
+static void halo_copy(eo_state *st, int face, int pack, double *msg)
+{
+    const long plane = (long)st->ny * st->nz;
+    const int bc = st->bc, ni = st->ni;
+    for (int f = 0; f < 7 + st->ns; f++)
+        for (int p = 0; p < bc; p++) {
+            int i;
+            if (pack)
+                i = face == 0 ? bc + 1 + p : ni + bc - 2 - p;
+            else
+                i = face == 0 ? bc - 1 - p : ni + bc + p;
+            double *node = halo_field(st, f) + (long)i * plane;
+            double *m = msg + ((long)f * bc + p) * plane;
+            if (pack)
+                memcpy(m, node, plane * sizeof(double));
+            else
+                memcpy(node, m, plane * sizeof(double));
+        }
+}
+
+long eo_halo_count(const eo_state *st) { return (long)(7 + st->ns) * st->bc * st->ny * st->nz; }
+void eo_halo_pack(eo_state *st, int face, double *msg) { halo_copy(st, face, 1, msg); }
+void eo_halo_unpack(eo_state *st, int face, const double *msg) { halo_copy(st, face, 0, (double *)msg); }
 
 int eo_step(eo_state *st, int nsteps, double dt)
 {

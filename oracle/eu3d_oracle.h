@@ -63,6 +63,15 @@ void eo_boundary(eo_state *st);
  * src/Flowfield.cpp:317-411, commented out in the reference). */
 void eo_set_boundary(eo_state *st, int kind);
 
+/* Domain decomposition along x (the reference's MPI layout with m_block_x > 1):
+ * x faces whose ghost nodes come from a neighbouring block are skipped by the
+ * ghost fill and filled by eo_halo_unpack (Flowfield::Mpi_Boundary,
+ * src/Flowfield.cpp:809-911). Messages hold eo_halo_count doubles. */
+void eo_set_exchange(eo_state *st, int x_low, int x_high);
+long eo_halo_count(const eo_state *st);
+void eo_halo_pack(eo_state *st, int face, double *msg);
+void eo_halo_unpack(eo_state *st, int face, const double *msg);
+
 /* Copy a named field out (SoA, haloed). Names: P D T U V W H E Gamma C Ma Wav
  * Rgas Cp (1 plane); Yi Di Mc CMS (ns planes); CS (ns+4 planes); Nchem (1 plane,
  * as doubles). Returns planes copied, or -1 for an unknown name. */

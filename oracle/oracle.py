@@ -88,12 +88,16 @@ def write_input_file(path, ns, nr, p_pre=101325.0, t_pre=1000.0, m_wave=3.0):
         f.write(f"P_pre    {p_pre!r}\nT_pre    {t_pre!r}\nM_wave    {m_wave!r}\nNS    {ns}\nNR    {nr}\n")
 
 
-def node_coordinates(n, a, b, bc=2):
-    """Node coordinates with mirrored ghosts, as src/Mesh.cpp:96-142 builds them (one block)."""
-    d = (b - a) / (n - 1)
+def node_coordinates(total_n, a, b, bc=2, blocks=1, block=0):
+    """Node coordinates with ghosts of block `block` of `blocks` along one axis:
+    Mesh::Initial (src/Mesh.cpp:96-119) gives the block (total_n - 1) / blocks + 1
+    nodes at the global spacing, Mesh::Boundary (:131-142) mirrors the ghosts
+    about the block's end nodes."""
+    n = (total_n - 1) // blocks + 1
+    d = (b - a) / (total_n - 1)
     x = np.zeros(n + 2 * bc)
     for i in range(bc, n + bc):
-        x[i] = a + (0 * (n - 1) + i - bc) * d
+        x[i] = a + (block * (n - 1) + i - bc) * d
     for i in range(bc):
         x[i] = 2 * x[bc] - x[2 * bc - i]
         x[n + bc + i] = 2 * x[n + bc - 1] - x[n + bc - 1 - i - 1]
@@ -241,6 +245,11 @@ class PortOracle:
             lib.eo_step.argtypes = [_P, _I, _D]
             lib.eo_boundary.argtypes = [_P]
             lib.eo_set_boundary.argtypes = [_P, _I]
+            lib.eo_set_exchange.argtypes = [_P, _I, _I]
+            lib.eo_halo_count.restype = ctypes.c_long
+            lib.eo_halo_count.argtypes = [_P]
+            lib.eo_halo_pack.argtypes = [_P, _I, _P]
+            lib.eo_halo_unpack.argtypes = [_P, _I, _P]
             lib.eo_get.restype = _I
             lib.eo_get.argtypes = [_P, ctypes.c_char_p, _P]
             lib.eo_thermo.argtypes = [_P, _D, _D, _I, _P]
@@ -299,6 +308,23 @@ class PortOracle:
 
     def boundary(self):
         self.lib().eo_boundary(self.h)
+
+    def set_exchange(self, x_low, x_high):
+        """x faces whose ghost nodes come from a neighbouring block (eo_halo_unpack)."""
+        self.lib().eo_set_exchange(self.h, int(bool(x_low)), int(bool(x_high)))
+
+    def halo_count(self):
+        return int(self.lib().eo_halo_count(self.h))
+
+    def halo_pack(self, face, out):
+        """Fill `out` (float64, contiguous, halo_count values) with the face's message."""
+        assert out.dtype == np.float64 and out.flags.c_contiguous and out.size == self.halo_count()
+        self.lib().eo_halo_pack(self.h, int(face), out.ctypes.data)
+
+    def halo_unpack(self, face, msg):
+        m = np.ascontiguousarray(msg, dtype=np.float64)
+        assert m.size == self.halo_count()
+        self.lib().eo_halo_unpack(self.h, int(face), m.ctypes.data)
 
     def get(self, name):
         planes = {"Yi": self.ns, "Di": self.ns, "Mc": self.ns, "CMS": self.ns, "CS": self.ns + 4}.get(name, 1)
