@@ -389,6 +389,58 @@ def znd_case(args, local, steps=1000, cells=4000, dx=25e-6):
                                                                  "recover_block": tuned["recover_block"]}}
 
 
+def odw_case(args, local, model, gate, grid=(1024, 512, 2), steps=2000):
+    """The 2-D oblique detonation case: 1024 x 512 x 2 nodes over the
+    reference's 2dODW extent (52.5 x 20 mm; the z spacing equals the x spacing),
+    a Mach 7.5 stoichiometric H2-air freestream at 40 kPa / 293 K meeting a 25
+    degree wedge (data/input-ODW.txt) in a wedge-aligned frame (the y-low face
+    is the wedge surface), the reference's ODW ghost fill (EU_BC_ODW), the
+    learned + mixed step with each dt from the CFL rule at 0.5 on the device,
+    2000 steps. Reports the device throughput, the time advanced, the peak
+    temperature and the shock angle: where p first exceeds 1.5 x the
+    freestream pressure from the top down, fitted over the middle half of x,
+    plus the wedge angle (the oblique-shock relation gives about 32 degrees
+    for an ideal gas at gamma 1.4)."""
+    ni, nj, nk = grid
+    dx = 0.0525 / (ni - 1)
+    ext = (0.0, 0.0525, 0.0, 0.02, 0.0, dx * (nk - 1))
+    x = cases.node_coordinates(ni, ext[0], ext[1])
+    y = cases.node_coordinates(nj, ext[2], ext[3])
+    z = cases.node_coordinates(nk, ext[4], ext[5])
+    mech = eu3d.parse_mechanism(cases.MECH_JA919, cases.THERMO)
+    prim, inflow = cases.odw(x, y, z, mech)
+    p, cs, T, E = eu3d.initial_state(mech, ni, nj, nk, *prim)
+    chem = "learned" if model is not None else "stiff"
+    s = eu3d.Solver(ni, nj, nk, ext, precision="mixed", chemistry=chem, arith="fast", device=local, boundary="odw")
+    s.set_mechanism(mech)
+    s.set_state(state_dict((p, cs, T, E)))
+    s.set_inflow(*inflow)
+    if model is not None:
+        import learned
+        learned.attach(s, model, gate)
+    tuned = s.autotune(reps=3)
+    st, t_adv = s.step_cfl(steps, CFL)
+    pr = s.get("P")[0, 2:-2, 2:-2, 2]
+    t_end = s.get("T")[0, 2:-2, 2:-2, 2]
+    s.close()
+    p0 = eu3d.read_value(cases.INPUT_ODW, "P")
+    angle = eu3d.read_value(cases.INPUT_ODW, "angle")
+    xs, hs = [], []
+    for i in range(ni // 4, 3 * ni // 4):
+        hit = np.nonzero(pr[i, ::-1] > 1.5 * p0)[0]
+        if hit.size:
+            xs.append(x[2 + i])
+            hs.append(y[2 + nj - 1 - hit[0]])
+    beta = (math.degrees(math.atan(np.polyfit(xs, hs, 1)[0])) + angle) if len(xs) > 8 else None
+    return {"grid": list(grid), "steps": steps, "time_advanced_s": t_adv, "chemistry": chem,
+            "value": round(ni * nj * nk * steps / (st["device_ms"] / 1e3) / 1e6, 3), "unit": "Mcell-steps/s",
+            "ms_per_step": round(st["device_ms"] / steps, 4), "peak_T_K": round(float(t_end.max()), 1),
+            "peak_p_Pa": round(float(pr.max()), 1), "shock_angle_deg": None if beta is None else round(beta, 2),
+            "learned_cells_last_step": st["learned"], "fallback_cells_last_step": st["fallback"],
+            "max_nchem_last_step": st["max_nchem"],
+            "autotune": {"flux_ci": tuned["flux_ci"], "recover_block": tuned["recover_block"]}}
+
+
 BATCH_SIZES = ((64, 64, 64), (128, 64, 64), (192, 96, 96))
 
 
@@ -705,12 +757,16 @@ def our_arm(args):
     batch = None
     if args.chem == "learned" and not args.no_batch:
         batch = batch_instances(args, model, gate, local, mech)
-    znd = None
+    znd = odw = None
     if not args.no_batch:
         try:
             znd = znd_case(args, local)
         except eu3d.EU3DError as e:  # reported, not fatal to the headline measurement
             znd = {"error": str(e)}
+        try:
+            odw = odw_case(args, local, model, gate)
+        except eu3d.EU3DError as e:
+            odw = {"error": str(e)}
 
     # -- per-kernel times (same stream, CUDA events around each kernel phase) -----------------
     sp = make_solver(args.chem, args.precision, args.arith, profile=True)
@@ -777,6 +833,7 @@ def our_arm(args):
                 "batch_instances": batch,
                 "mlp_roofline": mlp,
                 "znd_1d": znd,
+                "odw_2d": odw,
                 "roofline": roofline, "kernels_ms_per_step": per_kernel,
                 "max_nchem": stats["max_nchem"], "reacting_cells": stats["reacting"],
                 "learned_cells": stats["learned"], "fallback_cells": stats["fallback"],

@@ -42,6 +42,7 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
     long long dst, src;
     double su = 1, sv = 1, sw = 1;
     bool rebuild = false;
+    long long inflow = -1; // ODW x-low: index into the inflow tables
     if (t < nxf) {
         const int jk = fdiv(t, g.d_nk), q = fdiv(t, g.d_njnk); // q: 0 .. 2bc-1
         const int k = bc + int(t - (long long)jk * nk);
@@ -54,6 +55,10 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
         src = cell_index(g, si, j, k);
         if (g.bc_kind == 1) {
             su = q < bc ? -1 : 1;
+            rebuild = q >= bc;
+        } else if (g.bc_kind == 2) { // ODW: freestream tables in, rebuilt outflow out
+            if (q < bc)
+                inflow = (long long)(j - bc) * nk + (k - bc);
             rebuild = q >= bc;
         }
     } else if (t < nxf + nyf) {
@@ -82,6 +87,20 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
         dst = cell_index(g, i, j, k);
         src = cell_index(g, i, j, sk);
         sw = -1;
+        rebuild = g.bc_kind == 2; // ODW rebuilds the thermo on the z faces
+    }
+    if (inflow >= 0) {
+        const long long nt = (long long)nj * nk;
+#pragma unroll
+        for (int f = 0; f < 7 + NS; ++f) {
+            const double v = st.inflow[f * nt + inflow];
+            if (st.prim32)
+                st.prim32[f * n3 + dst] = float(v);
+            else
+                st.prim[f * n3 + dst] = v;
+        }
+        st.T[dst] = st.inflow[(7 + NS) * nt + inflow];
+        return;
     }
     // mixed precision keeps only the FP32 primitive planes current (the flux
     // kernel's input); the FP64 path its FP64 planes

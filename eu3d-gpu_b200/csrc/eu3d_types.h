@@ -71,6 +71,7 @@ struct DevState {
     double *cms;      // ns planes (or null)
     unsigned long long *counters; // see CounterIdx
     int *heavy;       // mixed precision: {count, next, cells...} of cells left to the warp-per-cell kinetics
+    const double *inflow; // ODW x-low ghost values per interior (j, k): 7 + ns primitive planes, then T
 };
 
 // Device counters. The first kCntPerStep are statistics of the latest step

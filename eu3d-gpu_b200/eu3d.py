@@ -24,7 +24,7 @@ STATUS = {0: "EU_OK", 1: "EU_ERR_INVALID_ARGUMENT", 2: "EU_ERR_CUDA", 3: "EU_ERR
 PRECISION = {"fp64": 0, "mixed": 1}
 CHEMISTRY = {"stiff": 0, "frozen": 1, "learned": 2}
 ARITH = {"strict": 0, "fast": 1}
-BOUNDARY = {"rsbi": 0, "znd": 1}
+BOUNDARY = {"rsbi": 0, "znd": 1, "odw": 2}
 
 
 class EU3DError(RuntimeError):
@@ -144,6 +144,8 @@ def library():
         lib.eu_batch_last_error.restype = ctypes.c_char_p
         for fn in ("eu_batch_create", "eu_batch_step", "eu_batch_destroy"):
             getattr(lib, fn).restype = _I
+        lib.eu_set_inflow.argtypes = [_P] * 7
+        lib.eu_set_inflow.restype = _I
         lib.eu_halo_bytes.argtypes = [_P, ctypes.POINTER(ctypes.c_size_t)]
         lib.eu_halo_pack.argtypes = [_P, _I, _P]
         lib.eu_halo_unpack.argtypes = [_P, _I, _P]
@@ -317,6 +319,12 @@ class Solver:
         order = ["CS", "T", "E", "P", "D", "U", "V", "W", "H", "Gamma", "Yi"]
         arrs = [_c(st[n]) for n in order]
         self._check(library().eu_set_state(self.h, *[a.ctypes.data for a in arrs]), "set_state")
+
+    def set_inflow(self, P, T, U, V, W, Y):
+        """EU_BC_ODW x-low inflow tables over the interior (j, k) nodes: planes
+        (nj, nk), Y (ns, nj, nk) (eu_set_inflow)."""
+        arrs = [_c(a) for a in (P, T, U, V, W, Y)]
+        self._check(library().eu_set_inflow(self.h, *[a.ctypes.data for a in arrs]), "set_inflow")
 
     def step(self, nsteps, dt, stats=True):
         s = StepStats()

@@ -9,6 +9,13 @@
   input-1dZND.txt in the reference's key/value format (P_bound, T_bound, P, T,
   and driver_nodes, this build's addition). The reference's ZND case is dead
   code (its boundary is commented out and its initialiser hard-codes RSBI).
+* ``odw`` — the oblique detonation wave cases: a Mach 7.5 H2-air freestream
+  (input-ODW.txt: P, T, Mach, wedge angle) meeting a 25 degree wedge. The
+  reference's FieldBoundary_3dODW has a symmetry (reflecting) y-low face and
+  x-low inflow tables it never fills; here the grid is wedge-aligned: the
+  y-low face is the wedge surface, the tip at x = 0, and the freestream (the
+  inflow tables and the initial field) arrives at the wedge angle. Optional
+  equivalence ratio phi(z) for the 3-D case.
 * ``shock_bubble`` — the 3-D reacting shock-bubble workload: a planar shock
   in N2 hitting a sphere of stoichiometric 2H2+O2 with a tanh interface and a
   seeded spherical-harmonic surface perturbation (l = 1..8, RMS amplitude 2 % of
@@ -35,6 +42,8 @@ THERMO = os.path.join(DATA, "thermo.dat")
 MECH_JA919_AR = os.path.join(DATA, "H2_JA919_Ar.txt")
 THERMO_AR = os.path.join(DATA, "thermo_Ar.dat")
 INPUT_ZND = os.path.join(DATA, "input-1dZND.txt")
+INPUT_ODW = os.path.join(DATA, "input-ODW.txt")
+GRID_3DODW = os.path.join(DATA, "grid-3dODW.txt")
 
 # species slots of H2_JA919 (H O H2O OH O2 H2 H2O2 HO2 N2)
 S_H2O, S_O2, S_H2, S_N2 = 2, 4, 5, 8
@@ -279,3 +288,83 @@ def znd(x, y, z, mw, ns, input_path=INPUT_ZND, mole=None, bc=2, interface_cells=
     T = t0 + f * (t_drv - t0)
     Z = np.zeros((nx, ny, nz))
     return P, T, Z, Z.copy(), Z.copy(), Y
+
+
+def h2_air(mw, ns, phi=1.0):
+    """Mass fractions of H2-air at equivalence ratio phi (2 phi H2 + O2 + 3.76 N2
+    by moles; phi = 1 gives Y_H2 0.0285, Y_O2 0.2264, Y_N2 0.7451)."""
+    phi = np.asarray(phi, dtype=np.float64)
+    m = {S_H2: 2.0 * phi, S_O2: np.ones_like(phi), S_N2: 3.76 * np.ones_like(phi)}
+    tot = sum(v * mw[s] for s, v in m.items())
+    Y = np.zeros((ns,) + phi.shape)
+    for s, v in m.items():
+        Y[s] = v * mw[s] / tot
+    return Y
+
+
+def mixture_gamma(mech, T, Y):
+    """cp / cv of a mixture from the NASA polynomials (the reference's GetCpi
+    form, src/Reaction.cpp:1165-1177) at temperature T; Y (ns, ...)."""
+    lo = T < 1000.0
+    c = np.where(lo, 1.0, 0.0)
+    a = np.asarray(mech["coeff_lo"]) * c + np.asarray(mech["coeff_hi"]) * (1 - c)  # (9, ns)
+    r_s = 8.31434 / np.asarray(mech["mw"])
+    cp_s = r_s * (a[0] * T ** -2 + a[1] / T + a[2] + a[3] * T + a[4] * T ** 2 + a[5] * T ** 3 + a[6] * T ** 4)
+    Ys = np.moveaxis(np.asarray(Y), 0, -1)
+    cp = Ys @ cp_s
+    r = Ys @ r_s
+    return cp / (cp - r), r * 1000
+
+
+def odw_inflow(mech, nj, nk, z=None, input_path=INPUT_ODW, phi=None):
+    """The freestream on the interior (j, k) nodes: P, T, U, V, W planes (nj, nk)
+    and Y (ns, nj, nk). The speed is Mach x the frozen sound speed of the
+    mixture; the velocity points into the wedge surface at the wedge angle
+    (U = V cos a, V = -V sin a). phi: equivalence ratio per k (length nk), or
+    None for 1."""
+    import eu3d
+    p0 = eu3d.read_value(input_path, "P")
+    t0 = eu3d.read_value(input_path, "T")
+    mach = eu3d.read_value(input_path, "Mach")
+    angle = math.radians(eu3d.read_value(input_path, "angle"))
+    ns = int(mech["ns"])
+    ph = np.ones(nk) if phi is None else np.asarray(phi, dtype=np.float64)
+    Yk = h2_air(mech["mw"], ns, ph)  # (ns, nk)
+    g, r = mixture_gamma(mech, t0, Yk)
+    speed = mach * np.sqrt(g * r * t0)  # (nk,)
+    P = np.full((nj, nk), p0)
+    T = np.full((nj, nk), t0)
+    U = np.broadcast_to(speed * math.cos(angle), (nj, nk)).copy()
+    V = np.broadcast_to(-speed * math.sin(angle), (nj, nk)).copy()
+    W = np.zeros((nj, nk))
+    Y = np.broadcast_to(Yk[:, None, :], (ns, nj, nk)).copy()
+    return P, T, U, V, W, Y
+
+
+def odw_phi(z, seed=4, modes=4, amplitude=0.1, bc=2):
+    """Equivalence ratio along z: 1 + sum_{m=1..modes} a_m sin(2 pi m z / L + theta_m),
+    the sum scaled so its largest magnitude over the interior nodes is
+    `amplitude` (a_m ~ N(0, 1), theta_m ~ U[0, 2 pi) from default_rng(seed))."""
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal(modes)
+    th = rng.uniform(0.0, 2 * math.pi, modes)
+    zi = np.asarray(z)[bc:-bc]
+    L = zi[-1] - zi[0] if len(zi) > 1 else 1.0
+    s = sum(a[m] * np.sin(2 * math.pi * (m + 1) * (zi - zi[0]) / L + th[m]) for m in range(modes))
+    peak = np.abs(s).max()
+    return 1.0 + (amplitude * s / peak if peak > 0 else 0 * s)
+
+
+def odw(x, y, z, mech, input_path=INPUT_ODW, phi=None, bc=2):
+    """The ODW case: the freestream of odw_inflow on every node (ghosts
+    included; the z ghosts repeat the nearest interior node's composition).
+    Returns (P, T, U, V, W, Y) over the haloed grid and the inflow tables."""
+    nx, ny, nz = len(x), len(y), len(z)
+    nj, nk = ny - 2 * bc, nz - 2 * bc
+    inflow = odw_inflow(mech, nj, nk, input_path=input_path, phi=phi)
+    kk = np.clip(np.arange(nz) - bc, 0, nk - 1)
+    fields = []
+    for a in inflow[:5]:
+        fields.append(np.broadcast_to(a[0][kk][None, None, :], (nx, ny, nz)).copy())
+    Y = np.broadcast_to(inflow[5][:, 0, kk][:, None, None, :], (int(mech["ns"]), nx, ny, nz)).copy()
+    return (*fields, Y), inflow

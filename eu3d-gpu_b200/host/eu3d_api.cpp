@@ -41,6 +41,7 @@ struct eu_handle {
     unsigned long long *d_cfl_slot = nullptr; // CFL minimum of the step being set up
     double *d_time = nullptr;                 // time advanced by the CFL-driven steps of a call
     double *d_scratch = nullptr;
+    double *d_inflow = nullptr; // EU_BC_ODW x-low tables ((8 + ns) planes of nj * nk)
     std::vector<void *> allocs;
     size_t bytes = 0;
     cudaStream_t stream = nullptr;
@@ -390,7 +391,7 @@ eu_status eu_create(const eu_config *cfg, eu_handle **out)
         return EU_ERR_INVALID_ARGUMENT;
     if (cfg->chemistry != EU_CHEM_STIFF && cfg->chemistry != EU_CHEM_FROZEN && cfg->chemistry != EU_CHEM_LEARNED)
         return EU_ERR_INVALID_ARGUMENT;
-    if (cfg->boundary != EU_BC_RSBI && cfg->boundary != EU_BC_ZND)
+    if (cfg->boundary != EU_BC_RSBI && cfg->boundary != EU_BC_ZND && cfg->boundary != EU_BC_ODW)
         return EU_ERR_INVALID_ARGUMENT;
     // x blocks: the reference's layout rule (src/Mesh.cpp:64-75) and at least
     // bc + 2 nodes per block (a message reaches node 2 bc)
@@ -619,6 +620,35 @@ eu_status eu_set_primitive(eu_handle *h, const double *P, const double *T, const
     const long long n3 = h->n3;
     return eu_set_state(h, cs.data(), Tv.data(), Ev.data(), &prim[0], &prim[n3], &prim[2 * n3], &prim[3 * n3],
                         &prim[4 * n3], &prim[5 * n3], &prim[6 * n3], &prim[7 * n3]);
+}
+
+eu_status eu_set_inflow(eu_handle *h, const double *P, const double *T, const double *U, const double *V,
+                        const double *W, const double *Y)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!P || !T || !U || !V || !W || !Y)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "null argument");
+    if (!h->has_mech)
+        return fail(h, EU_ERR_NOT_READY, "load a mechanism first");
+    // the (j, k) tables as a one-plane grid without ghosts: FieldInitial's
+    // derived values on every node
+    std::vector<double> prim, cs, Tv, Ev;
+    primitive_to_state(h->mech, 1, h->nj, h->nk, 0, P, T, U, V, W, Y, prim, cs, Tv, Ev);
+    const size_t nt = size_t(h->nj) * h->nk, nf = 7 + size_t(h->mech.ns);
+    prim.insert(prim.end(), Tv.begin(), Tv.end()); // T after the primitive planes
+    cudaSetDevice(h->cfg.device);
+    if (!h->d_inflow) {
+        eu_status st = dalloc(h, &h->d_inflow, (nf + 1) * nt);
+        if (st != EU_OK)
+            return st;
+    }
+    CK(h, cudaMemcpyAsync(h->d_inflow, prim.data(), (nf + 1) * nt * sizeof(double), cudaMemcpyHostToDevice,
+                          h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    h->st.inflow = h->d_inflow;
+    h->graph_dirty = true;
+    return EU_OK;
 }
 
 namespace {
@@ -1008,6 +1038,8 @@ eu_status step_impl(eu_handle *h, int nsteps, double dt, double cfl, eu_step_sta
 {
     if (!h->has_mech || !h->has_state)
         return fail(h, EU_ERR_NOT_READY, "mechanism and state must be set before stepping");
+    if (h->cfg.boundary == EU_BC_ODW && !h->g.exch_lo && !h->st.inflow)
+        return fail(h, EU_ERR_NOT_READY, "the ODW ghost fill needs its inflow tables (eu_set_inflow)");
     cudaSetDevice(h->cfg.device);
     const bool prof = h->cfg.profile != 0 && stats != nullptr;
     const LaunchArgs a = launch_args(h);

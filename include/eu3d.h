@@ -75,9 +75,14 @@ typedef enum {
 /* Ghost fill of the case (the reference wires one per case). */
 typedef enum {
     EU_BC_RSBI = 0, /* Flowfield::FieldBoundary_3dRSBI (src/Flowfield.cpp:593-807) */
-    EU_BC_ZND = 1   /* Flowfield::FieldBoundary_1dZND (src/Flowfield.cpp:317-411, commented out in the
+    EU_BC_ZND = 1,  /* Flowfield::FieldBoundary_1dZND (src/Flowfield.cpp:317-411, commented out in the
                        reference): reflecting wall at x low, outflow with the thermo rebuilt at x high;
                        y and z faces as RSBI */
+    EU_BC_ODW = 2   /* Flowfield::FieldBoundary_3dODW (src/Flowfield.cpp:412-592, compiled in the
+                       reference but not called): freestream inflow tables at x low (eu_set_inflow),
+                       outflow with the thermo rebuilt at x high, y as RSBI (symmetry with the thermo
+                       rebuilt at y low, zero gradient at y high), z mirrored with W reflected and
+                       the thermo rebuilt */
 } eu_boundary;
 
 typedef struct {
@@ -191,6 +196,15 @@ eu_status eu_set_primitive(eu_handle *h, const double *P, const double *T, const
 eu_status eu_set_state(eu_handle *h, const double *cs, const double *T, const double *E, const double *P,
                        const double *D, const double *U, const double *V, const double *W, const double *H,
                        const double *G, const double *Y);
+
+/* EU_BC_ODW inflow tables: the x-low ghost nodes take these values each step
+ * (Flowfield::FieldBoundary_3dODW, src/Flowfield.cpp:414-432, which copies the
+ * tables Uint .. Yint; the reference allocates them, :138-147, but never fills
+ * them). P, T, U, V, W: host planes over the interior (j, k) nodes, nj * nk values
+ * with k fastest; Y: ns such planes. D, H, Gamma are formed from P, T, Y as
+ * Flowfield::FieldInitial forms them (src/Flowfield.cpp:226-262). */
+eu_status eu_set_inflow(eu_handle *h, const double *P, const double *T, const double *U, const double *V,
+                        const double *W, const double *Y);
 
 /* Advance nsteps timesteps of fixed dt. Asynchronous on the handle's stream
  * unless stats is non-NULL (then it synchronises and fills stats). */

@@ -43,6 +43,8 @@ struct eo_state {
     int bad_nchem;
     int bc_kind; /* 0: RSBI ghost fill, 1: ZND */
     int exch_lo, exch_hi; /* x faces filled by the halo exchange, not the ghost fill */
+    double *inflow; /* ODW: x-low ghost values per interior (j, k), 9 + ns planes
+                       (P D T U V W H Gamma E Y...), or NULL */
 };
 
 #define IDX(st, i, j, k) (((long)(i) * (st)->ny + (j)) * (st)->nz + (k))
@@ -389,14 +391,15 @@ static void copy_cell(eo_state *st, long dst, long src, double su, double sv, do
 
 /* Ghost node d from node s0 with the thermo recomputed from the mirrored T,
  * p, Y (src/Flowfield.cpp:647-679; the same rebuild closes the ZND outflow,
- * :340-366); sv flips the y velocity. */
-static void rebuild_cell(eo_state *st, long d, long s0, double sv)
+ * :340-366, and the ODW faces, :436-461, :509-585); sv, sw flip the y and z
+ * velocities. */
+static void rebuild_cell_w(eo_state *st, long d, long s0, double sv, double sw)
 {
     const int ns = st->ns;
     const long n3 = st->n3;
     st->U[d] = st->U[s0];
     st->V[d] = sv * st->V[s0];
-    st->W[d] = st->W[s0];
+    st->W[d] = sw * st->W[s0];
     st->P[d] = st->P[s0];
     st->T[d] = st->T[s0];
     const double T = st->T[d];
@@ -421,6 +424,8 @@ static void rebuild_cell(eo_state *st, long d, long s0, double sv)
     st->G[d] = Cp / (Cp - Rgas);
 }
 
+static void rebuild_cell(eo_state *st, long d, long s0, double sv) { rebuild_cell_w(st, d, s0, sv, 1); }
+
 static void boundary_fill(eo_state *st)
 {
     const int ni = st->ni, nj = st->nj, nk = st->nk, bc = st->bc;
@@ -433,7 +438,26 @@ static void boundary_fill(eo_state *st)
             for (int k = bc; k < nk + bc; k++) {
                 const long lo = IDX(st, i, j, k), hi = IDX(st, ni + bc + i, j, k);
                 const long slo = IDX(st, 2 * bc - 1 - i, j, k), shi = IDX(st, 2 * (ni + bc) - 1 - (ni + bc + i), j, k);
-                if (st->bc_kind == 1) {
+                if (st->bc_kind == 2) {
+                    /* ODW: freestream inflow tables at x low (:414-432), outflow
+                     * with the thermo rebuilt at x high (:434-461) */
+                    if (!st->exch_lo && st->inflow) {
+                        const long nt = (long)nj * nk, t = (long)(j - bc) * nk + (k - bc);
+                        const double *f = st->inflow;
+                        st->P[lo] = f[0 * nt + t];
+                        st->D[lo] = f[1 * nt + t];
+                        st->T[lo] = f[2 * nt + t];
+                        st->U[lo] = f[3 * nt + t];
+                        st->V[lo] = f[4 * nt + t];
+                        st->W[lo] = f[5 * nt + t];
+                        st->H[lo] = f[6 * nt + t];
+                        st->G[lo] = f[7 * nt + t];
+                        st->E[lo] = f[8 * nt + t];
+                        for (int s = 0; s < st->ns; s++) st->Y[s * st->n3 + lo] = f[(9 + s) * nt + t];
+                    }
+                    if (!st->exch_hi)
+                        rebuild_cell(st, hi, shi, 1);
+                } else if (st->bc_kind == 1) {
                     if (!st->exch_lo)
                         copy_cell(st, lo, slo, -1, 1, 1);
                     if (!st->exch_hi)
@@ -454,12 +478,20 @@ static void boundary_fill(eo_state *st)
         for (int j = nj + bc; j < nj + 2 * bc; j++)
             for (int k = bc; k < nk + bc; k++)
                 copy_cell(st, IDX(st, i, j, k), IDX(st, i, 2 * (nj + bc) - 1 - j, k), 1, 1, 1);
-    /* z: mirror copy with W reflected (:710-802) */
+    /* z: mirror copy with W reflected (:710-802); ODW rebuilds the thermo
+     * there as well (:524-585) */
     for (int i = bc; i < ni + bc; i++)
         for (int j = bc; j < nj + bc; j++)
             for (int k = 0; k < bc; k++) {
-                copy_cell(st, IDX(st, i, j, k), IDX(st, i, j, 2 * bc - 1 - k), 1, 1, -1);
-                copy_cell(st, IDX(st, i, j, nk + bc + k), IDX(st, i, j, 2 * (nk + bc) - 1 - (nk + bc + k)), 1, 1, -1);
+                const long lo = IDX(st, i, j, k), slo = IDX(st, i, j, 2 * bc - 1 - k);
+                const long hi = IDX(st, i, j, nk + bc + k), shi = IDX(st, i, j, 2 * (nk + bc) - 1 - (nk + bc + k));
+                if (st->bc_kind == 2) {
+                    rebuild_cell_w(st, lo, slo, 1, -1);
+                    rebuild_cell_w(st, hi, shi, 1, -1);
+                } else {
+                    copy_cell(st, lo, slo, 1, 1, -1);
+                    copy_cell(st, hi, shi, 1, 1, -1);
+                }
             }
 }
 
@@ -597,6 +629,7 @@ void eo_destroy(eo_state *st)
                       st->Y, st->CS, st->cms, st->flux[0], st->flux[1], st->flux[2]};
     for (unsigned q = 0; q < sizeof(bufs) / sizeof(bufs[0]); q++) free(bufs[q]);
     free(st->nchem);
+    free(st->inflow);
     free(st);
 }
 
@@ -662,6 +695,42 @@ void eo_set_state(eo_state *st, const double *cs, const double *T, const double 
 void eo_boundary(eo_state *st) { boundary_fill(st); }
 
 void eo_set_boundary(eo_state *st, int kind) { st->bc_kind = kind; }
+
+void eo_set_inflow(eo_state *st, const double *P, const double *T, const double *U, const double *V,
+                   const double *W, const double *Y)
+{
+    const int ns = st->ns, nj = st->nj, nk = st->nk;
+    const long nt = (long)nj * nk;
+    free(st->inflow);
+    st->inflow = (double *)calloc((size_t)(9 + ns) * nt, sizeof(double));
+    double *f = st->inflow;
+    for (long t = 0; t < nt; t++) {
+        /* Flowfield::FieldInitial's derived quantities (src/Flowfield.cpp:226-262) */
+        double Yc[EO_MAXS], inv_w = 0, cp = 0, h = 0, e = 0;
+        for (int s = 0; s < ns; s++) Yc[s] = Y[s * nt + t];
+        for (int s = 0; s < ns; s++) inv_w += Yc[s] / st->mw[s];
+        const double Wav = 1.0 / inv_w;
+        const double Rgas = R_UNIV * 1000 / Wav;
+        const double Tc = T[t];
+        for (int s = 0; s < ns; s++) {
+            const double Hs = get_hi(st, Tc, st->ri[s], s);
+            cp += get_cpi(st, Tc, st->ri[s], s) * Yc[s];
+            h += Yc[s] * Hs;
+            e += Yc[s] * (Hs - st->ri[s] * Tc);
+        }
+        const double Cp = cp * 1000;
+        f[0 * nt + t] = P[t];
+        f[1 * nt + t] = P[t] / (Rgas * Tc);
+        f[2 * nt + t] = Tc;
+        f[3 * nt + t] = U[t];
+        f[4 * nt + t] = V[t];
+        f[5 * nt + t] = W[t];
+        f[6 * nt + t] = h * 1000;
+        f[7 * nt + t] = Cp / (Cp - R_UNIV * inv_w * 1000);
+        f[8 * nt + t] = e * 1000;
+        for (int s = 0; s < ns; s++) f[(9 + s) * nt + t] = Yc[s];
+    }
+}
 
 void eo_set_exchange(eo_state *st, int x_low, int x_high)
 {

@@ -60,7 +60,9 @@ int eo_step(eo_state *st, int nsteps, double dt);
 void eo_boundary(eo_state *st);
 /* Ghost fill kind: 0 RSBI (default), 1 ZND (reflecting wall at x low, outflow
  * with the thermo rebuilt at x high; Flowfield::FieldBoundary_1dZND,
- * src/Flowfield.cpp:317-411, commented out in the reference). */
+ * src/Flowfield.cpp:317-411, commented out in the reference), 2 ODW (inflow
+ * tables at x low, rebuilt outflow at x high, y as RSBI, z mirrored with W
+ * reflected and the thermo rebuilt; Flowfield::FieldBoundary_3dODW). */
 void eo_set_boundary(eo_state *st, int kind);
 
 /* Domain decomposition along x (the reference's MPI layout with m_block_x > 1):
@@ -68,6 +70,13 @@ void eo_set_boundary(eo_state *st, int kind);
  * ghost fill and filled by eo_halo_unpack (Flowfield::Mpi_Boundary,
  * src/Flowfield.cpp:809-911). Messages hold eo_halo_count doubles. */
 void eo_set_exchange(eo_state *st, int x_low, int x_high);
+
+/* ODW ghost fill (kind 2, Flowfield::FieldBoundary_3dODW, src/Flowfield.cpp:412-592):
+ * the x-low ghosts take these inflow tables (planes of nj * nk interior (j, k)
+ * nodes, k fastest; Y: ns planes), with D, H, Gamma, E formed as FieldInitial
+ * forms them (src/Flowfield.cpp:226-262). */
+void eo_set_inflow(eo_state *st, const double *P, const double *T, const double *U, const double *V,
+                   const double *W, const double *Y);
 long eo_halo_count(const eo_state *st);
 void eo_halo_pack(eo_state *st, int face, double *msg);
 void eo_halo_unpack(eo_state *st, int face, const double *msg);

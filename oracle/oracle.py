@@ -126,6 +126,8 @@ class RefOracle:
             lib.ref_set_primitive.argtypes = [_P] * 7
             lib.ref_step.argtypes = [_P, _I, _D]
             lib.ref_boundary.argtypes = [_P]
+            lib.ref_set_boundary.argtypes = [_P, _I]
+            lib.ref_set_inflow.argtypes = [_P] * 7
             lib.ref_thermo.argtypes = [_P, _D, _D, _I, _P]
             cls._lib = lib
         return cls._lib
@@ -214,6 +216,16 @@ class RefOracle:
     def boundary(self):
         self.lib().ref_boundary(self.h)
 
+    def set_boundary(self, kind):
+        """The ghost fill step() and boundary() run: "rsbi" (FieldBoundary_3dRSBI) or
+        "odw" (the reference's FieldBoundary_3dODW, which Euler::Computing never calls)."""
+        self.lib().ref_set_boundary(self.h, {"rsbi": 0, "odw": 1}[kind])
+
+    def set_inflow(self, P, T, U, V, W, Y):
+        """The ODW inflow tables (Uint .. Yint) over the interior (j, k) nodes."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (P, T, U, V, W, Y)]
+        self.lib().ref_set_inflow(self.h, *[a.ctypes.data for a in arrs])
+
     def thermo(self, T, R, s):
         out = np.zeros(3)
         self.lib().ref_thermo(self.h, float(T), float(R), int(s), out.ctypes.data)
@@ -246,6 +258,7 @@ class PortOracle:
             lib.eo_boundary.argtypes = [_P]
             lib.eo_set_boundary.argtypes = [_P, _I]
             lib.eo_set_exchange.argtypes = [_P, _I, _I]
+            lib.eo_set_inflow.argtypes = [_P] * 7
             lib.eo_halo_count.restype = ctypes.c_long
             lib.eo_halo_count.argtypes = [_P]
             lib.eo_halo_pack.argtypes = [_P, _I, _P]
@@ -279,7 +292,7 @@ class PortOracle:
                                ctypes.byref(m), int(nthreads))
         if not self.h:
             raise RuntimeError("eo_create failed")
-        lib.eo_set_boundary(self.h, {"rsbi": 0, "znd": 1}[boundary])
+        lib.eo_set_boundary(self.h, {"rsbi": 0, "znd": 1, "odw": 2}[boundary])
 
     def close(self):
         if self.h:
@@ -308,6 +321,11 @@ class PortOracle:
 
     def boundary(self):
         self.lib().eo_boundary(self.h)
+
+    def set_inflow(self, P, T, U, V, W, Y):
+        """ODW x-low inflow tables over the interior (j, k) nodes: planes (nj, nk), Y (ns, nj, nk)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (P, T, U, V, W, Y)]
+        self.lib().eo_set_inflow(self.h, *[a.ctypes.data for a in arrs])
 
     def set_exchange(self, x_low, x_high):
         """x faces whose ghost nodes come from a neighbouring block (eo_halo_unpack)."""

@@ -129,7 +129,7 @@ public:
         QuietCout quiet;
         const int bc = mesh.bc;
         flow.dt = dt;
-        flow.FieldBoundary_3dRSBI();
+        fill_ghosts();
         flow.Mpi_Boundary();
         flow.Advection(0 /* EE */, 1 /* MUSCL_2 */);
         flow.Update_after_Adv();
@@ -145,8 +145,60 @@ public:
         ++steps_done;
     }
 
+    /* The case's ghost fill: 0 FieldBoundary_3dRSBI (the one Euler::Computing
+     * calls, src/Euler.cpp:348), 1 FieldBoundary_3dODW (src/Flowfield.cpp:412-592,
+     * compiled but not called by the reference; its inflow tables come from
+     * set_inflow). */
+    int boundary_kind = 0;
+    void fill_ghosts()
+    {
+        if (boundary_kind == 1)
+            flow.FieldBoundary_3dODW();
+        else
+            flow.FieldBoundary_3dRSBI();
+    }
+
     /* The boundary fill alone (used to check ghost handling in isolation). */
-    void boundary() { QuietCout quiet; flow.FieldBoundary_3dRSBI(); }
+    void boundary() { QuietCout quiet; fill_ghosts(); }
+
+    /* ODW inflow tables Uint .. Yint over the interior (j, k) nodes from
+     * P, T, U, V, W and Y (planes of nj * nk, k fastest; Y: ns such planes),
+     * the derived D, H, Gamma, E with FieldInitial's arithmetic
+     * (src/Flowfield.cpp:226-262). The reference allocates these tables
+     * (:138-147) but never fills them. */
+    void set_inflow(const double *P, const double *T, const double *U, const double *V, const double *W,
+                    const double *Y)
+    {
+        Flowfield &F = flow;
+        const int NS = F.NS, nj = mesh.nj, nk = mesh.nk;
+        Function Fun;
+        for (int j = 0; j < nj; j++)
+            for (int k = 0; k < nk; k++) {
+                const size_t c = size_t(j) * nk + k;
+                Array<double, 1> Yt;
+                Yt.Initial(NS);
+                for (int s = 0; s < NS; s++) Yt(s) = Y[s * size_t(nj) * nk + c];
+                const double Wav = 1.0 / Fun.sum(3, Yt, F.Mw);
+                const double Rgas = F.R * 1000 / Wav;
+                const double D = P[c] / (Rgas * T[c]);
+                for (int s = 0; s < NS; s++) {
+                    F.Cpi(s) = F.React.GetCpi(T[c], F.Ri(s), s, F.Coeff0, F.Coeff1);
+                    F.Hi(s) = F.React.GetHi(T[c], F.Ri(s), s, F.Coeff0, F.Coeff1);
+                    F.Ei(s) = F.Hi(s) - F.Ri(s) * T[c];
+                }
+                const double Cp = Fun.sum(2, F.Cpi, Yt) * 1000;
+                F.Uint(j, k) = U[c];
+                F.Vint(j, k) = V[c];
+                F.Wint(j, k) = W[c];
+                F.Pint(j, k) = P[c];
+                F.Dint(j, k) = D;
+                F.Tint(j, k) = T[c];
+                F.Hint(j, k) = Fun.sum(2, Yt, F.Hi) * 1000;
+                F.Eint(j, k) = Fun.sum(2, Yt, F.Ei) * 1000;
+                F.Gint(j, k) = Cp / (Cp - F.R * Fun.sum(3, Yt, F.Mw) * 1000);
+                for (int s = 0; s < NS; s++) F.Yint(j, k, s) = Yt(s);
+            }
+    }
 
     Array<double, 3> *field3(const std::string &n)
     {
@@ -271,6 +323,16 @@ void ref_step(void *h, int nsteps, double dt)
 }
 
 void ref_boundary(void *h) { static_cast<Euler *>(h)->boundary(); }
+
+/* Ghost fill used by ref_step / ref_boundary: 0 RSBI (default), 1 ODW. */
+void ref_set_boundary(void *h, int kind) { static_cast<Euler *>(h)->boundary_kind = kind; }
+
+/* ODW inflow tables from interior (j, k) planes (k fastest). */
+void ref_set_inflow(void *h, const double *P, const double *T, const double *U, const double *V, const double *W,
+                    const double *Y)
+{
+    static_cast<Euler *>(h)->set_inflow(P, T, U, V, W, Y);
+}
 
 /* NASA thermo of one species at one temperature through the reference's own
  * Reaction::GetCpi/GetHi/GetSi (src/Reaction.cpp:1165-1220); R is the gas

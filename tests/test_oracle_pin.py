@@ -139,3 +139,47 @@ def test_znd_ghost_fill_of_the_restatement(port_lib):
     assert np.array_equal(u[ni + 2:ni + 4, 2, 2], u[ni + 1:ni - 1:-1, 2, 2])
     assert np.array_equal(p[ni + 2:ni + 4, 2, 2], p[ni + 1:ni - 1:-1, 2, 2])
     assert np.allclose(d[ni + 2:ni + 4, 2, 2], d[ni + 1:ni - 1:-1, 2, 2], rtol=1e-14)
+
+
+def test_odw_ghost_fill_matches_reference(ref_lib, port_lib):
+    """The restatement's ODW ghost fill against the reference's own
+    Flowfield::FieldBoundary_3dODW (src/Flowfield.cpp:412-592, compiled in the
+    reference but never called; the harness calls it with inflow tables the
+    reference allocates and leaves empty): every face layer bitwise, on a
+    state with random primitives, then three steps with that ghost fill."""
+    ni, nj, nk = 14, 9, 6
+    ext = (0.0, 0.013, 0.0, 0.008, 0.0, 0.005)
+    ref = ref_lib.from_grid(ni, nj, nk, ext, cases.MECH_JA919, cases.THERMO)
+    x, y, z = ref.nodes()
+    m = ref.mechanism()
+    rng = np.random.default_rng(1)
+    shape = ref.shape
+    P = 1e5 * (1 + 0.2 * rng.random(shape))
+    T = 800 + 900 * rng.random(shape)
+    U, V, W = (a * rng.standard_normal(shape) for a in (300.0, 100.0, 100.0))
+    Y = rng.random((m.ns,) + shape)
+    Y /= Y.sum(axis=0)
+    ref.set_primitive(P, T, U, V, W, Y)
+    inflow = [5e4 * (1 + rng.random((nj, nk))), 300 + 50 * rng.random((nj, nk)), 2000 + rng.random((nj, nk)),
+              -300 + rng.random((nj, nk)), np.zeros((nj, nk))]
+    yin = rng.random((m.ns, nj, nk))
+    inflow.append(yin / yin.sum(axis=0))
+    ref.set_boundary("odw")
+    ref.set_inflow(*inflow)
+    port = port_lib(ni, nj, nk, x, y, z, m, boundary="odw")
+    port.set_state(ref.state())
+    port.set_inflow(*inflow)
+    ref.boundary()
+    port.boundary()
+    b = 2
+    faces = [(slice(0, b), slice(b, -b), slice(b, -b)), (slice(-b, None), slice(b, -b), slice(b, -b)),
+             (slice(b, -b), slice(0, b), slice(b, -b)), (slice(b, -b), slice(-b, None), slice(b, -b)),
+             (slice(b, -b), slice(b, -b), slice(0, b)), (slice(b, -b), slice(b, -b), slice(-b, None))]
+    for f in ["P", "D", "U", "V", "W", "H", "Gamma", "T", "Yi"]:
+        r, p = ref.get(f), port.get(f)
+        for sl in faces:
+            assert n_unequal(p[(slice(None),) + sl], r[(slice(None),) + sl]) == 0, (f, sl)
+    ref.step(3, 2e-8)
+    port.step(3, 2e-8)
+    for f in ["CS", "T", "Nchem"]:
+        assert n_unequal(interior(port.get(f)), interior(ref.get(f))) == 0, f
