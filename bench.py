@@ -389,26 +389,31 @@ def znd_case(args, local, steps=1000, cells=4000, dx=25e-6):
                                                                  "recover_block": tuned["recover_block"]}}
 
 
-def odw_case(args, local, model, gate, grid=(1024, 512, 2), steps=2000):
-    """The 2-D oblique detonation case: 1024 x 512 x 2 nodes over the
-    reference's 2dODW extent (52.5 x 20 mm; the z spacing equals the x spacing),
+def odw_case(args, local, model, gate, grid=(1024, 512, 2), steps=2000, z_extent=None, phi_seed=None, cfl=CFL):
+    """The oblique detonation case. 2-D (default): 1024 x 512 x 2 nodes over the
+    reference's 2dODW extent (52.5 x 20 mm; the z spacing equals the x spacing).
+    3-D: 384 x 192 x 96 nodes over the 3dODW extent (52.5 x 20 x 20 mm) with the
+    equivalence ratio phi(z) of eu3d_cases.odw_phi on the inflow. Both:
     a Mach 7.5 stoichiometric H2-air freestream at 40 kPa / 293 K meeting a 25
     degree wedge (data/input-ODW.txt) in a wedge-aligned frame (the y-low face
     is the wedge surface), the reference's ODW ghost fill (EU_BC_ODW), the
-    learned + mixed step with each dt from the CFL rule at 0.5 on the device,
-    2000 steps. Reports the device throughput, the time advanced, the peak
-    temperature and the shock angle: where p first exceeds 1.5 x the
-    freestream pressure from the top down, fitted over the middle half of x,
-    plus the wedge angle (the oblique-shock relation gives about 32 degrees
-    for an ideal gas at gamma 1.4)."""
+    learned + mixed step with each dt from the CFL rule on the device, 2000
+    steps at CFL 0.5 in 2-D, 1000 steps at CFL 0.25 in 3-D (the reference's
+    forward-Euler MUSCL step goes non-finite at CFL 0.5 once the gas ignites
+    on grids as coarse as the 3-D one's, in the C restatement as well). Reports the device throughput, the time
+    advanced, the peak temperature and the shock angle in the middle z plane:
+    where p first exceeds 1.5 x the freestream pressure from the top down,
+    fitted over the middle half of x, plus the wedge angle (the oblique-shock
+    relation gives about 32 degrees for an ideal gas at gamma 1.4)."""
     ni, nj, nk = grid
     dx = 0.0525 / (ni - 1)
-    ext = (0.0, 0.0525, 0.0, 0.02, 0.0, dx * (nk - 1))
+    ext = (0.0, 0.0525, 0.0, 0.02, 0.0, dx * (nk - 1) if z_extent is None else z_extent)
     x = cases.node_coordinates(ni, ext[0], ext[1])
     y = cases.node_coordinates(nj, ext[2], ext[3])
     z = cases.node_coordinates(nk, ext[4], ext[5])
     mech = eu3d.parse_mechanism(cases.MECH_JA919, cases.THERMO)
-    prim, inflow = cases.odw(x, y, z, mech)
+    phi = cases.odw_phi(z, seed=phi_seed) if phi_seed is not None else None
+    prim, inflow = cases.odw(x, y, z, mech, phi=phi)
     p, cs, T, E = eu3d.initial_state(mech, ni, nj, nk, *prim)
     chem = "learned" if model is not None else "stiff"
     s = eu3d.Solver(ni, nj, nk, ext, precision="mixed", chemistry=chem, arith="fast", device=local, boundary="odw")
@@ -419,9 +424,9 @@ def odw_case(args, local, model, gate, grid=(1024, 512, 2), steps=2000):
         import learned
         learned.attach(s, model, gate)
     tuned = s.autotune(reps=3)
-    st, t_adv = s.step_cfl(steps, CFL)
-    pr = s.get("P")[0, 2:-2, 2:-2, 2]
-    t_end = s.get("T")[0, 2:-2, 2:-2, 2]
+    st, t_adv = s.step_cfl(steps, cfl)
+    pr = s.get("P")[0, 2:-2, 2:-2, 2 + nk // 2]  # the middle z plane
+    t_end = s.get("T")[0, 2:-2, 2:-2, :]
     s.close()
     p0 = eu3d.read_value(cases.INPUT_ODW, "P")
     angle = eu3d.read_value(cases.INPUT_ODW, "angle")
@@ -432,7 +437,7 @@ def odw_case(args, local, model, gate, grid=(1024, 512, 2), steps=2000):
             xs.append(x[2 + i])
             hs.append(y[2 + nj - 1 - hit[0]])
     beta = (math.degrees(math.atan(np.polyfit(xs, hs, 1)[0])) + angle) if len(xs) > 8 else None
-    return {"grid": list(grid), "steps": steps, "time_advanced_s": t_adv, "chemistry": chem,
+    return {"grid": list(grid), "steps": steps, "cfl": cfl, "time_advanced_s": t_adv, "chemistry": chem,
             "value": round(ni * nj * nk * steps / (st["device_ms"] / 1e3) / 1e6, 3), "unit": "Mcell-steps/s",
             "ms_per_step": round(st["device_ms"] / steps, 4), "peak_T_K": round(float(t_end.max()), 1),
             "peak_p_Pa": round(float(pr.max()), 1), "shock_angle_deg": None if beta is None else round(beta, 2),
@@ -757,7 +762,7 @@ def our_arm(args):
     batch = None
     if args.chem == "learned" and not args.no_batch:
         batch = batch_instances(args, model, gate, local, mech)
-    znd = odw = None
+    znd = odw = odw3 = None
     if not args.no_batch:
         try:
             znd = znd_case(args, local)
@@ -767,6 +772,11 @@ def our_arm(args):
             odw = odw_case(args, local, model, gate)
         except eu3d.EU3DError as e:
             odw = {"error": str(e)}
+        try:
+            odw3 = odw_case(args, local, model, gate, grid=(384, 192, 96), steps=1000, z_extent=0.02, phi_seed=4,
+                            cfl=0.25)
+        except eu3d.EU3DError as e:
+            odw3 = {"error": str(e)}
 
     # -- per-kernel times (same stream, CUDA events around each kernel phase) -----------------
     sp = make_solver(args.chem, args.precision, args.arith, profile=True)
@@ -834,6 +844,7 @@ def our_arm(args):
                 "mlp_roofline": mlp,
                 "znd_1d": znd,
                 "odw_2d": odw,
+                "odw_3d": odw3,
                 "roofline": roofline, "kernels_ms_per_step": per_kernel,
                 "max_nchem": stats["max_nchem"], "reacting_cells": stats["reacting"],
                 "learned_cells": stats["learned"], "fallback_cells": stats["fallback"],

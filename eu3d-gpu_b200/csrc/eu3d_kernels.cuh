@@ -954,6 +954,74 @@ __global__ void __launch_bounds__(128) k_react_queue(const __grid_constant__ Dev
     }
 }
 
+// Nchem routing of the learned mode: each active cell's Nchem is predicted
+// (Reaction::TrapezoidPrediction, src/Reaction.cpp:865-942); a cell needing at
+// most lp.min_nchem substeps takes the stiff kinetics here (its substeps cost
+// less than the model's evaluation and carry no model error), the others are
+// appended to the model's queue (lp.queue, length lp.counts[0]). With
+// lp.min_nchem <= 0 every active cell goes to the model unpredicted. A fixed
+// grid drains the active queue (length lp.counts[3], warp grabs on counts[4]).
+template <int NS, class Rt>
+__global__ void __launch_bounds__(128) k_learned_route(const __grid_constant__ DevMech m, const DevGrid g,
+                                                       const DevState st, LearnedParams lp,
+                                                       const double *__restrict__ dt_dev, int max_substeps)
+{
+    const int nq = *(volatile int *)(lp.counts + 3);
+    if (nq == 0)
+        return;
+    const int lane = threadIdx.x & 31;
+    const long long n3 = g.n3;
+    for (;;) {
+        int base = 0;
+        if (lane == 0)
+            base = atomicAdd(lp.counts + 4, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= nq)
+            break;
+        const int q = base + lane;
+        bool to_model = false;
+        long long c = 0;
+        if (q < nq) {
+            c = lp.active[q];
+            to_model = true;
+            if (lp.min_nchem > 0) {
+                CellState<NS> cell;
+                load_recovered<NS>(st, n3, c, cell);
+                double mc[NS];
+                SpeciesRates<NS> rates;
+                const double dtm = *dt_dev;
+                const int nchem = predict_nchem<NS, Rt>(m, cell, dtm, max_substeps, st.counters, mc, rates);
+                if (nchem <= lp.min_nchem) {
+                    to_model = false;
+#ifdef EU_HEAVY_QUEUE
+                    if (st.heavy && nchem > kHeavyNchem) {
+                        push_heavy(st.heavy, c);
+                    } else
+#endif
+                    {
+                        count_nchem(st.counters, nchem);
+                        run_substeps<NS, Rt>(m, cell, dtm, nchem, mc, rates, st.cms ? st.cms + c : nullptr, n3);
+                        st.nchem[c] = nchem;
+                        store_cell<NS>(m, st, n3, c, cell);
+                    }
+                }
+            }
+        }
+        const unsigned routed = __ballot_sync(0xffffffffu, q < nq && !to_model);
+        if (routed && lane == __ffs(routed) - 1)
+            atomicAdd(&st.counters[kCntRouted], (unsigned long long)__popc(routed));
+        const unsigned mask = __ballot_sync(0xffffffffu, to_model);
+        if (mask) {
+            int at = 0;
+            if (lane == __ffs(mask) - 1)
+                at = atomicAdd(&lp.counts[0], __popc(mask));
+            at = __shfl_sync(0xffffffffu, at, __ffs(mask) - 1);
+            if (to_model)
+                lp.queue[at + __popc(mask & ((1u << lane) - 1))] = int(c);
+        }
+    }
+}
+
 // ------------------------------------------------- warp-per-cell kinetics
 // The same kinetics as react_cell (prediction, Nchem trapezoid substeps,
 // state rebuild after each) with one warp per cell: lane r evaluates reaction

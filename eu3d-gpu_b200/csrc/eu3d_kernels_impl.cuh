@@ -164,6 +164,18 @@ cudaError_t react_queue_t(const LaunchArgs &a, const int *queue, int *count, int
 }
 
 template <int NS, int NR>
+cudaError_t route_t(const LaunchArgs &a, const LearnedParams &lp)
+{
+    const dim3 grid(queue_grid(a, 4));
+    if (a.spec == 1 && NS == Mech_JA919::NS && NR == Mech_JA919::NR)
+        k_learned_route<NS, Mech_JA919><<<grid, 128, 0, a.stream>>>(*a.mech, a.g, a.st, lp, a.dt_dev, a.max_substeps);
+    else
+        k_learned_route<NS, TableRates<NS, NR>><<<grid, 128, 0, a.stream>>>(*a.mech, a.g, a.st, lp, a.dt_dev,
+                                                                            a.max_substeps);
+    return cudaGetLastError();
+}
+
+template <int NS, int NR>
 cudaError_t state_from_tpy_t(const LaunchArgs &a, long long n, const double *T, const double *p, const double *Y,
                              double *cs, double *E)
 {
@@ -225,6 +237,7 @@ cudaError_t launch_to_f32(const double *src, float *dst, long long n, cudaStream
 cudaError_t launch_recover_classify(const LaunchArgs &a, const LearnedParams &lp) { EU3D_DISPATCH(classify_t, a, lp) }
 cudaError_t launch_learned_features(const LaunchArgs &a, const LearnedParams &lp) { EU3D_DISPATCH(features_t, a, lp) }
 cudaError_t launch_learned_apply(const LaunchArgs &a, const LearnedParams &lp) { EU3D_DISPATCH(apply_t, a, lp) }
+cudaError_t launch_learned_route(const LaunchArgs &a, const LearnedParams &lp) { EU3D_DISPATCH(route_t, a, lp) }
 cudaError_t launch_react_queue(const LaunchArgs &a, const int *queue, int *count, int counter)
 {
     EU3D_DISPATCH(react_queue_t, a, queue, count, counter)
@@ -284,7 +297,7 @@ cudaError_t launch_set_value(double *dst, double v, cudaStream_t s)
 const Launchers launchers = {&launch_boundary,         &launch_flux_update,      &launch_recover_react,
                              &launch_derived,          &launch_recover_classify, &launch_learned_features,
                              &launch_learned_apply,    &launch_react_queue,      &launch_react_heavy,
-                             &launch_materialize};
+                             &launch_materialize,      &launch_learned_route};
 
 #undef EU3D_DISPATCH
 

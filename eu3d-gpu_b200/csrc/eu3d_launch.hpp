@@ -39,6 +39,7 @@ struct Launchers {
     cudaError_t (*react_queue)(const LaunchArgs &a, const int *queue, int *count, int counter);
     cudaError_t (*react_heavy)(const LaunchArgs &a, int blocks);
     cudaError_t (*materialize)(const LaunchArgs &a);
+    cudaError_t (*learned_route)(const LaunchArgs &a, const LearnedParams &lp);
 };
 
 #define EU3D_DECLARE_LAUNCHERS(NSP)                                                                \
@@ -52,6 +53,7 @@ struct Launchers {
     cudaError_t launch_recover_classify(const LaunchArgs &a, const LearnedParams &lp);             \
     cudaError_t launch_learned_features(const LaunchArgs &a, const LearnedParams &lp);             \
     cudaError_t launch_learned_apply(const LaunchArgs &a, const LearnedParams &lp);                \
+    cudaError_t launch_learned_route(const LaunchArgs &a, const LearnedParams &lp);                \
     cudaError_t launch_react_queue(const LaunchArgs &a, const int *queue, int *count, int counter); \
     cudaError_t launch_state_from_tpy(const LaunchArgs &a, long long n, const double *T,           \
                                       const double *p, const double *Y, double *cs, double *E);    \

@@ -83,9 +83,10 @@ enum CounterIdx {
     kCntReacting = 2,
     kCntLearned = 3,
     kCntFallback = 4,
-    kCntPerStep = 5,
-    kCntNonfinite = 5,
-    kCntBadNchem = 6,
+    kCntRouted = 5, // learned mode: active cells the Nchem routing gave to the stiff kinetics
+    kCntPerStep = 6,
+    kCntNonfinite = 6,
+    kCntBadNchem = 7,
     kCntCount = 8
 };
 
@@ -93,8 +94,11 @@ enum CounterIdx {
 struct LearnedParams {
     float *feat;           // [queue capacity x (3 + NS)] fp32 model inputs
     float *pred;           // [members x queue length x (NS + 1)] fp32 physical outputs
-    int *queue, *fallback; // cell indices
-    int *counts;           // [0] learned queue length, [1] fallback queue length, [2] fallback cells taken
+    int *queue, *fallback; // cell indices: the model's queue, the gate's rejections
+    int *active;           // cells with chemistry to do (recovery's output, before the Nchem routing)
+    int *counts;           // [0] model queue length, [1] fallback queue length, [2] fallback cells taken,
+                           // [3] active cells, [4] active cells taken by the routing
+    int min_nchem;         // predicted Nchem <= this: stiff kinetics right away (0: all to the model)
     long long pred_row, pred_mem; // ensemble output o of member e for queue row q: pred[q pred_row + e pred_mem + o]
     int members;
     double frozen_y;       // a cell whose non-inert mass fraction is below this is frozen

@@ -49,7 +49,7 @@ class MechanismC(ctypes.Structure):
 
 class LearnedConfig(ctypes.Structure):
     _fields_ = [("tau", _D), ("frozen_y", _D), ("frozen_T", _D), ("frozen_radical", _D), ("box_lo", _P),
-                ("box_hi", _P), ("out_scale", _P), ("out_eps", _P), ("out_bound", _P)]
+                ("box_hi", _P), ("out_scale", _P), ("out_eps", _P), ("out_bound", _P), ("min_nchem", _I)]
 
 
 class TuneReport(ctypes.Structure):
@@ -70,7 +70,8 @@ class TuneReport(ctypes.Structure):
 class StepStats(ctypes.Structure):
     _fields_ = [("steps", _I), ("max_nchem", _I), ("sum_nchem", ctypes.c_longlong),
                 ("reacting", ctypes.c_longlong), ("learned", ctypes.c_longlong), ("fallback", ctypes.c_longlong),
-                ("nonfinite", ctypes.c_longlong), ("device_ms", _D), ("phase_ms", _D * 4), ("launches", _I)]
+                ("nonfinite", ctypes.c_longlong), ("device_ms", _D), ("phase_ms", _D * 4), ("launches", _I),
+                ("routed", ctypes.c_longlong)]
 
     def as_dict(self):
         d = {f: getattr(self, f) for f, _ in self._fields_}
@@ -367,12 +368,14 @@ class Solver:
                                               None if nchem is None else nchem.data_ptr()), "chem_advance")
 
     def set_learned(self, model, tau, box_lo, box_hi, out_scale, frozen_y=1e-9, frozen_T=0.0,
-                    frozen_radical=1e-9, out_eps=None, out_bound=None):
+                    frozen_radical=1e-9, out_eps=None, out_bound=None, min_nchem=0):
+        """min_nchem: active cells predicted to need at most this many substeps
+        take the stiff kinetics directly (0: all active cells to the model)."""
         keep = [np.ascontiguousarray(v, dtype=np.float64) for v in (box_lo, box_hi, out_scale)]
         keep += [None if v is None else np.ascontiguousarray(v, dtype=np.float64) for v in (out_eps, out_bound)]
         self._learned_keep = keep
         cfg = LearnedConfig(float(tau), float(frozen_y), float(frozen_T), float(frozen_radical),
-                            *[None if v is None else v.ctypes.data for v in keep])
+                            *[None if v is None else v.ctypes.data for v in keep], int(min_nchem))
         self._model = model
         self._check(library().eu_set_learned(self.h, model.h, ctypes.byref(cfg)), "set_learned")
 

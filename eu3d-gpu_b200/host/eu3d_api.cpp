@@ -751,10 +751,17 @@ eu_status learned_chemistry(eu_handle *h, const LaunchArgs &a, const Launchers &
 {
     LearnedParams lp = h->lp;
     const int ns = h->mech.ns;
-    CK(h, cudaMemsetAsync(lp.counts, 0, 3 * sizeof(int), h->stream));
-    CK(h, L.recover_classify(a, lp));
+    CK(h, cudaMemsetAsync(lp.counts, 0, 5 * sizeof(int), h->stream));
+    // recovery appends the active cells to lp.active (length counts[3]); the
+    // routing sends the ones needing few substeps to the stiff kinetics and
+    // the rest to the model's queue (lp.queue, length counts[0])
+    LearnedParams lpa = lp;
+    lpa.queue = lp.active;
+    lpa.counts = lp.counts + 3;
+    CK(h, L.recover_classify(a, lpa));
+    CK(h, L.learned_route(a, lp));
     CK(h, L.learned_features(a, lp));
-    *launches += 2;
+    *launches += 3;
     if (mlp_has_fused(h->model)) {
         lp.pred_row = (long long)lp.members * (ns + 1);
         lp.pred_mem = ns + 1;
@@ -909,13 +916,15 @@ eu_status eu_set_learned(eu_handle *h, eu_mlp *model, const eu_learned_config *l
         if ((s = dalloc(h, &lp.pred, size_t(cap) * members * (ns + 1))) != EU_OK) return s;
         if ((s = dalloc(h, &lp.queue, size_t(cap))) != EU_OK) return s;
         if ((s = dalloc(h, &lp.fallback, size_t(cap))) != EU_OK) return s;
-        if ((s = dalloc(h, &lp.counts, size_t(3))) != EU_OK) return s;
+        if ((s = dalloc(h, &lp.active, size_t(cap))) != EU_OK) return s;
+        if ((s = dalloc(h, &lp.counts, size_t(5))) != EU_OK) return s;
         h->lp_capacity = cap;
     }
     if (!h->h_counts)
         CK(h, cudaMallocHost(&h->h_counts, 2 * sizeof(int)));
     lp.members = members;
     lp.tau = lc->tau;
+    lp.min_nchem = lc->min_nchem;
     lp.frozen_y = lc->frozen_y;
     lp.frozen_T = lc->frozen_T;
     lp.frozen_radical = lc->frozen_radical;
@@ -1111,7 +1120,7 @@ eu_status step_impl(eu_handle *h, int nsteps, double dt, double cfl, eu_step_sta
     CK(h, cudaMemcpyAsync(cnt, h->st.counters, sizeof cnt, cudaMemcpyDeviceToHost, h->stream));
     int queued = 0, model_err = 0;
     if (learned && nsteps > 0) {
-        CK(h, cudaMemcpyAsync(&queued, h->lp.counts, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaMemcpyAsync(&queued, h->lp.counts + 3, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
         CK(h, cudaMemcpyAsync(&model_err, mlp_error_flag(h->model), sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     }
     CK(h, cudaStreamSynchronize(h->stream));
@@ -1124,6 +1133,7 @@ eu_status step_impl(eu_handle *h, int nsteps, double dt, double cfl, eu_step_sta
     stats->reacting = react ? (long long)h->ni * h->nj * h->nk : queued;
     stats->learned = (long long)cnt[kCntLearned];
     stats->fallback = (long long)cnt[kCntFallback];
+    stats->routed = (long long)cnt[kCntRouted];
     stats->nonfinite = (long long)cnt[kCntNonfinite];
     stats->device_ms = ms;
     stats->launches = launches;
@@ -1553,7 +1563,7 @@ eu_status eu_batch_step(eu_batch *b, int nsteps, const double *dt, eu_step_stats
         BCK(b, cudaMemcpyAsync(&cnt[size_t(i) * kCntCount], h->st.counters, kCntCount * sizeof(unsigned long long),
                                cudaMemcpyDeviceToHost, b->stream));
         if (h->cfg.chemistry == EU_CHEM_LEARNED && nsteps > 0) {
-            BCK(b, cudaMemcpyAsync(&queued[i], h->lp.counts, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+            BCK(b, cudaMemcpyAsync(&queued[i], h->lp.counts + 3, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
             BCK(b, cudaMemcpyAsync(&model_err[i], mlp_error_flag(h->model), sizeof(int), cudaMemcpyDeviceToHost,
                                    b->stream));
         }
@@ -1576,6 +1586,7 @@ eu_status eu_batch_step(eu_batch *b, int nsteps, const double *dt, eu_step_stats
             st.reacting = h->cfg.chemistry == EU_CHEM_STIFF ? (long long)h->ni * h->nj * h->nk : queued[i];
             st.learned = (long long)c[kCntLearned];
             st.fallback = (long long)c[kCntFallback];
+            st.routed = (long long)c[kCntRouted];
             st.nonfinite = (long long)c[kCntNonfinite];
             st.device_ms = ms;
             st.launches = nsteps * h->graph_launches;

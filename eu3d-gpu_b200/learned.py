@@ -39,6 +39,13 @@ OUT_EPS = np.array([1e-6] * N_SPECIES + [1e-2])
 # kinetics: along the stiff integrator's own trajectories the largest one-step
 # change of any mass fraction below 800 K was 1.5e-10 (700-800 K band).
 FROZEN_T, FROZEN_RADICAL, FROZEN_Y = 800.0, 1e-9, 1e-9
+# Active cells predicted to need at most this many substeps take the stiff
+# kinetics: a substep costs ~6 kflop in FP64 (1.4 ns a cell on a B200), the
+# ensemble 0.82 MFLOP in BF16 (3.6 ns at its measured rate), so the model pays
+# from about three substeps up; below that it would only add its error (in an
+# induction zone the error of many cheap cells adds up: on the oblique
+# detonation case it brought the ignition forward by ~2 us).
+MIN_NCHEM = 4
 RADICALS = (0, 1, 3, 6, 7)  # H, O, OH, H2O2, HO2 in H2_JA919's species order
 WIDTH, HIDDEN, MEMBERS = 256, 3, 3
 S_O2, S_H2, S_N2 = cases.S_O2, cases.S_H2, cases.S_N2
@@ -225,6 +232,7 @@ def load(path=CHECKPOINT, device=0):
             "out_bound": z["out_bound"] if "out_bound" in z.files else None}
     fz = z["frozen"] if "frozen" in z.files else np.array([FROZEN_Y, FROZEN_T, FROZEN_RADICAL])
     gate.update(frozen_y=float(fz[0]), frozen_T=float(fz[1]), frozen_radical=float(fz[2]))
+    gate["min_nchem"] = int(z["min_nchem"]) if "min_nchem" in z.files else MIN_NCHEM
     return m, gate
 
 
@@ -232,7 +240,7 @@ def attach(solver, model, gate):
     """Install a loaded model and its gate on a solver handle."""
     solver.set_learned(model, gate["tau"], gate["box_lo"], gate["box_hi"], gate["out_scale"],
                        frozen_y=gate["frozen_y"], frozen_T=gate["frozen_T"], frozen_radical=gate["frozen_radical"],
-                       out_eps=gate["out_eps"], out_bound=gate["out_bound"])
+                       out_eps=gate["out_eps"], out_bound=gate["out_bound"], min_nchem=gate.get("min_nchem", 0))
 
 
 def front_check(model, gate, steps=20, dt=2e-8, grid=(40, 16, 16), device=0):

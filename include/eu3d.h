@@ -134,6 +134,8 @@ typedef struct {
     double device_ms;       /* device time of the call (CUDA events) */
     double phase_ms[4];     /* with cfg.profile: ghost fill, flux + update, recovery + kinetics, other */
     int launches;           /* kernels launched by the call */
+    long long routed;       /* EU_CHEM_LEARNED: active cells whose predicted Nchem sent them to the
+                               stiff kinetics (eu_learned_config.min_nchem), last step */
 } eu_step_stats;
 
 /* Library version / ABI check. */
@@ -375,6 +377,11 @@ typedef struct {
     const double *out_scale; /* [ns + 1] */
     const double *out_eps;   /* [ns + 1], NULL: linear outputs */
     const double *out_bound; /* [ns + 1], NULL: no output range check */
+    int min_nchem;           /* active cells whose predicted Nchem (Reaction::TrapezoidPrediction,
+                                src/Reaction.cpp:865-942) is at most this take the stiff kinetics
+                                directly; the model sees the rest. 0: every active cell goes to the
+                                model. A substep costs ~6 kflop in FP64, the model 0.82 MFLOP in
+                                BF16, so the model pays only on cells that need several substeps */
 } eu_learned_config;
 
 eu_status eu_set_learned(eu_handle *h, eu_mlp *model, const eu_learned_config *cfg);

@@ -105,20 +105,22 @@ def test_trained_model_replaces_stiff_substeps(gpu):
     kinetics' own substeps (the same FP64 arithmetic). The gate is tight (tau
     calibrated for a mean species L1 of 5e-6 per step, then halved until the
     reaction front of an igniting validation block does not move), so on this
-    block of hot reacting gas it takes about 2 % of the cells. The
-    species error (mean over cells of sum_s |dY_s| against the stiff step)
-    stays within 1e-4."""
+    block of hot reacting gas it takes about 2 % of the cells. Here every
+    active cell goes to the model (min_nchem 0): on this block each cell needs
+    one substep, so the default Nchem routing (learned.MIN_NCHEM) would give
+    them all to the stiff kinetics and the model none. The species error (mean
+    over cells of sum_s |dY_s| against the stiff step) stays within 1e-4."""
     import learned
     dt = 5e-8
     a = hot_mixture(gpu, "stiff")
     b = hot_mixture(gpu, "learned")
     model, gate = learned.load()
-    learned.attach(b, model, gate)
+    learned.attach(b, model, dict(gate, min_nchem=0))
     sa = a.step(1, dt)
     sb = b.step(1, dt)
     n = 24 * 8 * 8
     assert sa["reacting"] == n and sb["reacting"] == n
-    assert sb["learned"] + sb["fallback"] == n
+    assert sb["learned"] + sb["fallback"] == n and sb["routed"] == 0, sb
     assert sb["learned"] >= 0.005 * n, sb
     assert sb["sum_nchem"] <= sa["sum_nchem"] - sb["learned"], (sa["sum_nchem"], sb["sum_nchem"], sb["learned"])
     ya, yb = interior(a.get("Yi")), interior(b.get("Yi"))
@@ -226,3 +228,27 @@ def test_learned_front_within_one_cell(gpu):
     assert max(cases.front_shift(a, b) for a, b in zip(ys["learned"], ys["stiff"])) <= 1
     l1 = np.abs(interior(ys["learned"][-1]) - interior(ys["stiff"][-1])).sum(axis=0)
     assert l1.mean() <= 1e-3, l1.mean()
+
+
+def test_nchem_routing_sends_cheap_cells_to_the_stiff_kinetics(gpu):
+    """With min_nchem above every cell's predicted Nchem the learned step is
+    the stiff step: no cell reaches the model, and the state is bitwise that of
+    the mixed-precision stiff step (the same prediction, substeps and state
+    rebuild). With min_nchem 0 every active cell goes to the model."""
+    import learned
+    dt = 2e-8
+    model, gate = learned.load()
+    a = hot_mixture(gpu, "stiff")
+    b = hot_mixture(gpu, "learned")
+    c = hot_mixture(gpu, "learned")
+    learned.attach(b, model, dict(gate, min_nchem=1 << 20))
+    learned.attach(c, model, dict(gate, min_nchem=0))
+    sa, sb, sc = a.step(2, dt), b.step(2, dt), c.step(2, dt)
+    n = 24 * 8 * 8
+    assert sb["routed"] == n and sb["learned"] == 0 and sb["fallback"] == 0, sb
+    assert sb["sum_nchem"] == sa["sum_nchem"] and sb["max_nchem"] == sa["max_nchem"]
+    for f in ("CS", "T", "Yi"):
+        assert n_unequal(a.get(f), b.get(f)) == 0, f
+    assert sc["routed"] == 0 and sc["learned"] + sc["fallback"] == n, sc
+    for s in (a, b, c):
+        s.close()
