@@ -68,8 +68,9 @@ def _initial_compositions(rng, n, mw):
 
 
 def generate(solver, n_traj, n_steps, seed=11, t_range=(300.0, 3500.0), p_range=(5e4, 5e6), dt_range=(1e-9, 3e-7),
-             max_substeps=20000):
-    """(inputs, targets) as torch CUDA fp32 tensors, up to n_traj * n_steps rows.
+             max_substeps=20000, with_nchem=False):
+    """(inputs, targets) as torch CUDA fp32 tensors, up to n_traj * n_steps rows
+    (with_nchem: and each row's Nchem, the stiff kinetics' substeps for it).
 
     A trajectory is dropped from the first step that leaves the physical
     range: more than max_substeps substeps (the solver handle's cap), a
@@ -96,6 +97,7 @@ def generate(solver, n_traj, n_steps, seed=11, t_range=(300.0, 3500.0), p_range=
     X = torch.empty(n_traj * n_steps, ns + 3, device=dev, dtype=torch.float32)
     Tg = torch.empty(n_traj * n_steps, ns + 1, device=dev, dtype=torch.float32)
     keep = torch.zeros(n_traj * n_steps, device=dev, dtype=torch.bool)
+    Ng = torch.zeros(n_traj * n_steps, device=dev, dtype=torch.int32)
     alive = torch.ones(n_traj, device=dev, dtype=torch.bool)
     nchem = torch.zeros(n_traj, device=dev, dtype=torch.int32)
     for k in range(n_steps):
@@ -115,8 +117,11 @@ def generate(solver, n_traj, n_steps, seed=11, t_range=(300.0, 3500.0), p_range=
         alive &= (nchem > 0) & (nchem < max_substeps) & torch.isfinite(T) & (T > 250.0) & (T < 4500.0)
         alive &= (Y_after.min(0).values > -1e-8) & ((Y_after - Y_before).abs().max(0).values < 0.5)
         keep[rows] = alive
+        Ng[rows] = nchem
         Tg[rows, :ns] = (Y_after - Y_before).T.float()
         Tg[rows, ns] = (T - T_before).float()
+    if with_nchem:
+        return X[keep].contiguous(), Tg[keep].contiguous(), Ng[keep].contiguous()
     return X[keep].contiguous(), Tg[keep].contiguous()
 
 
@@ -217,7 +222,8 @@ def save(path, model, scaling, gate, meta=None):
     np.savez(path, params=model.get_params(), shape=np.array([N_IN, WIDTH, HIDDEN, N_OUT, MEMBERS]),
              **scaling, tau=gate["tau"], box_lo=gate["box_lo"], box_hi=gate["box_hi"], out_eps=gate["out_eps"],
              out_bound=gate["out_bound"],
-             frozen=np.array([FROZEN_Y, FROZEN_T, FROZEN_RADICAL]), meta=np.array(repr(meta or {})))
+             frozen=np.array([FROZEN_Y, FROZEN_T, FROZEN_RADICAL]), min_nchem=np.array(gate.get("min_nchem", 0)),
+             meta=np.array(repr(meta or {})))
 
 
 def load(path=CHECKPOINT, device=0):

@@ -53,6 +53,11 @@ def main():
     ap.add_argument("--front-only", action="store_true",
                     help="keep the checkpoint's weights and gate; only tighten tau for the front criterion")
     ap.add_argument("--max-shift", type=int, default=0, help="largest reaction-front shift (cells) the gate may cause")
+    ap.add_argument("--rows-min-nchem", type=int, default=0,
+                    help="train and calibrate only on rows whose Nchem exceeds this (0: every active row). "
+                         "With 4 (the rows the default Nchem routing hands to the model) 0.69 M rows remain and "
+                         "the gate accepts 1.5e-5 of them at the L1 target: the network does not reach the "
+                         "per-step accuracy on stiff rows")
     args = ap.parse_args()
     if args.front_only:
         return front_only(args)
@@ -62,9 +67,9 @@ def main():
     t0 = time.time()
     s = eu3d.Solver(5, 5, 5, (0, 1, 0, 1, 0, 1), max_substeps=20000)
     s.load_mechanism(cases.MECH_JA919, cases.THERMO)
-    X, T = learned.generate(s, args.traj, args.steps_per_traj, seed=args.seed)
+    X, T, N = learned.generate(s, args.traj, args.steps_per_traj, seed=args.seed, with_nchem=True)
     s.close()
-    act = learned.active_rows(X)
+    act = learned.active_rows(X) & (N > args.rows_min_nchem)
     X, T = X[act].contiguous(), T[act].contiguous()
     n = X.shape[0]
     g = torch.Generator(device="cuda")
@@ -81,7 +86,9 @@ def main():
     print(f"trained in {time.time() - t1:.1f} s", flush=True)
     gate = learned.calibrate(model, scaling, X[va].contiguous(), T[va].contiguous(), target=args.target,
                              bound=bound)
+    gate["min_nchem"] = learned.MIN_NCHEM  # the routing the checkpoint is used with
     meta = {"traj": args.traj, "steps_per_traj": args.steps_per_traj, "train_steps": args.train_steps,
+            "rows_min_nchem": args.rows_min_nchem,
             "batch": args.batch, "lr": args.lr, "seed": args.seed, "samples": n,
             "accepted_fraction": gate["accepted_fraction"], "l1_accepted": gate["l1_accepted"], "tau": gate["tau"]}
     learned.save(args.out, model, scaling, gate, meta)

@@ -149,12 +149,12 @@ def test_graph_replay_equals_eager_launches(gpu, chemistry, precision):
         s.set_mechanism(mech)
         s.set_primitive(*prim)
         stats = []
-        if chemistry == "learned":
+        if chemistry == "learned":  # every active cell to the model, so it runs inside the graph
             model, gate = learned.load()
-            learned.attach(s, model, gate)
+            learned.attach(s, model, dict(gate, min_nchem=0))
         stats.append(s.step(3, 2e-8))
         if chemistry == "learned":
-            learned.attach(s, model, dict(gate, tau=gate["tau"] * 3))
+            learned.attach(s, model, dict(gate, tau=gate["tau"] * 3, min_nchem=0))
         stats.append(s.step(2, 2e-8))
         keep = ("max_nchem", "sum_nchem", "reacting", "learned", "fallback", "launches")
         out[graphs] = ([{k: st[k] for k in keep} for st in stats], s.get("CS"), s.get("T"), s.get("Yi"))
@@ -182,8 +182,8 @@ def test_batch_of_uneven_instances_equals_one_by_one(gpu):
                            precision=prec, arith="fast")
             s.set_mechanism(mech)
             s.set_primitive(*cases.hot_reacting_block(ni + 4, nj + 4, nk + 4, mech["mw"], mech["ns"]))
-            if chem == "learned":
-                learned.attach(s, model, gate)
+            if chem == "learned":  # every active cell to the model
+                learned.attach(s, model, dict(gate, min_nchem=0))
             out.append(s)
         return out
 
