@@ -272,6 +272,71 @@ __global__ void __launch_bounds__(kFluxTK *kFluxTJ, 1)
     }
 }
 
+// Flux divergence and update for grids thin in z (nk below half a warp),
+// where the (j, k) tiles of the kernels above and below would leave most lanes
+// idle: one thread per (j, k) column (flattened, k fastest) marching ci nodes
+// in x. The x face at i-1/2 is carried in registers from the previous node; the
+// thread forms the y and z faces on both sides of its cell from the stencil in
+// global memory (each interior y or z face twice, once by each of its cells).
+// The RHS is formed in the same order as the other flux kernels (FP32
+// differences and sum onto the FP64 conserved value for R = float, FP64 for
+// R = double).
+template <int NS, typename R, bool kStrict>
+__global__ void __launch_bounds__(128) k_flux_update_cols(const DevGrid g, const DevState st,
+                                                          const R *__restrict__ prim,
+                                                          const double *__restrict__ dt_dev, int ci)
+{
+    constexpr int NV = NS + 4;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.nj * g.nk)
+        return;
+    const int jj = t / g.nk;
+    const int j = g.bc + jj, k = g.bc + (t - jj * g.nk);
+    const int i_begin = g.bc + blockIdx.y * ci;
+    const int i_end = min(i_begin + ci, g.bc + g.ni);
+    const long long n3 = g.n3, sx = (long long)g.ny * g.nz, sy = g.nz;
+    const double dt = *dt_dev;
+    const double cy = dt / (g.y[j] - g.y[j - 1]);
+    const double cz = dt / (g.z[k] - g.z[k - 1]);
+    R Fm[NV];
+    face_flux<NS, 0, R, kStrict>(prim, n3, cell_index(g, i_begin - 1, j, k), sx, Fm);
+    for (int i = i_begin; i < i_end; ++i) {
+        const long long c = cell_index(g, i, j, k);
+        const double cx = -dt / (g.x[i] - g.x[i - 1]);
+        R Fp[NV], A[NV], B[NV];
+        face_flux<NS, 0, R, kStrict>(prim, n3, c, sx, Fp);
+        face_flux<NS, 1, R, kStrict>(prim, n3, c, sy, A);      // y face above
+        face_flux<NS, 1, R, kStrict>(prim, n3, c - sy, sy, B); // y face below
+        if (sizeof(R) == 4) {
+            const float cx32 = float(cx), cy32 = float(cy), cz32 = float(cz);
+            float rhs[NV];
+#pragma unroll
+            for (int q = 0; q < NV; ++q) rhs[q] = cx32 * float(Fp[q] - Fm[q]) - cy32 * float(A[q] - B[q]);
+            face_flux<NS, 2, R, kStrict>(prim, n3, c, 1, A);     // z face right
+            face_flux<NS, 2, R, kStrict>(prim, n3, c - 1, 1, B); // z face left
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
+                const float r = rhs[q] - cz32 * float(A[q] - B[q]);
+                st.cs[q * n3 + c] = st.cs[q * n3 + c] + double(r);
+                Fm[q] = Fp[q];
+            }
+        } else {
+            double rhs[NV];
+#pragma unroll
+            for (int q = 0; q < NV; ++q)
+                rhs[q] = cx * (double(Fp[q]) - double(Fm[q])) - cy * (double(A[q]) - double(B[q]));
+            face_flux<NS, 2, R, kStrict>(prim, n3, c, 1, A);
+            face_flux<NS, 2, R, kStrict>(prim, n3, c - 1, 1, B);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
+                const double r = rhs[q] - cz * (double(A[q]) - double(B[q]));
+                st.cs[q * n3 + c] = st.cs[q * n3 + c] + r;
+                Fm[q] = Fp[q];
+            }
+        }
+    }
+}
+
 // Plane-tiled flux divergence and update: the same faces, arithmetic and RHS
 // order as k_flux_update (bitwise the same result), with every primitive read
 // from HBM once per plane instead of once per stencil point, and the loads of

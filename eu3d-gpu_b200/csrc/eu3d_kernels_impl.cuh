@@ -68,9 +68,27 @@ cudaError_t tiled_flux_launch(const LaunchArgs &a, const R *prim)
     return cudaGetLastError();
 }
 
+// Grids thin in z: one thread per (j, k) column.
+constexpr int kThinNk = 16;
+
+template <int NS, typename R, bool kStrict>
+cudaError_t cols_flux_launch(const LaunchArgs &a, const R *prim)
+{
+    const DevGrid &g = a.g;
+    const int ci = a.flux_ci > 0 ? a.flux_ci : 16;
+    const dim3 grid(unsigned((g.nj * g.nk + 127) / 128), unsigned((g.ni + ci - 1) / ci));
+    k_flux_update_cols<NS, R, kStrict><<<grid, 128, 0, a.stream>>>(g, a.st, prim, a.dt_dev, ci);
+    return cudaGetLastError();
+}
+
 template <int NS, int NR>
 cudaError_t flux_t(const LaunchArgs &a)
 {
+    if (a.g.nk < kThinNk) {
+        if (a.precision == 1)
+            return cols_flux_launch<NS, float, false>(a, a.st.prim32);
+        return cols_flux_launch<NS, double, kStrictFlux>(a, a.st.prim);
+    }
     // mixed precision: FP32 reconstruction and AUSM (always the division-light
     // forms), plane-tiled
     if (a.precision == 1)

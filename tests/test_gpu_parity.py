@@ -116,11 +116,12 @@ def test_mixed_precision_error_is_bounded(gpu):
     assert rel_linf(interior(b.get("CS")), interior(a.get("CS"))).max() <= 1e-3
 
 
-@pytest.mark.parametrize("dims", [(40, 20, 45), (17, 7, 32), (17, 8, 32)])
+@pytest.mark.parametrize("dims", [(40, 20, 45), (17, 7, 32), (17, 8, 32), (33, 9, 5)])
 def test_mixed_precision_tiles_match_fp64_closely(gpu, dims):
     """The plane-tiled FP32 flux kernel on grids whose (j, k) extent is not a
     multiple of its 7 x 32 tile, on one that is exactly one tile, and on one
-    with a single row in its second tile: after
+    with a single row in its second tile, and the one-thread-per-column kernel
+    of grids thin in z (nk < 16, both precisions): after
     two steps the conserved state stays within 2e-6 of the all-FP64 run, each
     error measured against the scale of its quantity (species partial
     densities against the largest density, momentum components against the
