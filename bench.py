@@ -629,17 +629,17 @@ def our_arm_blocks(args, world, rank, local, dist):
     # end to end through the public API with host buffers (state up once, the
     # exchanged steps each synchronous, the conserved state down at the end)
     pinned = {}
-    for k, v in sd.items():
-        t = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)
-        t.numpy()[...] = v
+    for k in ("CS", "T", "E"):
+        t = torch.empty(sd[k].shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = sd[k]
         pinned[k] = t.numpy()
     cs_host = torch.empty(sd["CS"].shape, dtype=torch.float64, pin_memory=True).numpy()
-    se = make(args.chem, args.precision, args.arith, state=pinned)
+    se = make(args.chem, args.precision, args.arith)
     se.step(args.warmup, dt, stats=False)
     se.sync()
     barrier(dist, device)
     t0 = time.perf_counter()
-    se.set_state(pinned)
+    se.set_conserved(pinned["CS"], pinned["T"], pinned["E"])
     for _ in range(args.steps):
         se.step(1, dt, stats=True)
     cs_out = se.get("CS", out=cs_host)
@@ -801,18 +801,20 @@ def our_arm(args):
                 "dominant_share": round(phase[dominant] / max(sum(phase[:3]), 1e-9), 3)}
 
     # -- end to end through the public API with host buffers ----------------------------------
+    # the conserved state (CS, T, E) is what a step needs; eu_set_conserved forms
+    # the primitives on the device as the step's recovery does
     pinned = {}
-    for k, v in sd.items():
-        t = torch.empty(v.shape, dtype=torch.float64, pin_memory=True)
-        t.numpy()[...] = v
+    for k in ("CS", "T", "E"):
+        t = torch.empty(sd[k].shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = sd[k]
         pinned[k] = t.numpy()
     cs_host = torch.empty(sd["CS"].shape, dtype=torch.float64, pin_memory=True).numpy()
-    se = make_solver(args.chem, args.precision, args.arith, state=pinned)
+    se = make_solver(args.chem, args.precision, args.arith)
     se.step(args.warmup, dt)
     barrier(dist, device)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    se.set_state(pinned)
+    se.set_conserved(pinned["CS"], pinned["T"], pinned["E"])
     for _ in range(args.steps):
         se.step(1, dt)  # synchronous: reads the step's health counters back
     cs = se.get("CS", out=cs_host)

@@ -145,6 +145,8 @@ def library():
         lib.eu_batch_last_error.restype = ctypes.c_char_p
         for fn in ("eu_batch_create", "eu_batch_step", "eu_batch_destroy"):
             getattr(lib, fn).restype = _I
+        lib.eu_set_conserved.argtypes = [_P] * 4
+        lib.eu_set_conserved.restype = _I
         lib.eu_set_inflow.argtypes = [_P] * 7
         lib.eu_set_inflow.restype = _I
         lib.eu_halo_bytes.argtypes = [_P, ctypes.POINTER(ctypes.c_size_t)]
@@ -320,6 +322,11 @@ class Solver:
         order = ["CS", "T", "E", "P", "D", "U", "V", "W", "H", "Gamma", "Yi"]
         arrs = [_c(st[n]) for n in order]
         self._check(library().eu_set_state(self.h, *[a.ctypes.data for a in arrs]), "set_state")
+
+    def set_conserved(self, cs, T, E):
+        """Upload CS, T, E and form the primitives on the device (eu_set_conserved)."""
+        arrs = [_c(a) for a in (cs, T, E)]
+        self._check(library().eu_set_conserved(self.h, *[a.ctypes.data for a in arrs]), "set_conserved")
 
     def set_inflow(self, P, T, U, V, W, Y):
         """EU_BC_ODW x-low inflow tables over the interior (j, k) nodes: planes

@@ -606,6 +606,28 @@ eu_status eu_set_state(eu_handle *h, const double *cs, const double *T, const do
     return EU_OK;
 }
 
+eu_status eu_set_conserved(eu_handle *h, const double *cs, const double *T, const double *E)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!cs || !T || !E)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "null argument");
+    if (!h->has_mech)
+        return fail(h, EU_ERR_NOT_READY, "load a mechanism first");
+    cudaSetDevice(h->cfg.device);
+    const long long n3 = h->n3;
+    const size_t b = size_t(n3) * sizeof(double);
+    CK(h, cudaMemcpyAsync(h->st.cs, cs, (h->mech.ns + 4) * b, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->st.T, T, b, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaMemcpyAsync(h->st.E, E, b, cudaMemcpyHostToDevice, h->stream));
+    // Update_after_CS on the interior nodes (the recovery of the step, no kinetics)
+    CK(h, flavour(h).recover_react(launch_args(h), false));
+    CK(h, cudaStreamSynchronize(h->stream));
+    h->has_state = true;
+    h->prim_stale = h->st.prim32 != nullptr; // mixed precision: the FP64 planes are formed on demand
+    return EU_OK;
+}
+
 eu_status eu_set_primitive(eu_handle *h, const double *P, const double *T, const double *U, const double *V,
                            const double *W, const double *Y)
 {

@@ -199,6 +199,15 @@ eu_status eu_set_state(eu_handle *h, const double *cs, const double *T, const do
                        const double *D, const double *U, const double *V, const double *W, const double *H,
                        const double *G, const double *Y);
 
+/* Upload the conserved state alone (CS: ns + 4 haloed planes; T, E: haloed planes)
+ * and form the primitives on the device as the step's recovery does
+ * (Flowfield::Update_after_CS, src/Flowfield.cpp:1579-1617: T by the Newton
+ * inversion from the given T with the given E as its energy, then u, v, w, e, p,
+ * H, Gamma). Ghost primitives are formed by the next step's ghost fill. The
+ * reference's post_advection_state_host (include/ReactionCuda.cuh:266) takes the
+ * same inputs. Half the bytes of eu_set_state for a full state. */
+eu_status eu_set_conserved(eu_handle *h, const double *cs, const double *T, const double *E);
+
 /* EU_BC_ODW inflow tables: the x-low ghost nodes take these values each step
  * (Flowfield::FieldBoundary_3dODW, src/Flowfield.cpp:414-432, which copies the
  * tables Uint .. Yint; the reference allocates them, :138-147, but never fills

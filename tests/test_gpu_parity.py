@@ -270,3 +270,36 @@ def test_znd_against_restatement(gpu, port_lib, width, steps, tol):
     assert peak >= 1
     assert rel_linf(interior(s.get("CS")), interior(port.get("CS"))).max() <= tol
     assert n_unequal(interior(s.get("Nchem")), interior(port.get("Nchem"))) == 0
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-6)])
+def test_set_conserved_matches_set_state(gpu, precision, tol):
+    """eu_set_conserved (CS, T, E up; the primitives formed on the device by
+    the recovery) steps like eu_set_state with the full state: the recovered
+    temperature is within 1e-12 of the uploaded one, and after three steps each
+    conserved plane agrees to its relative tolerance (the transverse momenta,
+    whose planes peak at ~1e-6 of the streamwise one, carry the primitives'
+    initial rounding difference at a few 1e-10 of their own maxima)."""
+    ni, nj, nk = 33, 17, 17
+    ext = (0.0, 0.016, 0.0, 0.008, 0.0, 0.008)
+    mech = gpu.parse_mechanism(cases.MECH_JA919, cases.THERMO)
+    x, y, z = (cases.node_coordinates(n, a, b) for n, a, b in ((ni, 0, 0.016), (nj, 0, 0.008), (nk, 0, 0.008)))
+    prim = cases.shock_bubble(x, y, z, mech["mw"], mech["ns"], radius=3e-3, shock_x=3e-3, standoff=5e-3, seed=5)
+    p, cs, T, E = gpu.initial_state(mech, ni, nj, nk, *prim)
+    st = {"CS": cs, "T": T, "E": E, "P": p[0], "D": p[1], "U": p[2], "V": p[3], "W": p[4], "H": p[5],
+          "Gamma": p[6], "Yi": p[7:]}
+    out = []
+    for full in (True, False):
+        s = gpu.Solver(ni, nj, nk, ext, precision=precision, arith="fast")
+        s.set_mechanism(mech)
+        if full:
+            s.set_state(st)
+        else:
+            s.set_conserved(cs, T, E)
+            t0 = np.asarray(T).reshape((1,) + s.shape)
+            assert rel_linf(interior(s.get("T")), interior(t0)).max() <= 1e-12
+        s.step(3, 4e-8)
+        out.append((s.get("CS"), s.get("T")))
+        s.close()
+    for a, b in zip(out[0], out[1]):
+        assert rel_linf(interior(b), interior(a)).max() <= tol
