@@ -262,7 +262,8 @@ int main(int argc, char **argv)
     const std::string name = argv[3], dir = argv[4];
     {
         std::ofstream o(dir + "/eu3d_mech_" + name + ".cuh");
-        o << "// Generated by eu3d-gpu_b200/host/gen_mech.cpp from " << argv[1] << " and " << argv[2]
+        auto base = [](const std::string &path) { return path.substr(path.find_last_of('/') + 1); };
+        o << "// Generated by eu3d-gpu_b200/host/gen_mech.cpp from " << base(argv[1]) << " and " << base(argv[2])
           << ". Do not edit.\n#pragma once\n#include \"eu3d_device.cuh\"\n\nnamespace eu3d {\n\n"
           << "// Rates of mechanism " << name << " (" << m.ns << " species, " << m.nr << " reactions).\n"
           << "struct Mech_" << name << " {\n    static constexpr int NS = " << m.ns << ", NR = " << m.nr << ";\n"
