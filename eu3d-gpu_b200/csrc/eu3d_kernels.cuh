@@ -1146,7 +1146,9 @@ __device__ __forceinline__ void warp_rates(const DevMech &ms, double T, const do
         rtb = 1.0;
     const double fwd = kf * rrf, bwd = kf * kc_inv * rrb;
     double P = 0.0, Q = 0.0, W = 0.0;
-#pragma unroll 1
+    // unrolled: the shuffles of all reactions issue ahead of the sums, so a
+    // substep's latency is not NR shuffle round trips
+#pragma unroll
     for (int q = 0; q < NR; ++q) {
         const double fr = __shfl_sync(0xffffffffu, fwd, q);
         const double br = __shfl_sync(0xffffffffu, bwd, q);
