@@ -53,7 +53,7 @@ FLUX_BYTES = {"fp64": (16 + 26) * 8, "mixed": 16 * 4 + 26 * 8}
 # ncu capture summarised in profiles/flux_tiled_and_recover_classify_256x128x64.md
 # (dram__bytes_read.sum + dram__bytes_write.sum at 256 x 128 x 64 nodes, divided by
 # the cells; the traffic scales with the cells, so it is scaled to the grid).
-FLUX_TRAFFIC_PER_CELL = {"mixed": 287.4}
+FLUX_TRAFFIC_PER_CELL = {"mixed": 286.4}
 # FLOPs per row of the learned ensemble (3 members x 2 (12 256 + 256 256 + 256 256 + 256 10)).
 MLP_FLOP_PER_ROW = 820224
 # FP64 flops per cell-substep of the stiff kinetics (rates, trapezoid update,
