@@ -37,19 +37,24 @@ def _free_port():
 
 
 def _case(boundary, blocks=1, block=0):
-    """Coordinates and primitive fields of one block (the whole grid when blocks == 1)."""
+    """Coordinates and primitive fields of one block (the whole grid when blocks
+    == 1), and the ODW inflow tables (None for the other cases)."""
     mech = golden_mechanism()
     x = cases.node_coordinates(NI, EXT[0], EXT[1], blocks=blocks, block=block)
     xg = cases.node_coordinates(NI, EXT[0], EXT[1])
     y = cases.node_coordinates(NJ, EXT[2], EXT[3])
     z = cases.node_coordinates(NK, EXT[4], EXT[5])
+    inflow = None
     if boundary == "znd":
         prim = cases.znd(xg, y, z, mech.mw, mech.ns)
+    elif boundary == "odw":
+        md = {k: getattr(mech, k) for k in ("ns", "mw", "coeff_lo", "coeff_hi")}
+        prim, inflow = cases.odw(xg, y, z, md)
     else:
         prim = cases.shock_bubble(xg, y, z, mech.mw, mech.ns, radius=4e-3, shock_x=16e-3, standoff=6e-3, seed=3)
     if blocks > 1:  # the block's planes of the global fields
         prim = [slab.block_slice(np.asarray(a), NI, blocks, block) for a in prim]
-    return mech, x, y, z, prim
+    return mech, x, y, z, prim, inflow
 
 
 def _run_block(rank, ranks, port, boundary, out):
@@ -61,10 +66,12 @@ def _run_block(rank, ranks, port, boundary, out):
     import torch.distributed as dist
     import oracle
     dist.init_process_group("gloo", rank=rank, world_size=ranks, timeout=timedelta(seconds=60))
-    mech, x, y, z, prim = _case(boundary, ranks, rank)
+    mech, x, y, z, prim, inflow = _case(boundary, ranks, rank)
     first, n = slab.block_range(NI, ranks, rank)
     port_ = oracle.PortOracle(n, NJ, NK, x, y, z, mech, nthreads=1, boundary=boundary)
     port_.set_primitive(*prim)
+    if inflow is not None:  # every block holds the tables; only the x-low one fills from them
+        port_.set_inflow(*inflow)
     port_.set_exchange(rank > 0, rank < ranks - 1)
     halo = slab.HaloExchange(dist, rank, ranks, port_.halo_count(), torch.float64, "cpu")
     for _ in range(STEPS):
@@ -77,7 +84,7 @@ def _run_block(rank, ranks, port, boundary, out):
         out.put(fields)
 
 
-@pytest.mark.parametrize("boundary,ranks", [("rsbi", 3), ("znd", 2)])
+@pytest.mark.parametrize("boundary,ranks", [("rsbi", 3), ("znd", 2), ("odw", 2)])
 def test_blocks_match_one_block(port_lib, boundary, ranks):
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
@@ -91,9 +98,11 @@ def test_blocks_match_one_block(port_lib, boundary, ranks):
         p.join(timeout=60)
     assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
 
-    mech, x, y, z, prim = _case(boundary)
+    mech, x, y, z, prim, inflow = _case(boundary)
     one = port_lib(NI, NJ, NK, x, y, z, mech, boundary=boundary)
     one.set_primitive(*prim)
+    if inflow is not None:
+        one.set_inflow(*inflow)
     one.step(STEPS, DT)
     reach = 2 * STEPS + 3
     shared = [slab.block_range(NI, ranks, r)[0] for r in range(1, ranks)]
