@@ -4,12 +4,20 @@
 Workload: the 3-D reacting shock-bubble case, 256 x 128 x 128 nodes over
 64 x 32 x 32 mm (4,194,304 cells), H2_JA919 kinetics (9 species, 19 reactions),
 Mach 2.83 shock in N2 at 101.325 kPa / 300 K hitting a perturbed 2H2+O2 sphere
-(radius 8 mm, seed 3), fixed dt from the reference's CFL rule at 0.5 on the
-initial state. Synthetic inputs built by eu3d_cases.shock_bubble.
+(radius 8 mm, centred 16 mm downstream of the shock, seed 3), fixed dt from the
+reference's CFL rule at 0.5 on the initial state, 500 steps in all. Synthetic
+inputs built by eu3d_cases.shock_bubble.
 
 A step is one full timestep: RSBI ghost fill, MUSCL/AUSM flux divergence in x,
 y, z with the explicit update, state recovery with Newton temperature
 inversion, Nchem prediction and the adaptive trapezoid kinetics.
+
+The timed window: each arm advances the case untimed for WINDOW_START steps,
+until the shock has entered the bubble (it reaches the bubble's upstream
+surface after about 80 steps and runs through the bubble gas from then on),
+then warms up and times --steps steps there, then runs on to step 500. The
+learned + mixed arm and the plain FP64 arm each run their own trajectory from
+step 0, and their difference is stated at the end of the window and at step 500.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -19,6 +27,11 @@ per rank (the reference's MPI layout: neighbouring blocks share a node, so N
 ranks hold N x 255 + 1 nodes along x over N x 64 mm): every step exchanges the
 blocks' halo planes over NCCL before it runs, dt is the minimum of the blocks'
 CFL steps, and per-GPU work is fixed ("scaling": "weak").
+
+--impl reference times the reference's own CPU timestep (oracle/_ref, built from
+its unmodified sources) on the same grid, cut into independent sub-boxes of
+64 x 64 x 64 nodes (one host process per sub-box), and never loads this
+library.
 """
 from __future__ import annotations
 
@@ -30,7 +43,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -38,21 +50,23 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "eu3d-gpu_b200"))
 
-import eu3d  # noqa: E402
-import eu3d_cases as cases  # noqa: E402
+import eu3d_cases as cases  # noqa: E402  (numpy only; never loads the library)
 
 METRIC = "Mcell-steps/s reacting, learned+mixed vs plain FP64 on same B200 at ≤1e-3 Y err"
 GRID = (256, 128, 128)
 EXTENT = (0.0, 0.064, 0.0, 0.032, 0.0, 0.032)
 CFL = 0.5
-L2_BYTES = 126 * 2 ** 20
+# the config's run length, and the step at which the timed window starts (the
+# shock inside the bubble)
+TOTAL_STEPS = 500
+WINDOW_START = 250
 # Algorithmic bytes per cell-step of the flux + update kernel: 16 primitives
 # read, 13 conserved read and written (FP64); FP32 primitives in mixed mode.
 FLUX_BYTES = {"fp64": (16 + 26) * 8, "mixed": 16 * 4 + 26 * 8}
-# DRAM bytes per cell of one launch of the mixed-precision flux kernel, from the
-# ncu capture summarised in profiles/flux_tiled_and_recover_classify_256x128x64.md
-# (dram__bytes_read.sum + dram__bytes_write.sum at 256 x 128 x 64 nodes, divided by
-# the cells; the traffic scales with the cells, so it is scaled to the grid).
+# DRAM bytes per cell of one launch of each flux kernel, from its ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum over the cells of the captured
+# 256 x 128 x 64-node grid; the traffic scales with the cells, so it is scaled
+# to the benchmark grid).
 FLUX_TRAFFIC_PER_CELL = {"mixed": 286.4}
 # FLOPs per row of the learned ensemble (3 members x 2 (12 256 + 256 256 + 256 256 + 256 10)).
 MLP_FLOP_PER_ROW = 820224
@@ -62,6 +76,10 @@ MLP_FLOP_PER_ROW = 820224
 F_SUB = 6017
 # FP64 vector peak of a B200 (datasheet; no measured FP64 figure is available).
 FP64_PEAK_TFLOPS = 37.0
+# Nchem histogram bins (upper edges, inclusive)
+NCHEM_BINS = (0, 1, 2, 4, 8, 16, 64, 256, 1 << 30)
+# The reference arm's sub-boxes (nodes per side) tiling the grid.
+REF_BOX = (64, 64, 64)
 
 
 def env_int(name, default):
@@ -131,16 +149,29 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def build_workload(grid, seed=3):
-    ni, nj, nk = grid
-    x = cases.node_coordinates(ni, EXTENT[0], EXTENT[1])
-    y = cases.node_coordinates(nj, EXTENT[2], EXTENT[3])
-    z = cases.node_coordinates(nk, EXTENT[4], EXTENT[5])
+# ------------------------------------------------------------------ workload
+
+def full_axes(grid=GRID, extent=EXTENT):
+    """Node coordinates (with ghosts) of the whole grid along x, y, z."""
+    return tuple(cases.node_coordinates(n, extent[2 * a], extent[2 * a + 1]) for a, n in enumerate(grid))
+
+
+def bubble_field(x, y, z, mw, ns, grid=GRID, extent=EXTENT, seed=3):
+    """The shock-bubble primitives on the nodes x, y, z: the whole grid's
+    nodes or any sub-box of them (the bubble centre is the whole grid's, so a
+    sub-box gets exactly its part of the field)."""
+    _, yf, zf = full_axes(grid, extent)
+    scale = extent[1] / 0.064
+    return cases.shock_bubble(x, y, z, mw, ns, radius=8e-3 * scale, shock_x=4e-3 * scale, standoff=16e-3 * scale,
+                              center_yz=(0.5 * (yf[2] + yf[-3]), 0.5 * (zf[2] + zf[-3])), seed=seed)
+
+
+def build_workload(grid):
+    import eu3d
+    x, y, z = full_axes(grid)
     mech = eu3d.parse_mechanism(cases.MECH_JA919, cases.THERMO)
-    scale = EXTENT[1] / 0.064
-    prim = cases.shock_bubble(x, y, z, mech["mw"], mech["ns"], radius=8e-3 * scale, shock_x=4e-3 * scale,
-                              standoff=16e-3 * scale, seed=seed)
-    p, cs, T, E = eu3d.initial_state(mech, ni, nj, nk, *prim)
+    prim = bubble_field(x, y, z, mech["mw"], mech["ns"], grid=grid)
+    p, cs, T, E = eu3d.initial_state(mech, *grid, *prim)
     dt = cases.cfl_dt(x, y, p[0], p[1], p[2], p[3], p[6], CFL)
     return mech, prim, (p, cs, T, E), dt
 
@@ -150,6 +181,75 @@ def state_dict(st):
     return {"CS": cs, "T": T, "E": E, "P": p[0], "D": p[1], "U": p[2], "V": p[3], "W": p[4], "H": p[5],
             "Gamma": p[6], "Yi": p[7:]}
 
+
+def snapshot(s):
+    """The handle's whole state as host arrays (the set_state dictionary)."""
+    out = {k: s.get(k) for k in ("CS", "T", "E", "P", "D", "U", "V", "W", "H", "Gamma", "Yi")}
+    for k in ("T", "E", "P", "D", "U", "V", "W", "H", "Gamma"):
+        out[k] = out[k][0]
+    return out
+
+
+def interior(a, bc=2):
+    return a[..., bc:-bc, bc:-bc, bc:-bc]
+
+
+def species_error(a, b, bc=2):
+    """Mean over cells of sum_s |Y_a - Y_b| (all cells; and cells holding any
+    reactive species)."""
+    ya, yb = interior(a, bc), interior(b, bc)
+    l1 = np.abs(ya - yb).sum(axis=0)
+    reactive = yb[:8].sum(axis=0) > 1e-9
+    return float(l1.mean()), float(l1[reactive].mean()) if reactive.any() else 0.0
+
+
+def rel_linf(a, b, bc=2):
+    """max |a - b| / max |b| per plane (interior nodes), as a list."""
+    ai, bi = interior(a, bc), interior(b, bc)
+    n = ai.shape[0]
+    d = np.abs(ai - bi).reshape(n, -1).max(1)
+    s = np.abs(bi).reshape(n, -1).max(1)
+    return [float(v) for v in d / np.where(s > 0, s, 1.0)]
+
+
+def shock_shift(p, p_ref, p0=101325.0, bc=2):
+    """Largest |difference| (cells) over the (j, k) columns of the leading
+    shock's position: the largest x node whose pressure exceeds 1.5 p0."""
+    a, b = interior(p, bc)[0] > 1.5 * p0, interior(p_ref, bc)[0] > 1.5 * p0
+    n = a.shape[0]
+    ia = np.where(a.any(axis=0), n - 1 - a[::-1].argmax(axis=0), -1)
+    ib = np.where(b.any(axis=0), n - 1 - b[::-1].argmax(axis=0), -1)
+    return int(np.abs(ia - ib).max())
+
+
+def nchem_histogram(nchem, bc=2):
+    """Cells per Nchem bin: {"<=0": .., "1": .., "2": .., "3-4": .., ...}."""
+    v = interior(nchem, bc).ravel()
+    out, lo = {}, None
+    for hi in NCHEM_BINS:
+        sel = (v <= hi) if lo is None else ((v > lo) & (v <= hi))
+        key = "<=0" if lo is None else (str(hi) if hi == lo + 1 else
+                                        (f">{lo}" if hi >= 1 << 30 else f"{lo + 1}-{hi}"))
+        out[key] = int(sel.sum())
+        lo = hi
+    return out
+
+
+def window_composition(st, bc=2):
+    """What the window's cells hold: cells carrying reactants (Y_H2 + Y_O2 >
+    1e-9, the cells whose kinetics the plain FP64 path integrates with
+    non-zero rates), the peak temperature among them, and the shock-heated
+    ones (T > 400 K)."""
+    Y = interior(st["Yi"], bc)
+    T = interior(st["T"][None], bc)[0]
+    fuel = (Y[cases.S_H2] + Y[cases.S_O2]) > 1e-9
+    return {"fuel_cells": int(fuel.sum()), "shocked_fuel_cells": int((fuel & (T > 400.0)).sum()),
+            "peak_T_fuel_K": round(float(T[fuel].max()), 1) if fuel.any() else None,
+            "peak_T_K": round(float(T.max()), 1), "peak_H2O": float(Y[cases.S_H2O].max()),
+            "peak_OH": float(Y[3].max())}
+
+
+# ---------------------------------------------------------------- distribution
 
 def dist_setup(args):
     world = env_int("WORLD_SIZE", 1)
@@ -178,7 +278,6 @@ def reduce_max(dist, value, device):
 
 def barrier(dist, device):
     if dist is not None:
-        import torch
         if device.startswith("cuda"):
             dist.barrier(device_ids=[int(device.split(":")[1])])
         else:
@@ -187,65 +286,107 @@ def barrier(dist, device):
 
 # ---------------------------------------------------------------- reference arm
 
+def ref_boxes(grid=GRID, box=REF_BOX):
+    """The sub-boxes tiling the grid: (first node i, j, k) of each."""
+    return [(i, j, k) for i in range(0, grid[0], box[0]) for j in range(0, grid[1], box[1])
+            for k in range(0, grid[2], box[2])]
+
+
+def _ref_box(oracle, origin, box=REF_BOX):
+    """A RefOracle holding sub-box `origin` of the workload: the same node
+    spacing and positions, the field of the whole grid cut to the box."""
+    xf, yf, zf = full_axes()
+    lo = [origin[a] + 2 for a in range(3)]
+    ext = (xf[lo[0]], xf[lo[0] + box[0] - 1], yf[lo[1]], yf[lo[1] + box[1] - 1], zf[lo[2]], zf[lo[2] + box[2] - 1])
+    ref = oracle.RefOracle.from_grid(*box, ext, cases.MECH_JA919, cases.THERMO)
+    x, y, z = ref.nodes()
+    ref.set_primitive(*bubble_field(x, y, z, ref.mechanism().mw, ref.ns))
+    return ref
+
+
 def _ref_worker(task):
-    """One host process: the reference's own CPU timestep on a sub-box sample."""
+    """One host process: the reference's own CPU timestep on its sub-boxes,
+    one after the other. Returns the seconds of the timed steps."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    ni, nj, nk, steps, warmup, dt, seed = task
-    ext = (0.0, EXTENT[1] * (ni - 1) / (GRID[0] - 1), 0.0, EXTENT[3] * (nj - 1) / (GRID[1] - 1), 0.0,
-           EXTENT[5] * (nk - 1) / (GRID[2] - 1))
-    ref = oracle.RefOracle.from_grid(ni, nj, nk, ext, cases.MECH_JA919, cases.THERMO)
-    x, y, z = ref.nodes()
-    prim = cases.shock_bubble(x, y, z, ref.mechanism().mw, ref.ns, radius=min(ext[1], ext[3]) * 0.3,
-                              shock_x=ext[1] * 0.15, standoff=ext[1] * 0.45, seed=seed)
-    ref.set_primitive(*prim)
-    if warmup:
-        ref.step(warmup, dt)
-    t0 = time.perf_counter()
-    ref.step(steps, dt)
-    return time.perf_counter() - t0
+    origins, steps, warmup, dt = task
+    secs = 0.0
+    for origin in origins:
+        ref = _ref_box(oracle, origin)
+        if warmup:
+            ref.step(warmup, dt)
+        t0 = time.perf_counter()
+        ref.step(steps, dt)
+        secs += time.perf_counter() - t0
+        ref.close()
+    return secs
 
 
-def reference_sample(nproc, steps, warmup, dt, box=(32, 32, 32)):
-    """Time the reference's CPU timestep (oracle/_ref) in nproc host processes,
-    each advancing its own sub-box of the workload at the workload's node
-    spacing. Returns Mcell-steps/s of the aggregate."""
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
-    tasks = [(box[0], box[1], box[2], steps, warmup, dt, 3 + r) for r in range(nproc)]
-    with ctx.Pool(nproc) as pool:
-        times = pool.map(_ref_worker, tasks)
-    cells = box[0] * box[1] * box[2]
-    return cells * steps * nproc / max(times) / 1e6, max(times)
+def reference_dt(oracle):
+    """The workload's dt by the reference's CFL rule at 0.5 (cases.cfl_dt),
+    with density and gamma from the NASA polynomials in numpy, on the whole
+    grid's nodes of the sub-box holding the shock: the smallest CFL step of
+    the grid is in the uniform shocked N2 behind it. (The reference reads grid
+    extents to six significant digits, so its own sub-box nodes sit up to 4e-8
+    m off the workload's and its CFL step differs in the sixth digit; this is
+    the workload's, equal to the library's to rounding.)"""
+    ref = oracle.RefOracle.from_grid(2, 2, 2, (0.0, 1e-3, 0.0, 1e-3, 0.0, 1e-3), cases.MECH_JA919, cases.THERMO)
+    m = ref.mechanism()
+    ref.close()
+    xf, yf, zf = full_axes()
+    x, y, z = xf[:REF_BOX[0] + 4], yf[:REF_BOX[1] + 4], zf[:REF_BOX[2] + 4]
+    P, T, U, V, _, Y = bubble_field(x, y, z, m.mw, m.ns)
+    a = np.where((T < 1000.0)[None, None], m.coeff_lo[:, :, None, None, None], m.coeff_hi[:, :, None, None, None])
+    r_s = (8.31434 / m.mw)[:, None, None, None]
+    cp_s = r_s * (a[0] * T ** -2 + a[1] / T + a[2] + a[3] * T + a[4] * T ** 2 + a[5] * T ** 3 + a[6] * T ** 4)
+    cp, r = (Y * cp_s).sum(0), (Y * r_s).sum(0)
+    return cases.cfl_dt(x, y, P, P / (r * 1000.0 * T), U, V, cp / (cp - r), CFL)
 
 
 def reference_arm(args):
-    # Rank 0 alone times the host-side reference; the other ranks exit without
-    # work (no process group: the arm has no collective step).
+    """--impl reference: the reference's CPU timestep (oracle/_ref) on the
+    whole 256 x 128 x 128 grid, cut into 16 sub-boxes of 64^3 nodes, one host
+    process per box; the aggregate of independent single-rank runs, no halo
+    exchange between the boxes. With fewer than 16 host cores each step is a
+    bounded sample: one box per core, spread over the grid. Rank 0 alone runs
+    it; the other ranks exit without work."""
     world, rank = env_int("WORLD_SIZE", 1), env_int("RANK", 0)
     if rank != 0:
         return 0
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import multiprocessing as mp
+
     import oracle
     if not os.path.exists(oracle.REF_LIB):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libeu3d_ref.so not built"}))
         return 0
     ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
-    nproc = max(1, min(ncores, 64))
-    _, _, _, dt = build_workload((64, 32, 32))
-    steps = max(1, args.steps)
-    warmup = max(0, args.warmup)
-    box = (24, 24, 24)
-    value, secs = reference_sample(nproc, steps, warmup, dt, box)
-    sample = (f"{nproc} host processes x reference CPU timestep (oracle/_ref, unmodified sources) on "
-              f"{box[0]}x{box[1]}x{box[2]}-node sub-boxes of the shock-bubble workload at its node spacing, "
-              f"{steps} timed steps after {warmup} warm-up; aggregate of independent single-rank runs")
+    boxes = ref_boxes()
+    nproc = max(1, min(ncores, len(boxes)))
+    chosen = [boxes[r * len(boxes) // nproc] for r in range(nproc)]
+    dt = reference_dt(oracle)
+    steps, warmup = max(1, args.steps), max(0, args.warmup)
+    tasks = [([b], steps, warmup, dt) for b in chosen]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(nproc) as pool:
+        secs = max(pool.map(_ref_worker, tasks))
+    cells = nproc * REF_BOX[0] * REF_BOX[1] * REF_BOX[2]
+    value = cells * steps / secs / 1e6
+    whole = nproc == len(boxes)
+    sample = (f"reference CPU timestep (oracle/_ref, unmodified sources, -O3) on "
+              f"{'the whole ' if whole else ''}{GRID[0]}x{GRID[1]}x{GRID[2]} grid as "
+              f"{'all ' if whole else ''}{nproc} of its {len(boxes)} independent {REF_BOX[0]}^3-node sub-boxes, "
+              f"one host process each, {steps} timed steps after {warmup} warm-up from the initial field; the "
+              f"reference integrates every cell's kinetics with Nchem = 1 both here and in the timed window (the "
+              f"GPU FP64 run's substeps per cell there: plain_fp64.substeps_per_cell)")
     line = {"metric": METRIC, "value": round(value, 6), "unit": "Mcell-steps/s", "n_gpus": world,
             "steps": steps, "warmup": warmup, "ms_per_step": round(secs / steps * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": "3-D reacting shock-bubble 256x128x128 (H2_JA919), sampled", "grid": list(GRID),
-                       "chemistry": "stiff", "precision": "fp64"},
+            "config": {"workload": "3-D reacting shock-bubble, 256x128x128 nodes over 64x32x32 mm, H2_JA919 "
+                                   "(9 species, 19 reactions), Mach 2.83 in N2, seed 3",
+                       "grid": list(GRID), "dt": dt, "chemistry": "stiff", "precision": "fp64",
+                       "decomposition": f"{len(boxes)} sub-boxes of {REF_BOX[0]}x{REF_BOX[1]}x{REF_BOX[2]} nodes"},
             "cpu_baseline": {"value": round(value, 6), "unit": "Mcell-steps/s", "cores": nproc,
                              "kind": "reference", "sample": sample},
             "e2e": {"value": round(value, 6), "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0,
@@ -257,7 +398,8 @@ def reference_arm(args):
 # ---------------------------------------------------------------------- our arm
 
 def cpu_baseline(dt):
-    """The reference's CPU timestep on one core, on a bounded sample."""
+    """The reference's CPU timestep on one core, on a bounded sample: the
+    64^3-node sub-box holding the bubble's upstream half."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     try:
         import oracle
@@ -265,52 +407,36 @@ def cpu_baseline(dt):
             return None
     except ImportError:
         return None
-    box = (48, 48, 48)
     steps = 6
-    secs = _ref_worker((box[0], box[1], box[2], steps, 1, dt, 3))
-    cells = box[0] * box[1] * box[2]
+    secs = _ref_worker(([(64, 0, 0)], steps, 1, dt))
+    cells = REF_BOX[0] * REF_BOX[1] * REF_BOX[2]
     return {"value": round(cells * steps / secs / 1e6, 6), "unit": "Mcell-steps/s", "cores": 1,
             "kind": "reference",
-            "sample": f"reference CPU timestep (oracle/_ref) on a {box[0]}x{box[1]}x{box[2]}-node sub-box of the "
-                      f"workload at its node spacing, {steps} steps after 1 warm-up, single thread ({secs:.1f} s)"}
-
-
-def species_error(a, b, bc=2):
-    """Mean over cells of sum_s |Y_a - Y_b| (all cells; and cells holding any
-    reactive species)."""
-    ya = a[:, bc:-bc, bc:-bc, bc:-bc]
-    yb = b[:, bc:-bc, bc:-bc, bc:-bc]
-    l1 = np.abs(ya - yb).sum(axis=0)
-    reactive = yb[:8].sum(axis=0) > 1e-9
-    return float(l1.mean()), float(l1[reactive].mean()) if reactive.any() else 0.0
+            "sample": f"reference CPU timestep (oracle/_ref) on the {REF_BOX[0]}^3-node sub-box of the workload at "
+                      f"nodes (64, 0, 0) (the bubble's upstream half), {steps} steps after 1 warm-up, single thread "
+                      f"({secs:.1f} s)"}
 
 
 def mlp_roofline(model, rows=1 << 18, reps=5):
-    """The fused inference kernel (eu_mlp_predict_fused) on `rows` feature rows
-    drawn inside the model's input box: FLOPs of the 3-member ensemble per
-    second, against the measured BF16 dense peak."""
+    """The fused inference kernel on `rows` feature rows drawn inside the
+    model's input box, launched back to back with no host synchronisation
+    between launches: FLOPs of the 3-member ensemble per second, against the
+    measured BF16 dense peak."""
     import torch
-    z = np.load(__import__("learned").CHECKPOINT)
+    import learned
+    z = np.load(learned.CHECKPOINT)
     lo, hi = z["box_lo"].astype(np.float32), z["box_hi"].astype(np.float32)
     g = torch.Generator(device="cuda").manual_seed(7)
     X = (torch.from_numpy(lo).cuda() + torch.rand(rows, lo.size, device="cuda", generator=g) *
          torch.from_numpy(hi - lo).cuda()).contiguous()
     members = int(z["shape"][4])
     out = torch.empty(members, rows, int(z["shape"][3]), device="cuda")
-    model.predict_fused(X, out)
-    torch.cuda.synchronize()
-    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s0.record(torch.cuda.current_stream())
-    for _ in range(reps):
-        model.predict_fused(X, out)
-    s1.record(torch.cuda.current_stream())
-    torch.cuda.synchronize()
-    ms = s0.elapsed_time(s1) / reps
+    ms = model.time_fused_queue(X, out, reps=reps)
     _, bf16, kind = measured_peaks()
     tf = MLP_FLOP_PER_ROW * rows / (ms / 1e3) / 1e12
     return {"kernel": "mlp_fused", "bound": "tensor", "rows": rows, "ms": round(ms, 4), "achieved": round(tf, 2),
             "peak": bf16, "unit": "TFLOP/s", "frac": round(tf / bf16, 4), "peak_source": f"{kind} bf16_tflops",
-            "note": "each call synchronises the model's stream (error check), included"}
+            "note": "CUDA events on the model's stream around back-to-back launches (eu_mlp_predict_fused_async)"}
 
 
 def reacting_block(args, model, gate, local, dt=2e-8):
@@ -325,6 +451,7 @@ def reacting_block(args, model, gate, local, dt=2e-8):
     gas: its Nchem prediction, which ignores species below Y = 1e-6, lets the
     first radicals overshoot into a non-positive Nchem or non-finite state.)"""
     import torch
+    import eu3d
     import learned
     grid = (48, 32, 32)
     ext = (0.0, 0.012, 0.0, 0.008, 0.0, 0.008)
@@ -364,6 +491,7 @@ def znd_case(args, local, steps=1000, cells=4000, dx=25e-6):
     device, 1000 steps. Reports the device throughput, the time advanced and
     where the leading shock (the largest x with p > 2 x the quiescent
     pressure) is at the end."""
+    import eu3d
     ni = cells + 1
     ext = (0.0, cells * dx, 0.0, dx, 0.0, dx)
     x = cases.node_coordinates(ni, ext[0], ext[1])
@@ -405,6 +533,7 @@ def odw_case(args, local, model, gate, grid=(1024, 512, 2), steps=2000, z_extent
     where p first exceeds 1.5 x the freestream pressure from the top down,
     fitted over the middle half of x, plus the wedge angle (the oblique-shock
     relation gives about 32 degrees for an ideal gas at gamma 1.4)."""
+    import eu3d
     ni, nj, nk = grid
     dx = 0.0525 / (ni - 1)
     ext = (0.0, 0.0525, 0.0, 0.02, 0.0, dx * (nk - 1) if z_extent is None else z_extent)
@@ -473,6 +602,7 @@ def batch_instances(args, model, gate, local, mech, count=32):
     FP64 stiff path. Aggregate cell-steps per device second of each, and each
     instance's own step time one by one."""
     import torch
+    import eu3d
     import learned
     built = []
     for q, (grid, mach, radius, ext) in enumerate(batch_specs(count)):
@@ -528,12 +658,33 @@ def batch_instances(args, model, gate, local, mech, count=32):
             "seed": 5, "unit": "Mcell-steps/s"}
 
 
+def flux_roofline(phase, steps, ncell, precision):
+    """The flux + update kernel's algorithmic bytes per launch over its CUDA-event
+    time, against the measured copy bandwidth; the dominant kernel phase."""
+    hbm, _, peak_kind = measured_peaks()
+    names = ["ghost_fill", "flux_update", "recover_kinetics"]
+    flux_ms = phase[1] / steps
+    flux_gbs = FLUX_BYTES[precision] * ncell / (flux_ms / 1e3) / 1e9
+    dominant = max(range(3), key=lambda q: phase[q])
+    return {"kernel": "flux_update", "bound": "hbm", "achieved": round(flux_gbs, 1), "peak": hbm,
+            "unit": "GB/s", "frac": round(flux_gbs / hbm, 4),
+            "traffic": (round(FLUX_TRAFFIC_PER_CELL[precision] * ncell / 1e9, 4)
+                        if precision in FLUX_TRAFFIC_PER_CELL else None),
+            "traffic_unit": "GB per launch (ncu, scaled from 256x128x64)",
+            "algorithmic_bytes_per_cell": FLUX_BYTES[precision], "flux_ms": round(flux_ms, 4),
+            "peak_source": f"{peak_kind} hbm_gbs", "dominant_kernel": names[dominant],
+            "dominant_share": round(phase[dominant] / max(sum(phase[:3]), 1e-9), 3)}
+
+
 def our_arm_blocks(args, world, rank, local, dist):
     """The workload decomposed along x over the ranks (eu3d-gpu_b200/slab.py),
     one 256 x 128 x 128-node block per GPU, halo planes exchanged over NCCL
-    every step. The single-GPU side studies (reacting block, batch, ZND, model
-    roofline, CPU baseline) are N = 1 measurements and are not repeated."""
+    every step, advanced untimed to the same window as the one-GPU run (the
+    shock inside the bubble of block 0) before the timed steps. The
+    single-GPU side studies (reacting block, batch, ZND, model roofline, CPU
+    baseline) are N = 1 measurements and are not repeated."""
     import torch
+    import eu3d
     import slab
     device = f"cuda:{local}"
     ni, nj, nk = args.grid
@@ -555,6 +706,7 @@ def our_arm_blocks(args, world, rank, local, dist):
     if args.chem == "learned":
         import learned
         model, gate = learned.load(device=local)
+    start = min(getattr(args, "window_start", WINDOW_START), TOTAL_STEPS)
 
     def make(chem, precision, arith, profile=False, state=sd):
         s = slab.SlabSolver(dist, total_ni, nj, nk, ext, device=local, precision=precision, chemistry=chem,
@@ -586,6 +738,9 @@ def our_arm_blocks(args, world, rank, local, dist):
         return st, reduce_max(dist, ev0.elapsed_time(ev1), device), (clk.summary() if clk else None)
 
     s = make(args.chem, args.precision, args.arith)
+    if start:
+        s.step(start, dt, stats=False)
+    window_state = snapshot(s.solver)
     tuned = s.autotune(reps=5) if not args.no_autotune else None
     stats, ms, clocks = timed(s, clocks=True)
     value = ncell * args.steps * world / (ms / 1e3) / 1e6
@@ -597,6 +752,8 @@ def our_arm_blocks(args, world, rank, local, dist):
     plain = None
     if (args.chem, args.precision) != ("stiff", "fp64"):
         sp_ = make("stiff", "fp64", "fast")
+        if start:
+            sp_.step(start, dt, stats=False)
         _, pms, _ = timed(sp_)
         y_ref = sp_.get("Yi")
         sp_.close()
@@ -604,37 +761,28 @@ def our_arm_blocks(args, world, rank, local, dist):
         pvalue = ncell * args.steps * world / (pms / 1e3) / 1e6
         plain = {"value": round(pvalue, 3), "ms_per_step": round(pms / args.steps, 4),
                  "speedup": round(value / pvalue, 3), "species_l1_vs_plain": err_all,
-                 "species_l1_vs_plain_reactive_cells": err_reactive, "after_steps": args.warmup + args.steps,
+                 "species_l1_vs_plain_reactive_cells": err_reactive, "after_steps": start + args.warmup + args.steps,
                  "note": "rank 0's block"}
 
     # per-kernel phases of one exchanged step (CUDA events inside the library)
-    sp = make(args.chem, args.precision, args.arith, profile=True)
+    sp = make(args.chem, args.precision, args.arith, profile=True, state=window_state)
     sp.step(args.warmup, dt, stats=False)
     phase = sp.step(1, dt, stats=True)["phase_ms"]
     sp.close()
     names = ["ghost_fill", "flux_update", "recover_kinetics" if args.chem != "learned" else "recover_learned_chem"]
     per_kernel = {n: round(phase[q], 4) for q, n in enumerate(names)}
-    hbm, bf16, peak_kind = measured_peaks()
-    flux_gbs = FLUX_BYTES[args.precision] * ncell / (phase[1] / 1e3) / 1e9
-    dominant = max(range(3), key=lambda q: phase[q])
-    roofline = {"kernel": "flux_update", "bound": "hbm", "achieved": round(flux_gbs, 1), "peak": hbm,
-                "unit": "GB/s", "frac": round(flux_gbs / hbm, 4),
-                "traffic": (round(FLUX_TRAFFIC_PER_CELL[args.precision] * ncell / 1e9, 4)
-                            if args.precision in FLUX_TRAFFIC_PER_CELL else None),
-                "traffic_unit": "GB per launch (ncu, scaled from 256x128x64)",
-                "algorithmic_bytes_per_cell": FLUX_BYTES[args.precision], "peak_source": f"{peak_kind} hbm_gbs",
-                "dominant_kernel": names[dominant],
-                "dominant_share": round(phase[dominant] / max(sum(phase[:3]), 1e-9), 3)}
+    roofline = flux_roofline(phase, 1, ncell, args.precision)
 
     # end to end through the public API with host buffers (state up once, the
     # exchanged steps each synchronous, the conserved state down at the end)
     pinned = {}
     for k in ("CS", "T", "E"):
-        t = torch.empty(sd[k].shape, dtype=torch.float64, pin_memory=True)
-        t.numpy()[...] = sd[k]
+        src = window_state[k] if k == "CS" else window_state[k][None]
+        t = torch.empty(src.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = src
         pinned[k] = t.numpy()
-    cs_host = torch.empty(sd["CS"].shape, dtype=torch.float64, pin_memory=True).numpy()
-    se = make(args.chem, args.precision, args.arith)
+    cs_host = torch.empty(window_state["CS"].shape, dtype=torch.float64, pin_memory=True).numpy()
+    se = make(args.chem, args.precision, args.arith, state=window_state)
     se.step(args.warmup, dt, stats=False)
     se.sync()
     barrier(dist, device)
@@ -652,12 +800,14 @@ def our_arm_blocks(args, world, rank, local, dist):
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": "Mcell-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32+f64" if args.precision == "mixed" else "f64",
                 "data": "synthetic",
                 "config": {"workload": f"3-D reacting shock-bubble decomposed along x: {world} blocks of "
                                        f"{ni}x{nj}x{nk} nodes ({total_ni}x{nj}x{nk} global over "
                                        f"{ext[1] * 1e3:.0f}x32x32 mm), H2_JA919, Mach 2.83 in N2, seed 3",
                            "grid": [ni, nj, nk], "global_grid": [total_ni, nj, nk], "dt": dt,
+                           "window": f"steps {start + args.warmup} .. {start + args.warmup + args.steps}",
                            "precision": args.precision, "chemistry": args.chem, "arith": args.arith,
                            "parallelism": f"x blocks {world}, halo exchange over NCCL every step",
                            "halo_bytes_per_face": halo_bytes, "autotune": tuned,
@@ -679,6 +829,7 @@ def our_arm_blocks(args, world, rank, local, dist):
 
 def our_arm(args):
     import torch
+    import eu3d
     world, rank, local, dist = dist_setup(args)
     if world > 1:
         return our_arm_blocks(args, world, rank, local, dist)
@@ -692,6 +843,9 @@ def our_arm(args):
     if args.chem == "learned":
         import learned
         model, gate = learned.load(device=local)
+    start = min(args.window_start, args.total_steps)
+    window_end = start + args.warmup + args.steps
+    run_end = max(args.total_steps, window_end)
 
     def make_solver(chem, precision, arith, profile=False, state=sd):
         s = eu3d.Solver(*grid, EXTENT, precision=precision, chemistry=chem, arith=arith, device=local,
@@ -703,56 +857,83 @@ def our_arm(args):
             learned.attach(s, model, gate)
         return s
 
-    def timed(s):
-        s.step(args.warmup, dt)
-        barrier(dist, device)
+    def window_run(s, clocks=False, tune=False):
+        """Advance to the window untimed, (autotune,) warm up, time args.steps
+        steps, keep the state at the window's end, run on to run_end."""
+        if start:
+            s.step(start, dt, stats=False)
+        ws = snapshot(s) if clocks else None
+        tuned = s.autotune(reps=5) if tune else None
+        s.step(args.warmup, dt, stats=False)
         torch.cuda.synchronize()
+        clk = ClockSampler(torch.cuda.current_device()) if clocks else None
+        if clk:
+            clk.__enter__()
         st = s.step(args.steps, dt)
         torch.cuda.synchronize()
-        barrier(dist, device)
-        return st, reduce_max(dist, st["device_ms"], device)
+        if clk:
+            clk.__exit__(None, None, None)
+        end = {"Yi": s.get("Yi"), "P": s.get("P"), "CS": s.get("CS"), "T": s.get("T"), "Nchem": s.get("Nchem")}
+        if run_end > window_end:
+            s.step(run_end - window_end, dt, stats=False)
+        last = {"Yi": s.get("Yi"), "P": s.get("P"), "CS": s.get("CS")}
+        return st, end, last, ws, tuned, (clk.summary() if clk else None)
 
-    # -- device-resident throughput of the configured path (value) --------------------------
+    # -- the configured path (learned + mixed by default): value -------------------------------
     s = make_solver(args.chem, args.precision, args.arith)
-    # launch shapes picked on this state (kept for the later handles of this shape)
-    tuned = s.autotune(reps=5) if not args.no_autotune else None
-    s.step(args.warmup, dt)
-    barrier(dist, device)
-    torch.cuda.synchronize()
-    with ClockSampler(torch.cuda.current_device()) as clk:
-        stats = s.step(args.steps, dt)
-    torch.cuda.synchronize()
-    barrier(dist, device)
+    stats, end_fast, last_fast, window_state, tuned, clocks = window_run(s, clocks=True, tune=not args.no_autotune)
+    s.close()
     ms = reduce_max(dist, stats["device_ms"], device)
     value = ncell * args.steps * world / (ms / 1e3) / 1e6
-    clocks = clk.summary()
-    y_fast = s.get("Yi")
-    s.close()
+    window = window_composition({"Yi": end_fast["Yi"], "T": end_fast["T"][0]})
 
-    # -- the plain FP64 stiff step on the same input (the comparison the metric names) -------
+    # -- the plain FP64 stiff step, its own trajectory (the comparison the metric names) --------
     plain = None
     if (args.chem, args.precision) != ("stiff", "fp64"):
         sp_ = make_solver("stiff", "fp64", "fast")
-        pst, pms = timed(sp_)
-        y_ref = sp_.get("Yi")
+        pst, end_ref, last_ref, _, _, _ = window_run(sp_)
         sp_.close()
-        err_all, err_reactive = species_error(y_fast, y_ref)
-        # the kinetics phase of the plain step against the FP64 roofline
-        spk = make_solver("stiff", "fp64", "fast", profile=True)
+        pms = pst["device_ms"]
+        err_all, err_reactive = species_error(end_fast["Yi"], end_ref["Yi"])
+        err_all_500, err_reactive_500 = species_error(last_fast["Yi"], last_ref["Yi"])
+        # the kinetics phase of the plain step against the FP64 roofline, on the window state
+        spk = make_solver("stiff", "fp64", "fast", profile=True, state=window_state)
         spk.step(args.warmup, dt)
         kst = spk.step(args.steps, dt)
+        plain_phase = kst["phase_ms"]
         spk.close()
-        kin_ms = kst["phase_ms"][2] / args.steps
+        kin_ms = plain_phase[2] / args.steps
         kin_tf = F_SUB * kst["sum_nchem"] / (kin_ms / 1e3) / 1e12
         kin = {"kernel": "recover_react", "bound": "fp64", "achieved": round(kin_tf, 3),
                "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": round(kin_tf / FP64_PEAK_TFLOPS, 4),
                "peak_source": "datasheet", "flop_per_substep": F_SUB, "substeps_per_step": kst["sum_nchem"],
                "ms_per_step": round(kin_ms, 4)}
-        plain = {"kinetics_roofline": kin,
-                 "value": round(ncell * args.steps * world / (pms / 1e3) / 1e6, 3), "ms_per_step":
-                 round(pms / args.steps, 4), "speedup": round(value / (ncell * args.steps * world / (pms / 1e3) / 1e6), 3),
-                 "species_l1_vs_plain": err_all, "species_l1_vs_plain_reactive_cells": err_reactive,
-                 "after_steps": args.warmup + args.steps}
+        pvalue = ncell * args.steps * world / (pms / 1e3) / 1e6
+        plain = {"value": round(pvalue, 3), "ms_per_step": round(pms / args.steps, 4),
+                 "speedup": round(value / pvalue, 3),
+                 "kernels_ms_per_step": {n: round(plain_phase[q] / args.steps, 4)
+                                         for q, n in enumerate(("ghost_fill", "flux_update", "recover_kinetics"))},
+                 "flux_roofline": flux_roofline(plain_phase, args.steps, ncell, "fp64"),
+                 "kinetics_roofline": kin,
+                 "substeps_per_cell": round(pst["sum_nchem"] / ncell, 6), "max_nchem": pst["max_nchem"],
+                 "nchem_histogram_window_end": nchem_histogram(end_ref["Nchem"]),
+                 "error_vs_plain": {
+                     "at_window_end": {"step": window_end, "species_l1": err_all,
+                                       "species_l1_fuel_cells": err_reactive,
+                                       "interface_shift_cells": cases.front_shift(end_fast["Yi"], end_ref["Yi"],
+                                                                                  product=cases.S_H2),
+                                       "reaction_front_shift_cells": cases.front_shift(end_fast["Yi"], end_ref["Yi"]),
+                                       "shock_shift_cells": shock_shift(end_fast["P"], end_ref["P"]),
+                                       "cs_rel_linf_max": max(rel_linf(end_fast["CS"], end_ref["CS"]))},
+                     "at_step_500": {"step": run_end, "species_l1": err_all_500,
+                                     "species_l1_fuel_cells": err_reactive_500,
+                                     "interface_shift_cells": cases.front_shift(last_fast["Yi"], last_ref["Yi"],
+                                                                                product=cases.S_H2),
+                                     "reaction_front_shift_cells": cases.front_shift(last_fast["Yi"], last_ref["Yi"]),
+                                     "shock_shift_cells": shock_shift(last_fast["P"], last_ref["P"]),
+                                     "cs_rel_linf": rel_linf(last_fast["CS"], last_ref["CS"])}}}
+        del end_ref, last_ref
+    del last_fast
 
     # -- reacting gas: the chemistry phase the learned model replaces ---------------------------
     block = reacting_block(args, model, gate, local) if args.chem == "learned" else None
@@ -778,38 +959,27 @@ def our_arm(args):
         except eu3d.EU3DError as e:
             odw3 = {"error": str(e)}
 
-    # -- per-kernel times (same stream, CUDA events around each kernel phase) -----------------
-    sp = make_solver(args.chem, args.precision, args.arith, profile=True)
+    # -- per-kernel times on the window state (same stream, CUDA events around each phase) ----
+    sp = make_solver(args.chem, args.precision, args.arith, profile=True, state=window_state)
     sp.step(args.warmup, dt)
     pst = sp.step(args.steps, dt)
     phase = pst["phase_ms"]
     names = ["ghost_fill", "flux_update", "recover_kinetics" if args.chem != "learned" else "recover_learned_chem"]
     per_kernel = {n: round(phase[q] / args.steps, 4) for q, n in enumerate(names)}
     sp.close()
+    roofline = flux_roofline(phase, args.steps, ncell, args.precision)
 
-    hbm, bf16, peak_kind = measured_peaks()
-    flux_ms = phase[1] / args.steps
-    flux_gbs = FLUX_BYTES[args.precision] * ncell / (flux_ms / 1e3) / 1e9
-    dominant = max(range(3), key=lambda q: phase[q])
-    roofline = {"kernel": "flux_update", "bound": "hbm", "achieved": round(flux_gbs, 1), "peak": hbm,
-                "unit": "GB/s", "frac": round(flux_gbs / hbm, 4),
-                "traffic": (round(FLUX_TRAFFIC_PER_CELL[args.precision] * ncell / 1e9, 4)
-                            if args.precision in FLUX_TRAFFIC_PER_CELL else None),
-                "traffic_unit": "GB per launch (ncu, scaled from 256x128x64)",
-                "algorithmic_bytes_per_cell": FLUX_BYTES[args.precision], "peak_source": f"{peak_kind} hbm_gbs",
-                "dominant_kernel": names[dominant],
-                "dominant_share": round(phase[dominant] / max(sum(phase[:3]), 1e-9), 3)}
-
-    # -- end to end through the public API with host buffers ----------------------------------
+    # -- end to end through the public API with host buffers, on the window state -------------
     # the conserved state (CS, T, E) is what a step needs; eu_set_conserved forms
     # the primitives on the device as the step's recovery does
     pinned = {}
     for k in ("CS", "T", "E"):
-        t = torch.empty(sd[k].shape, dtype=torch.float64, pin_memory=True)
-        t.numpy()[...] = sd[k]
+        src = window_state[k] if k == "CS" else window_state[k][None]
+        t = torch.empty(src.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = src
         pinned[k] = t.numpy()
-    cs_host = torch.empty(sd["CS"].shape, dtype=torch.float64, pin_memory=True).numpy()
-    se = make_solver(args.chem, args.precision, args.arith)
+    cs_host = torch.empty(window_state["CS"].shape, dtype=torch.float64, pin_memory=True).numpy()
+    se = make_solver(args.chem, args.precision, args.arith, state=window_state)
     se.step(args.warmup, dt)
     barrier(dist, device)
     torch.cuda.synchronize()
@@ -833,13 +1003,25 @@ def our_arm(args):
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": "Mcell-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32+f64" if args.precision == "mixed" else "f64",
                 "data": "synthetic",
                 "config": {"workload": "3-D reacting shock-bubble, 256x128x128 nodes over 64x32x32 mm, "
                                        "H2_JA919 (9 species, 19 reactions), Mach 2.83 in N2, seed 3",
-                           "grid": list(grid), "dt": dt, "precision": args.precision, "chemistry": args.chem,
+                           "grid": list(grid), "dt": dt,
+                           "window": {"start_step": start, "timed_steps": [start + args.warmup, window_end],
+                                      "run_steps": run_end,
+                                      "why": "the shock reaches the bubble after about 80 steps; from then on it "
+                                             "runs through the bubble gas"},
+                           "precision": args.precision, "chemistry": args.chem,
                            "arith": args.arith, "parallelism": f"replicas x{world}", "autotune": tuned,
                            "l2": f"inputs larger than L2: {sd['CS'].nbytes * 3 // 2**20} MiB state > 126 MiB"},
+                "window_state": {**window,
+                                 "note": "the transmitted shock heats the bubble gas to about 600 K and the "
+                                         "shocked N2 is at 745 K: below the 800 K activity threshold, no radical "
+                                         "pool forms and no cell ignites within the run's 500 steps (49 us), so "
+                                         "the learned path finds no chemically active cell; reacting_block is "
+                                         "the figure on igniting gas"},
                 "plain_fp64": plain,
                 "reacting_block": block,
                 "batch_instances": batch,
@@ -850,6 +1032,7 @@ def our_arm(args):
                 "roofline": roofline, "kernels_ms_per_step": per_kernel,
                 "max_nchem": stats["max_nchem"], "reacting_cells": stats["reacting"],
                 "learned_cells": stats["learned"], "fallback_cells": stats["fallback"],
+                "nchem_histogram_window_end": nchem_histogram(end_fast["Nchem"]),
                 "clocks": clocks,
                 "e2e": {"value": round(e2e_value, 3), "unit": "Mcell-steps/s",
                         "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
@@ -858,6 +1041,18 @@ def our_arm(args):
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+    return 0
+
+
+def side_study(args):
+    """One side study on cuda:0, its result printed as JSON (for profiling a
+    kernel that the full run launches among many others)."""
+    import torch
+    import learned
+    torch.cuda.set_device(0)
+    model, gate = learned.load(device=0)
+    out = reacting_block(args, model, gate, 0) if args.only == "reacting_block" else mlp_roofline(model)
+    print(json.dumps({args.only: out}), flush=True)
     return 0
 
 
@@ -871,20 +1066,27 @@ def main():
     ap.add_argument("--chem", choices=["stiff", "frozen", "learned"], default="learned")
     ap.add_argument("--arith", choices=["strict", "fast"], default="fast")
     ap.add_argument("--grid", type=int, nargs=3, default=list(GRID))
+    ap.add_argument("--window-start", type=int, default=WINDOW_START,
+                    help="steps advanced untimed before the timed window")
+    ap.add_argument("--total-steps", type=int, default=TOTAL_STEPS,
+                    help="steps each arm runs in all (the window included); the errors are stated at the end")
+    ap.add_argument("--only", choices=["reacting_block", "mlp_roofline"],
+                    help="run one side study alone and print its result (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-instance workload")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
     if args.chem == "learned":
-        sys.path.insert(0, os.path.join(ROOT, "eu3d-gpu_b200"))
         import learned
         if not os.path.exists(learned.CHECKPOINT):
             print("no trained learned-chemistry checkpoint; measuring the stiff kinetics", file=sys.stderr)
             args.chem = "stiff"
-    if args.warmup < 3 and args.impl == "ours":
+    if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
-        return reference_arm(args)
+    if args.only:
+        return side_study(args)
     return our_arm(args)
 
 

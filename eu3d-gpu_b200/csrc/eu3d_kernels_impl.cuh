@@ -5,6 +5,7 @@
 
 #include <algorithm>
 
+#include "eu3d_attr.hpp"
 #include "eu3d_kernels.cuh"
 #include "eu3d_launch.hpp"
 
@@ -33,14 +34,10 @@ cudaError_t flux_launch(const LaunchArgs &a, const R *prim)
 {
     const DevGrid &g = a.g;
     const size_t smem = flux_smem_bytes<NS, R>();
-    static bool configured = false; // per instantiation, once per process
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_flux_update<NS, R, kStrict>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        if (e != cudaSuccess)
-            return e;
-        configured = true;
-    }
+    static SmemLimit limit; // per instantiation, per device
+    const cudaError_t e = limit.ensure(k_flux_update<NS, R, kStrict>, smem);
+    if (e != cudaSuccess)
+        return e;
     const dim3 block(kFluxTK, kFluxTJ);
     const int ci = a.flux_ci > 0 ? a.flux_ci : 16;
     const dim3 grid((g.nk + kFluxTK - 1) / kFluxTK, (g.nj + kFluxTJ - 1) / kFluxTJ, (g.ni + ci - 1) / ci);
@@ -53,14 +50,10 @@ cudaError_t tiled_flux_launch(const LaunchArgs &a, const R *prim)
 {
     const DevGrid &g = a.g;
     const size_t smem = tiled_flux_smem_bytes<NS, R>();
-    static bool configured = false; // per instantiation, once per process
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_flux_update_tiled<NS, R, kStrict>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        if (e != cudaSuccess)
-            return e;
-        configured = true;
-    }
+    static SmemLimit limit; // per instantiation, per device
+    const cudaError_t e = limit.ensure(k_flux_update_tiled<NS, R, kStrict>, smem);
+    if (e != cudaSuccess)
+        return e;
     const dim3 block(kTileK, kTileWarps);
     const int ci = a.flux_ci > 0 ? a.flux_ci : 16;
     const dim3 grid((g.nk + kTileK - 1) / kTileK, (g.nj + kTileJ - 1) / kTileJ, (g.ni + ci - 1) / ci);

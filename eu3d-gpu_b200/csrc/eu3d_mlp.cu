@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "eu3d.h"
+#include "eu3d_attr.hpp"
 #include "eu3d_gemm.cuh"
 #include "eu3d_mlp_fused.cuh"
 #include "eu3d_mlp_kernels.hpp"
@@ -19,14 +20,10 @@ cudaError_t gemm_launch(const __nv_bfloat16 *A, int lda, const __nv_bfloat16 *B,
                         int k_split, int *err, cudaStream_t s)
 {
     const size_t smem = gemm_smem_bytes<BN>();
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e =
-            cudaFuncSetAttribute(k_gemm_bf16<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        if (e != cudaSuccess)
-            return e;
-        configured = true;
-    }
+    static SmemLimit limit; // per instantiation, per device
+    const cudaError_t e = limit.ensure(k_gemm_bf16<BN>, smem);
+    if (e != cudaSuccess)
+        return e;
     const dim3 grid((M + kGemmBM - 1) / kGemmBM, (N + BN - 1) / BN, k_split);
     k_gemm_bf16<BN>
         <<<grid, kGemmThreads, smem, s>>>(A, lda, B, ldb, M, N, K, bias, act, Cf, Cb, Cpre, ldc, Z, k_split, err);
@@ -245,13 +242,10 @@ cudaError_t mlp_fused(const FusedMlpParams &p, const float *feat, int ld_feat, i
     if (!fused_supported(p.in_pad, p.width, p.out_pad, p.members, p.layers))
         return cudaErrorInvalidValue;
     const size_t smem = fused_smem_bytes(p.in_pad, p.width);
-    static size_t configured = 0;
-    if (configured < smem) {
-        cudaError_t e = cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        if (e != cudaSuccess)
-            return e;
-        configured = smem;
-    }
+    static SmemLimit limit; // per device: the largest size set so far
+    const cudaError_t e = limit.ensure(k_mlp_fused, smem);
+    if (e != cudaSuccess)
+        return e;
     if (grid < 1)
         return cudaSuccess;
     k_mlp_fused<<<grid, kFusedThreads, smem, s>>>(p, feat, ld_feat, count_host, count_dev, max_rows, out, s_row, s_mem,

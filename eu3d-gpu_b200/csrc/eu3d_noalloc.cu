@@ -24,9 +24,13 @@ constexpr size_t kScratchBytes = size_t(16) << 20; // EU_MLP_NOALLOC_SCRATCH_BYT
 constexpr size_t kAlign = 256;
 static_assert(kScratchBytes == EU_MLP_NOALLOC_SCRATCH_BYTES, "header and library disagree on the scratch size");
 
-// Every GPU that loads the library holds this array until the process exits.
+// The array is device memory of this file's own CUDA module. CUDA loads
+// modules lazily, so the array takes its 16 MiB on a device when its address
+// is first looked up there: eu_mlp_init does that on the model's device
+// (eu3d::noalloc_setup), before the caller can give its free memory away.
+// From then on the device holds the array until the process exits.
 // In host code the name is only a stand-in for the symbol: the device address
-// comes from cudaGetSymbolAddress, once per device (scratch_on()).
+// comes from cudaGetSymbolAddress, once per device.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
@@ -35,16 +39,25 @@ unsigned char *g_scratch_addr[kMaxDevices] = {};
 
 size_t round_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 
-// Device address of the scratch array on `device` (the current device).
+cudaError_t lookup_locked(int device)
+{
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+        return e;
+    g_scratch_addr[device] = static_cast<unsigned char *>(p);
+    return cudaSuccess;
+}
+
+// Device address of the scratch array on `device` (the current device), as
+// the set-up recorded it.
 cudaError_t scratch_on(int device, unsigned char **out)
 {
     std::lock_guard<std::mutex> guard(g_lock);
     if (!g_scratch_addr[device]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        const cudaError_t e = lookup_locked(device);
         if (e != cudaSuccess)
             return e;
-        g_scratch_addr[device] = static_cast<unsigned char *>(p);
     }
     *out = g_scratch_addr[device];
     return cudaSuccess;
@@ -66,6 +79,18 @@ eu_status fail_cuda(eu_mlp *m, cudaError_t e, const char *what)
 }
 
 } // namespace
+
+// Set-up, with `device` current: load the array there and record its address.
+// It runs at every eu_mlp_init, so a model created again after a
+// cudaDeviceReset (which unloads the module and drops every allocation,
+// the model's own included) records the new address.
+cudaError_t eu3d::noalloc_setup(int device)
+{
+    if (device < 0 || device >= kMaxDevices)
+        return cudaSuccess; // eu_mlp_predict_noalloc rejects such a device
+    std::lock_guard<std::mutex> guard(g_lock);
+    return lookup_locked(device);
+}
 
 extern "C" eu_status eu_mlp_predict_noalloc(eu_mlp *m, const float *X, long long n, float *out)
 {

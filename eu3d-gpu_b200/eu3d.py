@@ -158,6 +158,12 @@ def library():
             getattr(lib, fn).restype = _I
         lib.eu_mlp_predict_fused.argtypes = [_P, _P, ctypes.c_longlong, _P]
         lib.eu_mlp_predict_fused.restype = _I
+        lib.eu_mlp_predict_fused_async.argtypes = [_P, _P, ctypes.c_longlong, _P]
+        lib.eu_mlp_predict_fused_async.restype = _I
+        lib.eu_mlp_sync.argtypes = [_P]
+        lib.eu_mlp_sync.restype = _I
+        lib.eu_mlp_stream.argtypes = [_P, ctypes.POINTER(_P)]
+        lib.eu_mlp_stream.restype = _I
         lib.eu_mlp_predict_noalloc.restype = _I
         for fn in ("eu_mlp_create", "eu_mlp_destroy", "eu_mlp_gemm", "eu_mlp_init", "eu_mlp_set_scaling",
                    "eu_mlp_get_params", "eu_mlp_set_params", "eu_mlp_loss_grad", "eu_mlp_train", "eu_mlp_predict"):
@@ -542,6 +548,36 @@ class Mlp:
         """predict() from the one persistent tensor-core kernel the learned
         timestep uses (eu_mlp_predict_fused)."""
         self._check(library().eu_mlp_predict_fused(self.h, X.data_ptr(), X.shape[0], out.data_ptr()), "predict_fused")
+
+    def predict_fused_async(self, X, out):
+        """predict_fused() queued on the model's stream without waiting
+        (eu_mlp_predict_fused_async); sync() waits and checks."""
+        self._check(library().eu_mlp_predict_fused_async(self.h, X.data_ptr(), X.shape[0], out.data_ptr()),
+                    "predict_fused_async")
+
+    def sync(self):
+        self._check(library().eu_mlp_sync(self.h), "sync")
+
+    def stream(self):
+        """The model's CUDA stream handle (eu_mlp_stream)."""
+        s = _P()
+        self._check(library().eu_mlp_stream(self.h, ctypes.byref(s)), "stream")
+        return s.value
+
+    def time_fused_queue(self, X, out, reps=5):
+        """Milliseconds per launch of the fused inference on X: CUDA events on
+        the model's stream around reps back-to-back launches, one check at the
+        end."""
+        import torch
+        self.predict_fused(X, out)
+        stream = torch.cuda.ExternalStream(self.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            self.predict_fused_async(X, out)
+        e1.record(stream)
+        self.sync()
+        return e0.elapsed_time(e1) / reps
 
     def predict_noalloc(self, X, out):
         """predict() with its scratch in the library's fixed device array

@@ -467,6 +467,9 @@ eu_status eu_mlp_init(eu_mlp *m, int n_in, int width, int hidden_layers, int n_o
             return s;
     }
     MCK(m, cudaStreamSynchronize(m->stream));
+    // the no-allocation entry point's fixed array is loaded on this device now,
+    // before the caller can hand its free memory to a pool of its own
+    MCK(m, eu3d::noalloc_setup(m->device));
     m->ready = true;
     return EU_OK;
 }
@@ -648,6 +651,42 @@ eu_status eu_mlp_predict_fused(eu_mlp *m, const float *X, long long n, float *ou
     MCK(m, eu3d::mlp_fused(p, X, m->n_in, int(n), nullptr, int(n), out, m->n_out, n * m->n_out, m->d_err, grid,
                            m->stream));
     return check_err(m);
+}
+
+eu_status eu_mlp_predict_fused_async(eu_mlp *m, const float *X, long long n, float *out)
+{
+    if (!m || !X || !out || n < 0 || n > 0x7fffffffLL)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!m->ready)
+        return mfail(m, EU_ERR_NOT_READY, "eu_mlp_init first");
+    if (!m->fused)
+        return mfail(m, EU_ERR_UNSUPPORTED, "the model's shape has no fused inference kernel");
+    cudaSetDevice(m->device);
+    eu3d::FusedMlpParams p;
+    eu3d::mlp_fused_params(m, &p);
+    const long long tiles = (n + 127) / 128;
+    const int grid = int(tiles < m->sms ? tiles : m->sms);
+    MCK(m, eu3d::mlp_fused(p, X, m->n_in, int(n), nullptr, int(n), out, m->n_out, n * m->n_out, m->d_err, grid,
+                           m->stream));
+    return EU_OK;
+}
+
+eu_status eu_mlp_sync(eu_mlp *m)
+{
+    if (!m)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!m->ready)
+        return mfail(m, EU_ERR_NOT_READY, "eu_mlp_init first");
+    cudaSetDevice(m->device);
+    return check_err(m);
+}
+
+eu_status eu_mlp_stream(eu_mlp *m, void **stream)
+{
+    if (!m || !stream)
+        return EU_ERR_INVALID_ARGUMENT;
+    *stream = m->stream;
+    return EU_OK;
 }
 
 eu_status eu_mlp_predict(eu_mlp *m, const float *X, long long n, float *out)

@@ -32,6 +32,10 @@ struct MlpLayerView {
 };
 bool mlp_view(const eu_mlp *m, MlpView *v);
 bool mlp_layer_view(const eu_mlp *m, int member, int layer, MlpLayerView *v);
+// Loads the no-allocation entry point's fixed scratch array on `device` (the
+// current device) and records its device address (eu3d_noalloc.cu); called by
+// eu_mlp_init, so the array exists from the model's set-up on.
+cudaError_t noalloc_setup(int device);
 // Records msg as the model's last error and returns s.
 eu_status mlp_fail(eu_mlp *m, eu_status s, const char *msg);
 // The fused inference kernel: whether the model's shape has one, its launch

@@ -345,6 +345,17 @@ eu_status eu_mlp_predict(eu_mlp *m, const float *X, long long n, float *out);
  * (its DNN scheme runs no model, src/Euler.cpp:1473-1480). */
 eu_status eu_mlp_predict_fused(eu_mlp *m, const float *X, long long n, float *out);
 
+/* eu_mlp_predict_fused without waiting: the kernel is queued on the model's
+ * stream (eu_mlp_stream) and the call returns. X and out must stay valid until
+ * that stream has run it. eu_mlp_sync waits for the stream and reports a
+ * tensor-core pipeline wait that gave up (EU_ERR_TIMEOUT) in any work queued
+ * since the last check. For callers that overlap inference with other work
+ * and for timing the kernel with events on that stream. No counterpart in the
+ * reference. */
+eu_status eu_mlp_predict_fused_async(eu_mlp *m, const float *X, long long n, float *out);
+eu_status eu_mlp_sync(eu_mlp *m);
+eu_status eu_mlp_stream(eu_mlp *m, void **stream);
+
 /* eu_mlp_predict without any device allocation, for callers that cannot call
  * cudaMalloc while they run: a solver that gives all free device memory to its
  * own pool after start-up (where a library's allocation fails or fragments
@@ -352,13 +363,18 @@ eu_status eu_mlp_predict_fused(eu_mlp *m, const float *X, long long n, float *ou
  * cudaMalloc/cudaFree. It has no counterpart in the reference.
  * Same inputs, outputs and results as eu_mlp_predict. The scratch (packed
  * inputs, hidden activations, outputs before unscaling, an error flag) is one
- * fixed array of EU_MLP_NOALLOC_SCRATCH_BYTES in the library's device memory,
- * held on every GPU that loads the library until the process exits; n may be
+ * fixed array of EU_MLP_NOALLOC_SCRATCH_BYTES in the library's device memory.
+ * eu_mlp_init loads it on the model's device and looks up its device address
+ * there (CUDA loads the library's modules lazily, so this is when the device
+ * memory is taken); from then on that GPU holds it until the process exits.
+ * Create the model before handing free device memory to a pool of your own,
+ * and before any stream capture. After a cudaDeviceReset the model is gone
+ * with the rest of the device's memory: eu_mlp_init of a new one looks the
+ * address up again. n may be
  * at most (EU_MLP_NOALLOC_SCRATCH_BYTES - 1024) / (2 in_pad + 4 width + 4
  * out_pad) rows (in_pad, out_pad: n_in, n_out rounded up to 16), 14978 for
  * the 12 -> 256 x 3 -> 10 chemistry model; more is EU_ERR_INVALID_ARGUMENT.
- * The first call on a device looks up the array's device address (once per
- * device); make that first call before any stream capture. All calls share
+ * All calls share
  * the one array: calls that overlap on the GPU (other threads, other streams
  * of the same device) race and corrupt each other's results. Returns after
  * the model's stream has finished the work. */

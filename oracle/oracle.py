@@ -76,6 +76,7 @@ class Mechanism:
 
 def write_grid_file(path, ni, nj, nk, xa, xb, ya, yb, za, zb, bc=2):
     """A grid file in the reference's ``key value`` format (input/grid-3dRSBI.txt)."""
+    xa, xb, ya, yb, za, zb = (float(v) for v in (xa, xb, ya, yb, za, zb))  # repr of a plain float
     with open(path, "w") as f:
         f.write(f"total_ni    {ni}\nxa    {xa!r}\nxb    {xb!r}\n"
                 f"total_nj    {nj}\nya    {ya!r}\nyb    {yb!r}\n"

@@ -16,7 +16,8 @@ for p in (ROOT, os.path.join(ROOT, "oracle"), os.path.join(ROOT, "eu3d-gpu_b200"
         sys.path.insert(0, p)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REFERENCE = "/root/reference"
+# the reference checkout the oracle/_ref build compiles from (absent on GPU boxes)
+REFERENCE = os.environ.get("EU3D_REFERENCE", "/root/reference")
 
 
 def pytest_configure(config):
@@ -42,7 +43,7 @@ def ref_lib():
     checkout is present; it also travels prebuilt to GPU hosts."""
     import oracle
     if not os.path.exists(oracle.REF_LIB) and os.path.isdir(REFERENCE):
-        _make(os.path.join(ROOT, "oracle"), "ref")
+        _make(os.path.join(ROOT, "oracle"), "ref", f"REFERENCE={REFERENCE}")
     if not os.path.exists(oracle.REF_LIB):
         pytest.skip("oracle/_ref not built and the reference sources are not present")
     return oracle.RefOracle

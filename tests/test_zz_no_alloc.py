@@ -41,8 +41,9 @@ def test_noalloc_predict_matches_predict_on_consecutive_calls(gpu):
         free_before = torch.cuda.mem_get_info()[0]
         m.predict_noalloc(X, got)
         torch.cuda.synchronize()
-        if call == 1:  # the first call on the device has set up; this one must not touch the allocator
-            assert torch.cuda.mem_get_info()[0] == free_before
+        # eu_mlp_init has loaded the fixed array: no call, the first included,
+        # may take device memory
+        assert torch.cuda.mem_get_info()[0] == free_before, call
         assert torch.isfinite(got).all(), call
         err = float((got - want).abs().max())
         scale = max(1.0, float(want.abs().max()))
