@@ -5,7 +5,7 @@ Workload: the 3-D reacting shock-bubble case, 256 x 128 x 128 nodes over
 64 x 32 x 32 mm (4,194,304 cells), H2_JA919 kinetics (9 species, 19 reactions),
 Mach 2.83 shock in N2 at 101.325 kPa / 300 K hitting a perturbed 2H2+O2 sphere
 (radius 8 mm, centred 16 mm downstream of the shock, seed 3), fixed dt from the
-reference's CFL rule at 0.5 on the initial state, 500 steps in all. Synthetic
+reference's CFL rule at 0.25 on the initial state, 500 steps in all. Synthetic
 inputs built by eu3d_cases.shock_bubble.
 
 A step is one full timestep: RSBI ghost fill, MUSCL/AUSM flux divergence in x,
@@ -14,7 +14,7 @@ inversion, Nchem prediction and the adaptive trapezoid kinetics.
 
 The timed window: each arm advances the case untimed for WINDOW_START steps,
 until the shock has entered the bubble (it reaches the bubble's upstream
-surface after about 80 steps and runs through the bubble gas from then on),
+surface after about 160 steps and runs through the bubble gas from then on),
 then warms up and times --steps steps there, then runs on to step 500. The
 learned + mixed arm and the plain FP64 arm each run their own trajectory from
 step 0, and their difference is stated at the end of the window and at step 500.
@@ -55,7 +55,13 @@ import eu3d_cases as cases  # noqa: E402  (numpy only; never loads the library)
 METRIC = "Mcell-steps/s reacting, learned+mixed vs plain FP64 on same B200 at ≤1e-3 Y err"
 GRID = (256, 128, 128)
 EXTENT = (0.0, 0.064, 0.0, 0.032, 0.0, 0.032)
-CFL = 0.5
+# The reference's CFL rule (dx, dy only) at 0.25: its forward-Euler MUSCL/AUSM
+# step goes non-finite on this case at 0.5 once the shock runs into the bubble
+# (steps 120-130, FP64 and mixed alike) and at 0.35 by step 240-280; at 0.25 it
+# runs the 500 steps.
+CFL = 0.25
+# the 1-D ZND and 2-D ODW cases run at the reference's usual 0.5
+CFL_THIN = 0.5
 # the config's run length, and the step at which the timed window starts (the
 # shock inside the bubble)
 TOTAL_STEPS = 500
@@ -323,7 +329,7 @@ def _ref_worker(task):
 
 
 def reference_dt(oracle):
-    """The workload's dt by the reference's CFL rule at 0.5 (cases.cfl_dt),
+    """The workload's dt by the reference's CFL rule at CFL (cases.cfl_dt),
     with density and gamma from the NASA polynomials in numpy, on the whole
     grid's nodes of the sub-box holding the shock: the smallest CFL step of
     the grid is in the uniform shocked N2 behind it. (The reference reads grid
@@ -503,7 +509,7 @@ def znd_case(args, local, steps=1000, cells=4000, dx=25e-6):
     s.set_mechanism(mech)
     s.set_state(state_dict((p, cs, T, E)))
     tuned = s.autotune(reps=3)  # a 2 x 2 cross-section: the x-march length matters most
-    st, t_adv = s.step_cfl(steps, CFL)
+    st, t_adv = s.step_cfl(steps, CFL_THIN)
     pr = s.get("P")[0, 2:-2, 2, 2]
     t_end = s.get("T")[0, 2:-2, 2, 2]
     s.close()
@@ -517,62 +523,88 @@ def znd_case(args, local, steps=1000, cells=4000, dx=25e-6):
                                                                  "recover_block": tuned["recover_block"]}}
 
 
-def odw_case(args, local, model, gate, grid=(1024, 512, 2), steps=2000, z_extent=None, phi_seed=None, cfl=CFL):
-    """The oblique detonation case. 2-D (default): 1024 x 512 x 2 nodes over the
-    reference's 2dODW extent (52.5 x 20 mm; the z spacing equals the x spacing).
-    3-D: 384 x 192 x 96 nodes over the 3dODW extent (52.5 x 20 x 20 mm) with the
-    equivalence ratio phi(z) of eu3d_cases.odw_phi on the inflow. Both:
-    a Mach 7.5 stoichiometric H2-air freestream at 40 kPa / 293 K meeting a 25
-    degree wedge (data/input-ODW.txt) in a wedge-aligned frame (the y-low face
-    is the wedge surface), the reference's ODW ghost fill (EU_BC_ODW), the
-    learned + mixed step with each dt from the CFL rule on the device, 2000
-    steps at CFL 0.5 in 2-D, 1000 steps at CFL 0.25 in 3-D (the reference's
-    forward-Euler MUSCL step goes non-finite at CFL 0.5 once the gas ignites
-    on grids as coarse as the 3-D one's, in the C restatement as well). Reports the device throughput, the time
-    advanced, the peak temperature and the shock angle in the middle z plane:
-    where p first exceeds 1.5 x the freestream pressure from the top down,
-    fitted over the middle half of x, plus the wedge angle (the oblique-shock
-    relation gives about 32 degrees for an ideal gas at gamma 1.4)."""
+def odw_case(args, local, model, gate, grid=(1024, 512, 2), steps=2000, extent=(0.040, 0.020, None),
+             phi_seed=None, cfl=CFL_THIN, input_path=None, chem="learned", precision="mixed", keep_y=False):
+    """The oblique detonation case (data/input-ODW-M7.txt: Mach 7, 300 K,
+    101.325 kPa stoichiometric H2-air, a 25 degree wedge whose tip is 5 mm
+    from the inflow face). 2-D (default): 1024 x 512 x 2 nodes over 40 x 20
+    mm (the z spacing equals the x spacing). 3-D: 384 x 192 x 96 nodes over 40
+    x 20 x 10 mm with the equivalence ratio phi(z) of eu3d_cases.odw_phi on
+    the inflow. The grid is wedge-aligned (the y-low face is the wedge surface
+    from the tip on, the freestream ahead of it, eu_set_odw_wall), with the
+    reference's ODW ghost fill (EU_BC_ODW) and each dt from the CFL rule on
+    the device: 2000 steps at CFL 0.5 in 2-D, 1000 steps at CFL 0.25 in 3-D
+    (the reference's forward-Euler MUSCL step goes non-finite at CFL 0.5 once
+    the gas ignites on grids as coarse as the 3-D one's, in the C restatement
+    as well). chem/precision: "learned"/"mixed" or the plain "stiff"/"fp64".
+    Reports the device throughput, the time advanced, the peak temperature
+    and the shock angle in the middle z plane: where p first exceeds 1.5 x the
+    freestream pressure from the top down, fitted over the wedge's middle
+    half, plus the wedge angle (the oblique-shock relation gives about 32
+    degrees for an ideal gas at gamma 1.4)."""
     import eu3d
+    input_path = input_path or cases.INPUT_ODW_M7
     ni, nj, nk = grid
-    dx = 0.0525 / (ni - 1)
-    ext = (0.0, 0.0525, 0.0, 0.02, 0.0, dx * (nk - 1) if z_extent is None else z_extent)
+    dx = extent[0] / (ni - 1)
+    ext = (0.0, extent[0], 0.0, extent[1], 0.0, dx * (nk - 1) if extent[2] is None else extent[2])
     x = cases.node_coordinates(ni, ext[0], ext[1])
     y = cases.node_coordinates(nj, ext[2], ext[3])
     z = cases.node_coordinates(nk, ext[4], ext[5])
     mech = eu3d.parse_mechanism(cases.MECH_JA919, cases.THERMO)
     phi = cases.odw_phi(z, seed=phi_seed) if phi_seed is not None else None
-    prim, inflow = cases.odw(x, y, z, mech, phi=phi)
+    prim, inflow = cases.odw(x, y, z, mech, input_path=input_path, phi=phi)
     p, cs, T, E = eu3d.initial_state(mech, ni, nj, nk, *prim)
-    chem = "learned" if model is not None else "stiff"
-    s = eu3d.Solver(ni, nj, nk, ext, precision="mixed", chemistry=chem, arith="fast", device=local, boundary="odw")
+    if chem == "learned" and model is None:
+        chem = "stiff"
+    s = eu3d.Solver(ni, nj, nk, ext, precision=precision, chemistry=chem, arith="fast", device=local,
+                    boundary="odw")
     s.set_mechanism(mech)
     s.set_state(state_dict((p, cs, T, E)))
     s.set_inflow(*inflow)
-    if model is not None:
+    wall = cases.odw_wall_node(x, input_path)
+    s.set_odw_wall(wall)
+    if chem == "learned":
         import learned
         learned.attach(s, model, gate)
     tuned = s.autotune(reps=3)
     st, t_adv = s.step_cfl(steps, cfl)
     pr = s.get("P")[0, 2:-2, 2:-2, 2 + nk // 2]  # the middle z plane
     t_end = s.get("T")[0, 2:-2, 2:-2, :]
+    yi = s.get("Yi") if keep_y else None
     s.close()
-    p0 = eu3d.read_value(cases.INPUT_ODW, "P")
-    angle = eu3d.read_value(cases.INPUT_ODW, "angle")
+    p0 = eu3d.read_value(input_path, "P")
+    angle = eu3d.read_value(input_path, "angle")
     xs, hs = [], []
-    for i in range(ni // 4, 3 * ni // 4):
+    span = ni - wall
+    for i in range(wall + span // 4, wall + 3 * span // 4):
         hit = np.nonzero(pr[i, ::-1] > 1.5 * p0)[0]
         if hit.size:
             xs.append(x[2 + i])
             hs.append(y[2 + nj - 1 - hit[0]])
     beta = (math.degrees(math.atan(np.polyfit(xs, hs, 1)[0])) + angle) if len(xs) > 8 else None
-    return {"grid": list(grid), "steps": steps, "cfl": cfl, "time_advanced_s": t_adv, "chemistry": chem,
-            "value": round(ni * nj * nk * steps / (st["device_ms"] / 1e3) / 1e6, 3), "unit": "Mcell-steps/s",
-            "ms_per_step": round(st["device_ms"] / steps, 4), "peak_T_K": round(float(t_end.max()), 1),
-            "peak_p_Pa": round(float(pr.max()), 1), "shock_angle_deg": None if beta is None else round(beta, 2),
-            "learned_cells_last_step": st["learned"], "fallback_cells_last_step": st["fallback"],
-            "max_nchem_last_step": st["max_nchem"],
-            "autotune": {"flux_ci": tuned["flux_ci"], "recover_block": tuned["recover_block"]}}
+    out = {"grid": list(grid), "extent_m": [ext[1], ext[3], ext[5]], "steps": steps, "cfl": cfl,
+           "time_advanced_s": t_adv, "chemistry": chem, "precision": precision,
+           "freestream": {k: eu3d.read_value(input_path, k) for k in ("Mach", "P", "T")}, "wall_first_node": wall,
+           "value": round(ni * nj * nk * steps / (st["device_ms"] / 1e3) / 1e6, 3), "unit": "Mcell-steps/s",
+           "ms_per_step": round(st["device_ms"] / steps, 4), "peak_T_K": round(float(t_end.max()), 1),
+           "peak_p_Pa": round(float(pr.max()), 1), "shock_angle_deg": None if beta is None else round(beta, 2),
+           "learned_cells_last_step": st["learned"], "fallback_cells_last_step": st["fallback"],
+           "max_nchem_last_step": st["max_nchem"],
+           "autotune": {"flux_ci": tuned["flux_ci"], "recover_block": tuned["recover_block"]}}
+    return (out, yi) if keep_y else out
+
+
+def odw_2d(args, local, model, gate):
+    """Config 2: the 2-D oblique detonation, plain FP64 stiff against learned +
+    mixed, each 2000 steps at CFL 0.5 from the same initial state, with the
+    species L1 and the reaction-front shift between the two at the end."""
+    plain, y_ref = odw_case(args, local, model, gate, chem="stiff", precision="fp64", keep_y=True)
+    fast, y_fast = odw_case(args, local, model, gate, keep_y=True)
+    l1 = np.abs(y_fast - y_ref)[:, 2:-2, 2:-2, 2:-2].sum(axis=0)
+    return {"plain_fp64": plain, "learned_mixed": fast,
+            "speedup": round(fast["value"] / plain["value"], 3) if plain["value"] else None,
+            "species_l1_mean": float(l1.mean()), "species_l1_max": float(l1.max()),
+            "reaction_front_shift_cells": cases.front_shift(y_fast, y_ref)}
 
 
 BATCH_SIZES = ((64, 64, 64), (128, 64, 64), (192, 96, 96))
@@ -698,7 +730,7 @@ def our_arm_blocks(args, world, rank, local, dist):
     p, cs, T, E = eu3d.initial_state(mech, ni, nj, nk, *prim)
     sd = state_dict((p, cs, T, E))
     ncell = ni * nj * nk
-    # dt: the reference's CFL rule at 0.5, minimum over the blocks
+    # dt: the reference's CFL rule, minimum over the blocks
     dt_t = torch.tensor([cases.cfl_dt(x, y, p[0], p[1], p[2], p[3], p[6], CFL)], dtype=torch.float64, device=device)
     dist.all_reduce(dt_t, op=dist.ReduceOp.MIN)
     dt = float(dt_t.item())
@@ -950,12 +982,12 @@ def our_arm(args):
         except eu3d.EU3DError as e:  # reported, not fatal to the headline measurement
             znd = {"error": str(e)}
         try:
-            odw = odw_case(args, local, model, gate)
+            odw = odw_2d(args, local, model, gate)
         except eu3d.EU3DError as e:
             odw = {"error": str(e)}
         try:
-            odw3 = odw_case(args, local, model, gate, grid=(384, 192, 96), steps=1000, z_extent=0.02, phi_seed=4,
-                            cfl=0.25)
+            odw3 = odw_case(args, local, model, gate, grid=(384, 192, 96), steps=1000, extent=(0.040, 0.020, 0.010),
+                            phi_seed=4, cfl=0.25)
         except eu3d.EU3DError as e:
             odw3 = {"error": str(e)}
 
@@ -1011,7 +1043,7 @@ def our_arm(args):
                            "grid": list(grid), "dt": dt,
                            "window": {"start_step": start, "timed_steps": [start + args.warmup, window_end],
                                       "run_steps": run_end,
-                                      "why": "the shock reaches the bubble after about 80 steps; from then on it "
+                                      "why": "the shock reaches the bubble after about 160 steps; from then on it "
                                              "runs through the bubble gas"},
                            "precision": args.precision, "chemistry": args.chem,
                            "arith": args.arith, "parallelism": f"replicas x{world}", "autotune": tuned,
@@ -1019,7 +1051,7 @@ def our_arm(args):
                 "window_state": {**window,
                                  "note": "the transmitted shock heats the bubble gas to about 600 K and the "
                                          "shocked N2 is at 745 K: below the 800 K activity threshold, no radical "
-                                         "pool forms and no cell ignites within the run's 500 steps (49 us), so "
+                                         "pool forms and no cell ignites within the run's 500 steps (24.5 us), so "
                                          "the learned path finds no chemically active cell; reacting_block is "
                                          "the figure on igniting gas"},
                 "plain_fp64": plain,

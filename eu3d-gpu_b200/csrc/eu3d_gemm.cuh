@@ -23,15 +23,35 @@ constexpr int kGemmBM = 128, kGemmBK = 64, kGemmThreads = 128;
 
 // Epilogue modes: 0 none, 1 SiLU, 2 multiply by SiLU'(Z) (backward through an
 // activation whose pre-activation Z is given), 3 accumulate into Cf with
-// atomics (split-K partial sums; no bias).
-enum GemmAct { kActNone = 0, kActSilu = 1, kActSiluGrad = 2, kActAccumulate = 3 };
+// atomics (split-K partial sums; no bias), 4 SiLU in its inference form
+// (silu_fast, the fused inference kernel's activation).
+enum GemmAct { kActNone = 0, kActSilu = 1, kActSiluGrad = 2, kActAccumulate = 3, kActSiluFast = 4 };
 
 // SiLU with the hardware's approximate division (reciprocal and multiply, about
 // two units in the last place): the activations are rounded to bf16 next, eight
 // bits of mantissa, so the division's last bits rarely survive. For x below
 // about -87 the denominator overflows and the result is 0 (the exact value is
-// below 1e-36 in magnitude).
+// below 1e-36 in magnitude). Training's forward pass uses this form.
 __device__ __forceinline__ float silu(float x) { return __fdividef(x, 1.0f + __expf(-x)); }
+
+// SiLU for inference: x sigmoid(x) = h + h tanh(h), h = x / 2, with the
+// hardware's approximate tanh, one special-function instruction (relative
+// error below 2^-10.9) instead of the two (exponential, reciprocal) of silu();
+// those instructions bound the fused inference kernel's epilogues. The value
+// is rounded to bf16 next, whose spacing is 2^-8 relative, so the two forms
+// give the same activation except near bf16 rounding midpoints. For large |x|
+// tanh saturates at +-1 and the result is x or 0.
+__device__ __forceinline__ float tanh_approx(float x)
+{
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float silu_fast(float x)
+{
+    const float h = 0.5f * x;
+    return fmaf(h, tanh_approx(h), h);
+}
 __device__ __forceinline__ float silu_grad(float z)
 {
     const float s = 1.0f / (1.0f + __expf(-z));
@@ -173,6 +193,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                             Cpre[o] = x;
                         if (act == kActSilu)
                             x = silu(x);
+                        else if (act == kActSiluFast)
+                            x = silu_fast(x);
                         else if (act == kActSiluGrad)
                             x *= silu_grad(Z[o]);
                         if (Cf)

@@ -71,8 +71,12 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
         dst = cell_index(g, i, j, k);
         src = cell_index(g, i, sj, k);
         if (q < bc) {
-            sv = -1;
-            rebuild = true;
+            if (g.bc_kind == 2 && i - bc < g.wall_i0) {
+                inflow = k - bc; // ODW ahead of the wall: the freestream (first table row)
+            } else {
+                sv = -1;
+                rebuild = true;
+            }
         }
     } else {
         // the ghost index runs fastest: the 2 bc ghosts of one (i, j) row sit in
@@ -342,8 +346,8 @@ __global__ void __launch_bounds__(128) k_flux_update_cols(const DevGrid g, const
 // from HBM once per plane instead of once per stencil point, and the loads of
 // the next plane overlapped with the current plane's arithmetic.
 //
-// A block owns a kTileJ x kTileK tile of (j, k) columns and marches along x
-// with kTileJ + 1 warps. Warps 0 .. kTileJ-1 own a row of cells each: every
+// A block owns a kTileJ x kTileK tile of (j, k) columns (TileShape) and
+// marches along x with kTileJ + 1 warps. Warps 0 .. kTileJ-1 own a row of cells each: every
 // thread keeps its column's x-stencil (planes i-1 .. i+2 of every primitive) in
 // registers and loads plane i+3 one node ahead. Plane i of the tile plus a
 // two-node halo in j and k is staged in shared memory, from which the y- and
@@ -360,26 +364,35 @@ __global__ void __launch_bounds__(128) k_flux_update_cols(const DevGrid g, const
 // forms a fourth face, so no warp waits at the plane's barrier for another's
 // extra face. Partial tiles: the faces of the valid rows/columns are formed,
 // including the one past the last valid row/column.
-constexpr int kTileK = 32, kTileJ = 7, kTileWarps = kTileJ + 1;
-constexpr int kTileRows = kTileJ + 4, kTileCols = kTileK + 4;
-// staged by cp.async: rows 0, 1 and kTileJ + 3 over the full width, and the
-// two columns each side of rows 2 .. kTileJ + 2 (the cell rows and the edge
-// warp's row)
-constexpr int kTileHalo = 3 * kTileCols + 4 * (kTileJ + 1);
+//
+// Tile height: 7 cell rows (8 warps) in FP32; 3 cell rows (4 warps) in FP64,
+// whose x-stencil window takes twice the registers, so that two blocks still
+// fit per SM (98 KB of shared memory each).
+constexpr int kTileK = 32, kTileCols = kTileK + 4;
+template <typename R>
+struct TileShape {
+    static constexpr int J = sizeof(R) == 4 ? 7 : 3; // cell rows
+    static constexpr int Warps = J + 1, Rows = J + 4;
+    // staged by cp.async: rows 0, 1 and J + 3 over the full width, and the
+    // two columns each side of rows 2 .. J + 2 (the cell rows and the edge
+    // warp's row)
+    static constexpr int Halo = 3 * kTileCols + 4 * (J + 1);
+};
 
 template <int NS, typename R>
 constexpr size_t tiled_flux_smem_bytes()
 {
-    return sizeof(double) * (NS + 4) * kTileJ * kTileK + sizeof(R) * 2 * (7 + NS) * kTileRows * kTileCols +
-           sizeof(R) * (NS + 4) * ((kTileJ + 1) * kTileK + kTileJ * (kTileK + 1));
+    constexpr int J = TileShape<R>::J, Rows = TileShape<R>::Rows;
+    return sizeof(double) * (NS + 4) * J * kTileK + sizeof(R) * 2 * (7 + NS) * Rows * kTileCols +
+           sizeof(R) * (NS + 4) * ((J + 1) * kTileK + J * (kTileK + 1));
 }
 
 // Face flux from four consecutive stencil points of the staged plane tile,
 // starting at (r, c) and stepping (DR, DC). own: the values of stencil point 2
 // when that point is the thread's own node (kept in registers), else null.
 template <int NS, int DIR, int DR, int DC, typename R, bool kStrict, bool kOwn>
-__device__ __forceinline__ void tile_face_flux(const R (*sP)[kTileRows][kTileCols], int r, int c, const R *own,
-                                               R (&F)[NS + 4])
+__device__ __forceinline__ void tile_face_flux(const R (*sP)[TileShape<R>::Rows][kTileCols], int r, int c,
+                                               const R *own, R (&F)[NS + 4])
 {
     face_ausm<NS, DIR, R, kStrict, R>(
         [&](int f, int p) { return (kOwn && p == 2) ? own[f] : sP[f][r + p * DR][c + p * DC]; }, F);
@@ -392,11 +405,13 @@ __device__ __forceinline__ void window_face_flux(const R (&w)[4][7 + NS], R (&F)
 }
 
 template <int NS, typename R, bool kStrict>
-__global__ void __launch_bounds__(kTileK *kTileWarps, 2)
+__global__ void __launch_bounds__(kTileK *TileShape<R>::Warps, 2)
     k_flux_update_tiled(const DevGrid g, const DevState st, const R *__restrict__ prim, const double *__restrict__ dt_dev,
                         int ci)
 {
     constexpr int NP = 7 + NS, NV = NS + 4;
+    constexpr int kTileJ = TileShape<R>::J, kTileWarps = TileShape<R>::Warps, kTileRows = TileShape<R>::Rows;
+    constexpr int kTileHalo = TileShape<R>::Halo;
     using Plane = R[NP][kTileRows][kTileCols];
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double(*sC)[kTileJ][kTileK] = reinterpret_cast<double(*)[kTileJ][kTileK]>(smem_raw);
@@ -455,7 +470,12 @@ __global__ void __launch_bounds__(kTileK *kTileWarps, 2)
         }
         if (halo) {
 #pragma unroll
-            for (int f = 0; f < NP; ++f) tc::cp_async4(&stage[s][f][hr][hc], prim + f * n3 + hcol + p * sx);
+            for (int f = 0; f < NP; ++f) {
+                if constexpr (sizeof(R) == 4)
+                    tc::cp_async4(&stage[s][f][hr][hc], prim + f * n3 + hcol + p * sx);
+                else
+                    tc::cp_async8(&stage[s][f][hr][hc], prim + f * n3 + hcol + p * sx);
+            }
         }
         tc::cp_async_commit();
     };
@@ -1343,6 +1363,26 @@ __global__ void k_derived(const __grid_constant__ DevMech m, const DevGrid g, co
         }
     }
     out[c] = v;
+}
+
+// Stage combination of the three-stage TVD Runge-Kutta advection (Shu and
+// Osher's SSP-RK3; the reference's TimeAdv::TVD_RK3, src/TimeAdv.cpp:210-221,
+// is an empty stub): CS = a CS0 + b CS on the interior nodes, each product and
+// the sum rounded separately (the same value in every arithmetic flavour).
+__global__ void k_rk_combine(const DevGrid g, double *__restrict__ cs, const double *__restrict__ cs0, int planes,
+                             double a, double b)
+{
+    const long long n = (long long)g.ni * g.nj * g.nk;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        interior_node(g, t, i, j, k);
+        const long long c = cell_index(g, i, j, k);
+        for (int q = 0; q < planes; ++q) {
+            const long long o = q * g.n3 + c;
+            cs[o] = __dadd_rn(__dmul_rn(a, cs0[o]), __dmul_rn(b, cs[o]));
+        }
+    }
 }
 
 // Writes a scalar (the timestep) into device memory from a kernel argument, so

@@ -54,9 +54,10 @@ cudaError_t tiled_flux_launch(const LaunchArgs &a, const R *prim)
     const cudaError_t e = limit.ensure(k_flux_update_tiled<NS, R, kStrict>, smem);
     if (e != cudaSuccess)
         return e;
-    const dim3 block(kTileK, kTileWarps);
+    const dim3 block(kTileK, TileShape<R>::Warps);
     const int ci = a.flux_ci > 0 ? a.flux_ci : 16;
-    const dim3 grid((g.nk + kTileK - 1) / kTileK, (g.nj + kTileJ - 1) / kTileJ, (g.ni + ci - 1) / ci);
+    const dim3 grid((g.nk + kTileK - 1) / kTileK, (g.nj + TileShape<R>::J - 1) / TileShape<R>::J,
+                    (g.ni + ci - 1) / ci);
     k_flux_update_tiled<NS, R, kStrict><<<grid, block, smem, a.stream>>>(g, a.st, prim, a.dt_dev, ci);
     return cudaGetLastError();
 }
@@ -83,10 +84,11 @@ cudaError_t flux_t(const LaunchArgs &a)
         return cols_flux_launch<NS, double, kStrictFlux>(a, a.st.prim);
     }
     // mixed precision: FP32 reconstruction and AUSM (always the division-light
-    // forms), plane-tiled
+    // forms); FP64: the reference's forms (strict) or the division-light
+    // limiter (fast). Both plane-tiled.
     if (a.precision == 1)
         return tiled_flux_launch<NS, float, false>(a, a.st.prim32);
-    return flux_launch<NS, double, kStrictFlux>(a, a.st.prim);
+    return tiled_flux_launch<NS, double, kStrictFlux>(a, a.st.prim);
 }
 
 template <int NS, int NR>
@@ -296,6 +298,14 @@ cudaError_t launch_halo(const LaunchArgs &a, int nf, int face, bool pack, void *
     else
         k_halo_copy<double><<<blocks, 256, 0, a.stream>>>(a.st.prim, static_cast<double *>(msg), nf, g.bc, g.n3, plane,
                                                         first, step, pack);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rk_combine(const LaunchArgs &a, const double *cs0, double ca, double cb)
+{
+    const long long n = (long long)a.g.ni * a.g.nj * a.g.nk;
+    const unsigned blocks = unsigned(std::min<long long>((n + 255) / 256, (long long)(a.sms > 0 ? a.sms : 148) * 8));
+    k_rk_combine<<<blocks, 256, 0, a.stream>>>(a.g, a.st.cs, cs0, a.mech->ns + 4, ca, cb);
     return cudaGetLastError();
 }
 

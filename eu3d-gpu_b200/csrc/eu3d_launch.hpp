@@ -49,6 +49,7 @@ struct Launchers {
     cudaError_t launch_recover_react(const LaunchArgs &a, bool react);                             \
     cudaError_t launch_derived(const LaunchArgs &a, int which, double *out);                       \
     cudaError_t launch_set_value(double *dst, double v, cudaStream_t s);                           \
+    cudaError_t launch_rk_combine(const LaunchArgs &a, const double *cs0, double ca, double cb);   \
     cudaError_t launch_cfl(const LaunchArgs &a, double cfl, unsigned long long *slot, double *time); \
     cudaError_t launch_recover_classify(const LaunchArgs &a, const LearnedParams &lp);             \
     cudaError_t launch_learned_features(const LaunchArgs &a, const LearnedParams &lp);             \

@@ -9,11 +9,11 @@ namespace eu3d {
 
 // The fused inference kernel (eu3d_mlp_fused.cuh): model shape, packed weight
 // slabs and per-layer biases.
-constexpr int kFusedMaxMembers = 8, kFusedMaxLayers = 9, kFusedSlabK = 64;
+constexpr int kFusedMaxMembers = 8, kFusedMaxLayers = 9, kFusedSlabK = 32;
 struct FusedMlpParams {
     int members, layers; // layers = hidden + output
     int n_in, in_pad, width, out_pad, n_out;
-    const void *slabs;                                    // bf16, K-slabs of 64 columns in core-matrix layout
+    const void *slabs;                                    // bf16, K-slabs of kFusedSlabK columns, core-matrix layout
     long long off[kFusedMaxMembers][kFusedMaxLayers];     // element offset of layer (e, l)'s first slab
     const float *bias[kFusedMaxMembers][kFusedMaxLayers]; // [N] per layer
     const float *in_shift, *in_scale, *out_shift, *out_scale;

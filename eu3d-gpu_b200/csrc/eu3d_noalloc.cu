@@ -147,7 +147,7 @@ extern "C" eu_status eu_mlp_predict_noalloc(eu_mlp *m, const float *X, long long
             eu3d::mlp_layer_view(m, member, l, &L);
             const void *A = l == 0 ? xs : h[(l - 1) & 1];
             const int lda = l == 0 ? v.in_pad : v.width;
-            NCK(eu3d::gemm_bf16(A, lda, L.Wb, L.in_pad, rows, L.out_pad, L.in_pad, L.b, 1, nullptr, h[l & 1],
+            NCK(eu3d::gemm_bf16(A, lda, L.Wb, L.in_pad, rows, L.out_pad, L.in_pad, L.b, 4, nullptr, h[l & 1],
                                 nullptr, v.width, nullptr, 1, err, s));
         }
         eu3d::mlp_layer_view(m, member, v.hidden, &L);

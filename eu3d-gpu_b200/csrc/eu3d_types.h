@@ -57,6 +57,9 @@ struct DevGrid {
     // x faces whose ghost nodes come from a neighbouring block (halo exchange)
     // instead of the boundary condition
     int exch_lo, exch_hi;
+    // EU_BC_ODW: y-low ghosts of local x nodes below wall_i0 take the freestream
+    // (the wedge surface starts there); 0: the wall runs along the whole face
+    int wall_i0;
 };
 
 // Primitive planes the stencils read, in this order (haloed, FP64).

@@ -116,6 +116,16 @@ def library():
         lib.eu_read_state.argtypes = [_P, ctypes.c_char_p, ctypes.POINTER(_I), ctypes.POINTER(_I),
                                       ctypes.POINTER(_D), ctypes.POINTER(_D)]
         lib.eu_read_state.restype = _I
+        lib.eu_set_time_scheme.argtypes = [_P, _I]
+        lib.eu_set_time_scheme.restype = _I
+        lib.eu_set_odw_wall.argtypes = [_P, _I]
+        lib.eu_set_odw_wall.restype = _I
+        lib.eu_output_async.argtypes = [_P, _I, ctypes.c_char_p, _I, _I, _D, _D]
+        lib.eu_output_async.restype = _I
+        lib.eu_output_wait.argtypes = [_P]
+        lib.eu_output_wait.restype = _I
+        lib.eu_write_tecplot.argtypes = [_P, ctypes.c_char_p]
+        lib.eu_write_tecplot.restype = _I
         lib.eu_chem_states.argtypes = [_P, ctypes.c_longlong, _P, _P, _P, _P, _P]
         lib.eu_chem_advance.argtypes = [_P, ctypes.c_longlong, _P, _P, _P, _P, _P]
         lib.eu_set_learned.argtypes = [_P, _P, ctypes.POINTER(LearnedConfig)]
@@ -340,6 +350,16 @@ class Solver:
         arrs = [_c(a) for a in (P, T, U, V, W, Y)]
         self._check(library().eu_set_inflow(self.h, *[a.ctypes.data for a in arrs]), "set_inflow")
 
+    def set_time_scheme(self, scheme):
+        """Advection time scheme: "ee" (the reference's Euler explicit) or
+        "rk3" (three-stage TVD Runge-Kutta; eu_set_time_scheme)."""
+        self._check(library().eu_set_time_scheme(self.h, {"ee": 0, "rk3": 1}[scheme]), "set_time_scheme")
+
+    def set_odw_wall(self, first_wall_node):
+        """EU_BC_ODW: the y-low wall starts at this global x node; the face
+        ahead of it takes the freestream (eu_set_odw_wall)."""
+        self._check(library().eu_set_odw_wall(self.h, int(first_wall_node)), "set_odw_wall")
+
     def step(self, nsteps, dt, stats=True):
         s = StepStats()
         st = library().eu_step(self.h, int(nsteps), float(dt), ctypes.byref(s) if stats else None)
@@ -410,6 +430,21 @@ class Solver:
         self._check(library().eu_read_state(self.h, str(path).encode(), ctypes.byref(it), ctypes.byref(num),
                                             ctypes.byref(t), ctypes.byref(dt)), "read_state")
         return it.value, num.value, t.value, dt.value
+
+    def output_async(self, path, kind="state", iteration=0, num=0, final_time=0.0, dt=0.0):
+        """Queue an output file of the current state (eu_output_async): kind
+        "state" (EU3D_STATE_V1_LE dump) or "tecplot"; stepping may continue
+        at once, output_wait() waits for the file."""
+        k = {"state": 0, "tecplot": 1}[kind]
+        self._check(library().eu_output_async(self.h, k, str(path).encode(), int(iteration), int(num),
+                                              float(final_time), float(dt)), "output_async")
+
+    def output_wait(self):
+        self._check(library().eu_output_wait(self.h), "output_wait")
+
+    def write_tecplot(self, path):
+        """The reference's Tecplot file of the current state (eu_write_tecplot)."""
+        self._check(library().eu_write_tecplot(self.h, str(path).encode()), "write_tecplot")
 
     def halo_bytes(self):
         """Bytes of one halo message (eu_halo_bytes)."""

@@ -9,13 +9,15 @@
   input-1dZND.txt in the reference's key/value format (P_bound, T_bound, P, T,
   and driver_nodes, this build's addition). The reference's ZND case is dead
   code (its boundary is commented out and its initialiser hard-codes RSBI).
-* ``odw`` — the oblique detonation wave cases: a Mach 7.5 H2-air freestream
-  (input-ODW.txt: P, T, Mach, wedge angle) meeting a 25 degree wedge. The
+* ``odw`` — the oblique detonation wave cases: an H2-air freestream
+  (input-ODW.txt: Mach 7.5, 40 kPa, 293 K; input-ODW-M7.txt: Mach 7,
+  101.325 kPa, 300 K; both a 25 degree wedge) meeting the wedge. The
   reference's FieldBoundary_3dODW has a symmetry (reflecting) y-low face and
   x-low inflow tables it never fills; here the grid is wedge-aligned: the
-  y-low face is the wedge surface, the tip at x = 0, and the freestream (the
-  inflow tables and the initial field) arrives at the wedge angle. Optional
-  equivalence ratio phi(z) for the 3-D case.
+  y-low face is the wedge surface, the tip at x = wedge_x (0 when the file has
+  none; ahead of it the face takes the freestream, eu_set_odw_wall), and the
+  freestream (the inflow tables and the initial field) arrives at the wedge
+  angle. Optional equivalence ratio phi(z) for the 3-D case.
 * ``shock_bubble`` — the 3-D reacting shock-bubble workload: a planar shock
   in N2 hitting a sphere of stoichiometric 2H2+O2 with a tanh interface and a
   seeded spherical-harmonic surface perturbation (l = 1..8, RMS amplitude 2 % of
@@ -43,6 +45,9 @@ MECH_JA919_AR = os.path.join(DATA, "H2_JA919_Ar.txt")
 THERMO_AR = os.path.join(DATA, "thermo_Ar.dat")
 INPUT_ZND = os.path.join(DATA, "input-1dZND.txt")
 INPUT_ODW = os.path.join(DATA, "input-ODW.txt")
+# the oblique-detonation configuration of the benchmark: Mach 7, 300 K,
+# 101.325 kPa stoichiometric H2-air, the wedge tip 5 mm from the inflow face
+INPUT_ODW_M7 = os.path.join(DATA, "input-ODW-M7.txt")
 GRID_3DODW = os.path.join(DATA, "grid-3dODW.txt")
 
 # species slots of H2_JA919 (H O H2O OH O2 H2 H2O2 HO2 N2)
@@ -353,6 +358,16 @@ def odw_phi(z, seed=4, modes=4, amplitude=0.1, bc=2):
     s = sum(a[m] * np.sin(2 * math.pi * (m + 1) * (zi - zi[0]) / L + th[m]) for m in range(modes))
     peak = np.abs(s).max()
     return 1.0 + (amplitude * s / peak if peak > 0 else 0 * s)
+
+
+def odw_wall_node(x, input_path=INPUT_ODW, bc=2):
+    """First x node of the wedge surface: the input file's wedge_x (distance
+    from the inflow face along the wedge, 0 when absent) on the haloed
+    coordinates x."""
+    import eu3d
+    wx = eu3d.read_value(input_path, "wedge_x", 0.0)
+    xi = np.asarray(x)[bc:-bc]
+    return int(np.searchsorted(xi, xi[0] + wx - 1e-12))
 
 
 def odw(x, y, z, mech, input_path=INPUT_ODW, phi=None, bc=2):

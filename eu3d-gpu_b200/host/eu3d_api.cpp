@@ -13,6 +13,7 @@
 #include <new>
 #include <tuple>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -67,6 +68,18 @@ struct eu_handle {
     unsigned graph_gen = 0; // captures so far (batches rebuild when it changes)
     // launch shapes picked by eu_autotune (0: defaults)
     int flux_ci = 0, recover_block = 0, recover_minb = 0;
+    // advection time scheme (eu_set_time_scheme) and the RK start-of-step state
+    int time_scheme = EU_TIME_EE;
+    double *d_cs0 = nullptr;
+    // asynchronous output (eu_output_async): device snapshot of the fields a
+    // file needs, its pinned host copy, the copy stream and the writer thread
+    double *d_snap = nullptr, *h_snap = nullptr;
+    size_t snap_bytes = 0;
+    cudaStream_t out_stream = nullptr;
+    cudaEvent_t ev_snap = nullptr, ev_host = nullptr;
+    std::thread out_thread;
+    eu_status out_status = EU_OK;
+    std::string out_err;
     std::string err;
 };
 
@@ -504,10 +517,17 @@ eu_status eu_destroy(eu_handle *h)
     if (!h)
         return EU_ERR_INVALID_ARGUMENT;
     cudaSetDevice(h->cfg.device);
+    if (h->out_thread.joinable())
+        h->out_thread.join();
     if (h->stream)
         cudaStreamSynchronize(h->stream);
     drop_graph(h);
     free_all(h);
+    if (h->d_snap) cudaFree(h->d_snap);
+    if (h->h_snap) cudaFreeHost(h->h_snap);
+    if (h->ev_snap) cudaEventDestroy(h->ev_snap);
+    if (h->ev_host) cudaEventDestroy(h->ev_host);
+    if (h->out_stream) cudaStreamDestroy(h->out_stream);
     if (h->h_counts)
         cudaFreeHost(h->h_counts);
     for (auto &e : h->pev)
@@ -673,6 +693,45 @@ eu_status eu_set_inflow(eu_handle *h, const double *P, const double *T, const do
     return EU_OK;
 }
 
+eu_status eu_set_time_scheme(eu_handle *h, int scheme)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (scheme != EU_TIME_EE && scheme != EU_TIME_RK3)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "unknown time scheme %d", scheme);
+    if (!h->has_mech)
+        return fail(h, EU_ERR_NOT_READY, "load a mechanism first");
+    if (scheme == EU_TIME_RK3 && !h->d_cs0) {
+        cudaSetDevice(h->cfg.device);
+        eu_status st = dalloc(h, &h->d_cs0, size_t(h->n3) * (h->mech.ns + 4));
+        if (st != EU_OK)
+            return st;
+    }
+    h->time_scheme = scheme;
+    h->graph_dirty = true;
+    return EU_OK;
+}
+
+eu_status eu_set_odw_wall(eu_handle *h, int first_wall_node)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (h->cfg.boundary != EU_BC_ODW)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "the wall start applies to EU_BC_ODW handles");
+    if (first_wall_node < 0 || first_wall_node > h->cfg.total_ni)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "first wall node %d outside 0 .. %d", first_wall_node,
+                    h->cfg.total_ni);
+    // this block's local index of that global node (x blocks share one node)
+    const int first = (h->cfg.blocks_x > 1 ? h->cfg.block_x : 0) * (h->ni - 1);
+    int local = first_wall_node - first;
+    local = local < 0 ? 0 : (local > h->ni ? h->ni : local);
+    if (local > 0 && !h->st.inflow)
+        return fail(h, EU_ERR_NOT_READY, "set the freestream tables (eu_set_inflow) first");
+    h->g.wall_i0 = local;
+    h->graph_dirty = true;
+    return EU_OK;
+}
+
 namespace {
 
 // Atoms of each element in a species name such as "H2O2" or "AR".
@@ -825,11 +884,38 @@ eu_status step_launches(eu_handle *h, const LaunchArgs &a, const Launchers &L, b
     }
     CK(h, cudaMemsetAsync(h->st.counters, 0, kCntPerStep * sizeof(unsigned long long), h->stream));
     if (prof) CK(h, cudaEventRecord(h->pev[0], h->stream));
-    CK(h, L.boundary(a));
-    if (prof) CK(h, cudaEventRecord(h->pev[1], h->stream));
-    CK(h, L.flux_update(a));
-    if (prof) CK(h, cudaEventRecord(h->pev[2], h->stream));
-    *launches += 2;
+    if (h->time_scheme == EU_TIME_RK3) {
+        // three-stage TVD Runge-Kutta advection (Shu-Osher): each stage its ghost
+        // fill, flux divergence (CS += dt L), combination with the start-of-step
+        // state and recovery; the chemistry phase below recovers the last stage.
+        // Profile phases: ghost fill = the first stage's, flux = the rest of
+        // the advection.
+        const size_t cs_bytes = size_t(h->n3) * (h->mech.ns + 4) * sizeof(double);
+        CK(h, cudaMemcpyAsync(h->d_cs0, h->st.cs, cs_bytes, cudaMemcpyDeviceToDevice, h->stream));
+        static const double ca[3] = {0.0, 0.75, 1.0 / 3.0}, cb[3] = {1.0, 0.25, 2.0 / 3.0};
+        for (int q = 0; q < 3; ++q) {
+            CK(h, L.boundary(a));
+            if (prof && q == 0) CK(h, cudaEventRecord(h->pev[1], h->stream));
+            CK(h, L.flux_update(a));
+            *launches += 2;
+            if (q > 0) {
+                // explicitly rounded products and sum: the same in every flavour
+                CK(h, strict::launch_rk_combine(a, h->d_cs0, ca[q], cb[q]));
+                ++*launches;
+            }
+            if (q < 2) {
+                CK(h, L.recover_react(a, false));
+                ++*launches;
+            }
+        }
+        if (prof) CK(h, cudaEventRecord(h->pev[2], h->stream));
+    } else {
+        CK(h, L.boundary(a));
+        if (prof) CK(h, cudaEventRecord(h->pev[1], h->stream));
+        CK(h, L.flux_update(a));
+        if (prof) CK(h, cudaEventRecord(h->pev[2], h->stream));
+        *launches += 2;
+    }
     const bool heavy = h->st.heavy && (learned || react);
     if (heavy)
         CK(h, cudaMemsetAsync(h->st.heavy, 0, 2 * sizeof(int), h->stream));
@@ -1403,6 +1489,250 @@ eu_status eu_read_state(eu_handle *h, const char *path, int *iteration, int *num
     if (final_time) *final_time = t;
     if (dt) *dt = d;
     return EU_OK;
+}
+
+// ------------------------------------------------------ asynchronous output
+// A snapshot of the fields an output file needs is copied, in stream order,
+// into a device buffer of the handle (so the timestep may go on at once), then
+// to pinned host memory on a second stream, and a host thread formats and
+// writes the file once that copy has landed.
+
+namespace {
+// Tecplot output of Euler::Output (src/Euler.cpp:1600-1790): block data over
+// every haloed node, i fastest, these variables after X, Y, Z
+const char *kTecplotFields[6] = {"T", "D", "P", "U", "V", "Ma"};
+constexpr int kTecplotSpecies = 7;
+// EU3D_STATE_V1_LE dump: the 14 one-plane fields after X, Y, Z, in column order
+const char *kDumpPlanes[14] = {"D", "T", "U", "V", "W", "E", "Wav", "Rgas", "Cp", "P", "H", "Gamma", "C", "Ma"};
+
+// Snapshot layout: double planes of n3 values; for the state dump 14 planes,
+// Di (ns), Yi (ns), CS (ns + 4), CMS (ns), then Nchem as n3 ints.
+size_t snap_planes(int kind, int ns)
+{
+    return kind == EU_OUTPUT_TECPLOT ? 6 + kTecplotSpecies : 14 + 4 * size_t(ns) + 4;
+}
+
+// One plane of field `name` into dst on the handle's stream (device to device).
+eu_status snap_plane(eu_handle *h, const std::string &n, double *dst)
+{
+    const long long n3 = h->n3;
+    const size_t b = size_t(n3) * sizeof(double);
+    const char *prim_names[7] = {"P", "D", "U", "V", "W", "H", "Gamma"};
+    for (int f = 0; f < 7; ++f)
+        if (n == prim_names[f]) {
+            CK(h, cudaMemcpyAsync(dst, h->st.prim + f * n3, b, cudaMemcpyDeviceToDevice, h->stream));
+            return EU_OK;
+        }
+    if (n == "T" || n == "E") {
+        CK(h, cudaMemcpyAsync(dst, n == "T" ? h->st.T : h->st.E, b, cudaMemcpyDeviceToDevice, h->stream));
+        return EU_OK;
+    }
+    const char *derived[5] = {"Wav", "Rgas", "Cp", "C", "Ma"};
+    for (int w = 0; w < 5; ++w)
+        if (n == derived[w]) {
+            const LaunchArgs a = launch_args(h);
+            CK(h, flavour(h).derived(a, w, dst));
+            return EU_OK;
+        }
+    return fail(h, EU_ERR_INVALID_ARGUMENT, "unknown field %s", n.c_str());
+}
+
+// The reference writes each value with an ostream's default format: six
+// significant digits, %g style.
+void put_g(std::string &out, double v)
+{
+    char buf[40];
+    const int n = std::snprintf(buf, sizeof buf, "%g\n", v);
+    out.append(buf, size_t(n));
+}
+
+eu_status write_tecplot_file(const char *path, const eu_handle *h, const double *snap, std::string &err)
+{
+    std::FILE *f = std::fopen(path, "wb");
+    if (!f) {
+        err = std::string("cannot open ") + path + " for writing";
+        return EU_ERR_IO;
+    }
+    const long long n3 = h->n3;
+    std::string out = "Variables = X,Y,Z,T,D,P,U,V,Ma,Y1,Y2,Y3,Y4,Y5,Y6,Y7\n";
+    out += "ZONE I=" + std::to_string(h->nx) + "\tJ=" + std::to_string(h->ny) + "\tK=" + std::to_string(h->nz) +
+           "\ndatapacking=block\n";
+    bool ok = true;
+    auto flush = [&]() {
+        ok = ok && std::fwrite(out.data(), 1, out.size(), f) == out.size();
+        out.clear();
+    };
+    // node (i, j, k) in the reference's loop order: k outermost, i fastest
+    for (int v = 0; v < 3 + 6 + kTecplotSpecies && ok; ++v) {
+        for (int k = 0; k < h->nz; ++k) {
+            for (int j = 0; j < h->ny; ++j)
+                for (int i = 0; i < h->nx; ++i) {
+                    const long long c = (static_cast<long long>(i) * h->ny + j) * h->nz + k;
+                    put_g(out, v == 0 ? h->x[i] : v == 1 ? h->y[j] : v == 2 ? h->z[k] : snap[(v - 3) * n3 + c]);
+                }
+            if (out.size() > (size_t(1) << 22))
+                flush();
+        }
+    }
+    flush();
+    if (std::fclose(f) != 0 || !ok) {
+        err = std::string("writing ") + path + " failed";
+        return EU_ERR_IO;
+    }
+    return EU_OK;
+}
+
+eu_status write_dump_file(const char *path, const eu_handle *h, const double *snap, int iteration, int num,
+                          double final_time, double dt, std::string &err)
+{
+    std::FILE *f = std::fopen(path, "wb");
+    if (!f) {
+        err = std::string("cannot open ") + path + " for writing";
+        return EU_ERR_IO;
+    }
+    const int ns = h->mech.ns;
+    const long long n3 = h->n3;
+    const double *di = snap + 14 * n3, *yi = di + ns * n3, *cs = yi + ns * n3, *cms = cs + (ns + 4) * n3;
+    const int *nchem = reinterpret_cast<const int *>(cms + ns * n3);
+    const int blocks_x = h->cfg.blocks_x > 1 ? h->cfg.blocks_x : 1;
+    std::fprintf(f, "%s\n%d %d %d %d %d %d %d %d 0 0 %d 1 1 %d %d %d %d %.17g %.17g\n%s\n", kDumpMagic, ns,
+                 h->cfg.total_ni, h->nj, h->nk, h->ni, h->nj, h->nk, h->cfg.block_x, blocks_x, h->cfg.block_x, blocks_x,
+                 iteration, num, final_time, dt, dump_columns(ns).c_str());
+    const int ncols = 22 + 5 * ns;
+    std::vector<double> row(ncols);
+    bool ok = true;
+    for (int i = h->bc; i < h->bc + h->ni && ok; ++i)
+        for (int j = h->bc; j < h->bc + h->nj && ok; ++j)
+            for (int k = h->bc; k < h->bc + h->nk; ++k) {
+                const long long c = (static_cast<long long>(i) * h->ny + j) * h->nz + k;
+                row[0] = h->x[i];
+                row[1] = h->y[j];
+                row[2] = h->z[k];
+                for (int q = 0; q < 14; ++q) row[3 + q] = snap[q * n3 + c];
+                int o = 17;
+                for (int q = 0; q < ns; ++q) row[o++] = di[q * n3 + c];
+                for (int q = 0; q < ns; ++q) row[o++] = yi[q * n3 + c];
+                // Update_after_CS: Mc = Di / Mw * 1000 (src/Flowfield.cpp:1589)
+                for (int q = 0; q < ns; ++q) row[o++] = di[q * n3 + c] / h->mech.mw[q] * 1000;
+                for (int q = 0; q < ns + 4; ++q) row[o++] = cs[q * n3 + c];
+                for (int q = 0; q < ns; ++q) row[o++] = cms[q * n3 + c];
+                row[o] = nchem[c];
+                if (std::fwrite(row.data(), sizeof(double), ncols, f) != size_t(ncols)) {
+                    ok = false;
+                    break;
+                }
+            }
+    if (std::fclose(f) != 0 || !ok) {
+        err = std::string("writing ") + path + " failed";
+        return EU_ERR_IO;
+    }
+    return EU_OK;
+}
+} // namespace
+
+eu_status eu_output_wait(eu_handle *h)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (h->out_thread.joinable())
+        h->out_thread.join();
+    const eu_status s = h->out_status;
+    h->out_status = EU_OK;
+    if (s != EU_OK)
+        return fail(h, s, "%s", h->out_err.c_str());
+    return EU_OK;
+}
+
+eu_status eu_output_async(eu_handle *h, int kind, const char *path, int iteration, int num, double final_time,
+                          double dt)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!path || (kind != EU_OUTPUT_STATE && kind != EU_OUTPUT_TECPLOT))
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "null path or unknown output kind %d", kind);
+    if (!h->has_mech || !h->has_state)
+        return fail(h, EU_ERR_NOT_READY, "no state");
+    if (kind == EU_OUTPUT_TECPLOT && h->mech.ns < kTecplotSpecies)
+        return fail(h, EU_ERR_UNSUPPORTED, "the Tecplot output writes 7 species; the mechanism has %d", h->mech.ns);
+    // one output in flight per handle: the previous writer finishes first
+    eu_status prev = eu_output_wait(h);
+    if (prev != EU_OK)
+        return prev;
+    cudaSetDevice(h->cfg.device);
+    const int ns = h->mech.ns;
+    const long long n3 = h->n3;
+    const size_t bytes = snap_planes(kind, ns) * size_t(n3) * sizeof(double);
+    if (bytes > h->snap_bytes) {
+        if (h->d_snap) cudaFree(h->d_snap);
+        if (h->h_snap) cudaFreeHost(h->h_snap);
+        h->d_snap = h->h_snap = nullptr;
+        h->snap_bytes = 0;
+        CK(h, cudaMalloc(&h->d_snap, bytes));
+        CK(h, cudaMallocHost(&h->h_snap, bytes));
+        h->snap_bytes = bytes;
+    }
+    if (!h->out_stream) {
+        CK(h, cudaStreamCreateWithFlags(&h->out_stream, cudaStreamNonBlocking));
+        CK(h, cudaEventCreateWithFlags(&h->ev_snap, cudaEventDisableTiming));
+        CK(h, cudaEventCreateWithFlags(&h->ev_host, cudaEventDisableTiming));
+    }
+    if (h->prim_stale) {
+        const LaunchArgs a = launch_args(h);
+        CK(h, flavour(h).materialize(a));
+        h->prim_stale = false;
+    }
+    const size_t b = size_t(n3) * sizeof(double);
+    double *d = h->d_snap;
+    eu_status st = EU_OK;
+    if (kind == EU_OUTPUT_TECPLOT) {
+        for (int q = 0; q < 6 && st == EU_OK; ++q) st = snap_plane(h, kTecplotFields[q], d + q * n3);
+        if (st == EU_OK)
+            CK(h, cudaMemcpyAsync(d + 6 * n3, h->st.prim + 7 * n3, kTecplotSpecies * b, cudaMemcpyDeviceToDevice,
+                                  h->stream));
+    } else {
+        for (int q = 0; q < 14 && st == EU_OK; ++q) st = snap_plane(h, kDumpPlanes[q], d + q * n3);
+        if (st == EU_OK) {
+            double *di = d + 14 * n3, *yi = di + ns * n3, *cs = yi + ns * n3, *cms = cs + (ns + 4) * n3;
+            CK(h, cudaMemcpyAsync(di, h->st.cs, ns * b, cudaMemcpyDeviceToDevice, h->stream));
+            CK(h, cudaMemcpyAsync(yi, h->st.prim + 7 * n3, ns * b, cudaMemcpyDeviceToDevice, h->stream));
+            CK(h, cudaMemcpyAsync(cs, h->st.cs, (ns + 4) * b, cudaMemcpyDeviceToDevice, h->stream));
+            // no recorded sources: the reference's CMS array holds zeros until written
+            if (h->st.cms)
+                CK(h, cudaMemcpyAsync(cms, h->st.cms, ns * b, cudaMemcpyDeviceToDevice, h->stream));
+            else
+                CK(h, cudaMemsetAsync(cms, 0, ns * b, h->stream));
+            CK(h, cudaMemcpyAsync(cms + ns * n3, h->st.nchem, size_t(n3) * sizeof(int), cudaMemcpyDeviceToDevice,
+                                  h->stream));
+        }
+    }
+    if (st != EU_OK)
+        return st;
+    CK(h, cudaEventRecord(h->ev_snap, h->stream));
+    CK(h, cudaStreamWaitEvent(h->out_stream, h->ev_snap, 0));
+    CK(h, cudaMemcpyAsync(h->h_snap, h->d_snap, bytes, cudaMemcpyDeviceToHost, h->out_stream));
+    CK(h, cudaEventRecord(h->ev_host, h->out_stream));
+    const std::string file(path);
+    h->out_thread = std::thread([h, kind, file, iteration, num, final_time, dt]() {
+        cudaSetDevice(h->cfg.device);
+        const cudaError_t e = cudaEventSynchronize(h->ev_host);
+        if (e != cudaSuccess) {
+            h->out_status = EU_ERR_CUDA;
+            h->out_err = std::string("output copy: ") + cudaGetErrorString(e);
+            return;
+        }
+        h->out_status = kind == EU_OUTPUT_TECPLOT
+                            ? write_tecplot_file(file.c_str(), h, h->h_snap, h->out_err)
+                            : write_dump_file(file.c_str(), h, h->h_snap, iteration, num, final_time, dt, h->out_err);
+    });
+    return EU_OK;
+}
+
+eu_status eu_write_tecplot(eu_handle *h, const char *path)
+{
+    const eu_status s = eu_output_async(h, EU_OUTPUT_TECPLOT, path, 0, 0, 0.0, 0.0);
+    if (s != EU_OK)
+        return s;
+    return eu_output_wait(h);
 }
 
 eu_status eu_sync(eu_handle *h)

@@ -114,8 +114,10 @@ long long params_per_member(const eu_mlp *m)
     return n;
 }
 
-// forward of member e over n packed rows in m->X (on stream s; training keeps
-// the pre-activations)
+// forward of member e over n packed rows in m->X (on stream s). Training keeps
+// the pre-activations and uses the exact-form SiLU (epilogue mode 1);
+// inference uses the fused kernel's form (mode 4), so the layer-wise and fused
+// predictions agree bitwise.
 eu_status forward(eu_mlp *m, int e, int n, cudaStream_t s = nullptr, bool keep_pre = true)
 {
     if (!s)
@@ -125,8 +127,8 @@ eu_status forward(eu_mlp *m, int e, int n, cudaStream_t s = nullptr, bool keep_p
         const void *A = l == 0 ? m->X : m->H[l - 1];
         const int lda = l == 0 ? m->in_pad : m->width;
         const Layer &L = net[l];
-        MCK(m, eu3d::gemm_bf16(A, lda, L.Wb, L.in_pad, n, L.out_pad, L.in_pad, L.b, 1, nullptr, m->H[l],
-                               keep_pre ? m->Z[l] : nullptr, m->width, nullptr, 1, m->d_err, s));
+        MCK(m, eu3d::gemm_bf16(A, lda, L.Wb, L.in_pad, n, L.out_pad, L.in_pad, L.b, keep_pre ? 1 : 4, nullptr,
+                               m->H[l], keep_pre ? m->Z[l] : nullptr, m->width, nullptr, 1, m->d_err, s));
     }
     const Layer &L = net[m->hidden];
     MCK(m, eu3d::gemm_bf16(m->H[m->hidden - 1], m->width, L.Wb, L.in_pad, n, L.out_pad, L.in_pad, L.b, 0, m->Y, nullptr,
@@ -701,7 +703,7 @@ eu_status eu_mlp_predict(eu_mlp *m, const float *X, long long n, float *out)
         MCK(m, eu3d::pack_features(X + r0 * m->n_in, nb, m->n_in, nullptr, m->in_shift, m->in_scale, m->X, m->in_pad,
                                    m->stream));
         for (int e = 0; e < m->members; ++e) {
-            eu_status s = forward(m, e, nb);
+            eu_status s = forward(m, e, nb, nullptr, false);
             if (s != EU_OK)
                 return s;
             MCK(m, eu3d::unscale_outputs(m->Y, nb, m->out_pad, m->n_out, m->out_shift, m->out_scale,

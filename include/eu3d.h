@@ -216,6 +216,28 @@ eu_status eu_set_conserved(eu_handle *h, const double *cs, const double *T, cons
  * Flowfield::FieldInitial forms them (src/Flowfield.cpp:226-262). */
 eu_status eu_set_inflow(eu_handle *h, const double *P, const double *T, const double *U, const double *V,
                         const double *W, const double *Y);
+/* Time scheme of the advection part of eu_step. EU_TIME_EE (default): the
+ * reference's Euler-explicit stage (TimeAdv::EE, src/TimeAdv.cpp:42-56).
+ * EU_TIME_RK3: the three-stage TVD Runge-Kutta of Shu and Osher, U1 = U0 +
+ * dt L(U0), U2 = 3/4 U0 + 1/4 (U1 + dt L(U1)), U3 = 1/3 U0 + 2/3 (U2 + dt
+ * L(U2)), each stage with its own ghost fill and state recovery, then the
+ * chemistry once on U3 (the reference declares TimeAdv::TVD_RK3,
+ * src/TimeAdv.cpp:210-221, with an empty body). Each combination rounds its
+ * two products and their sum separately. The start-of-step copy of the
+ * conserved planes is allocated at the first switch to RK3. */
+#define EU_TIME_EE 0
+#define EU_TIME_RK3 1
+eu_status eu_set_time_scheme(eu_handle *h, int scheme);
+
+/* EU_BC_ODW: where the wall begins on the y-low face. The ghost nodes of the
+ * y-low face below global x node first_wall_node take the freestream (the
+ * first row of the eu_set_inflow tables, per k) instead of the reflecting
+ * wall, so the wedge surface starts at that node with free flow ahead of it
+ * (a wedge tip inside the domain). 0, the default, is the reference's fill
+ * (FieldBoundary_3dODW, src/Flowfield.cpp:464-493: symmetry along the whole
+ * face). Needs the inflow tables when the freestream part is not empty. No
+ * counterpart in the reference. */
+eu_status eu_set_odw_wall(eu_handle *h, int first_wall_node);
 
 /* Advance nsteps timesteps of fixed dt. Asynchronous on the handle's stream
  * unless stats is non-NULL (then it synchronises and fills stats). */
@@ -246,6 +268,33 @@ eu_status eu_write_state(eu_handle *h, const char *path, int iteration, int num,
  * eu_set_state; the header's iteration, output number, time and dt are returned
  * (NULL to skip). */
 eu_status eu_read_state(eu_handle *h, const char *path, int *iteration, int *num, double *final_time, double *dt);
+
+/* Output without stalling the time loop (the reference's Euler::Output,
+ * src/Euler.cpp:1540-1790, writes synchronously from host arrays). The fields
+ * the file needs are copied, in the handle's stream order, into a device
+ * snapshot buffer of the handle, so eu_step may be called again at once; a
+ * second stream moves the snapshot to pinned host memory and a host thread
+ * writes the file. kind:
+ *   EU_OUTPUT_STATE    the EU3D_STATE_V1_LE dump of eu_write_state (same bytes;
+ *                      iteration, num, final_time and dt go to its header);
+ *   EU_OUTPUT_TECPLOT  the reference's Tecplot file (Euler::Output,
+ *                      src/Euler.cpp:1600-1790): "Variables = X,Y,Z,T,D,P,U,V,
+ *                      Ma,Y1,...,Y7", one zone over every haloed node, block
+ *                      packing with i fastest and k slowest, each value as a
+ *                      C++ stream writes it by default (six significant digits);
+ *                      the caller names the file (the reference's is
+ *                      output_<ranks>/results/Series<name><num>_<rank>.dat).
+ * One output is in flight per handle: a call waits for the previous one.
+ * eu_output_wait waits for the file and returns the writer's status. The
+ * snapshot buffers (device and pinned host, the size of the fields written)
+ * are allocated at the first call and kept by the handle. */
+#define EU_OUTPUT_STATE 0
+#define EU_OUTPUT_TECPLOT 1
+eu_status eu_output_async(eu_handle *h, int kind, const char *path, int iteration, int num, double final_time,
+                          double dt);
+eu_status eu_output_wait(eu_handle *h);
+/* The Tecplot file of EU_OUTPUT_TECPLOT, written before the call returns. */
+eu_status eu_write_tecplot(eu_handle *h, const char *path);
 
 /* Wait for all work queued on the handle. */
 eu_status eu_sync(eu_handle *h);

@@ -43,8 +43,12 @@ struct eo_state {
     int bad_nchem;
     int bc_kind; /* 0: RSBI ghost fill, 1: ZND */
     int exch_lo, exch_hi; /* x faces filled by the halo exchange, not the ghost fill */
+    int wall_i0;    /* ODW: first local x node of the y-low wall (0: the whole face) */
     double *inflow; /* ODW: x-low ghost values per interior (j, k), 9 + ns planes
                        (P D T U V W H Gamma E Y...), or NULL */
+    int scheme;     /* 0: Euler explicit (TimeAdv::EE), 1: three-stage TVD Runge-Kutta */
+    double *cs0;    /* RK: the conserved state at the start of the step */
+    double rk_a, rk_b; /* RK stage combination CS = a CS0 + b CS (phase 4) */
 };
 
 #define IDX(st, i, j, k) (((long)(i) * (st)->ny + (j)) * (st)->nz + (k))
@@ -469,10 +473,30 @@ static void boundary_fill(eo_state *st)
                         copy_cell(st, hi, shi, 1, 1, 1);
                 }
             }
-    /* y front: symmetry with thermo recomputed from mirrored T, p, Y (:647-679) */
+    /* y front: symmetry with thermo recomputed from mirrored T, p, Y (:647-679);
+     * ODW with a wall start (this build's addition): ahead of it the ghosts
+     * take the freestream, the first row of the inflow tables */
     for (int i = bc; i < ni + bc; i++)
         for (int j = 0; j < bc; j++)
-            for (int k = bc; k < nk + bc; k++) rebuild_cell(st, IDX(st, i, j, k), IDX(st, i, 2 * bc - 1 - j, k), -1);
+            for (int k = bc; k < nk + bc; k++) {
+                const long d = IDX(st, i, j, k);
+                if (st->bc_kind == 2 && i - bc < st->wall_i0 && st->inflow) {
+                    const long nt = (long)nj * nk, t = (long)(k - bc);
+                    const double *f = st->inflow;
+                    st->P[d] = f[0 * nt + t];
+                    st->D[d] = f[1 * nt + t];
+                    st->T[d] = f[2 * nt + t];
+                    st->U[d] = f[3 * nt + t];
+                    st->V[d] = f[4 * nt + t];
+                    st->W[d] = f[5 * nt + t];
+                    st->H[d] = f[6 * nt + t];
+                    st->G[d] = f[7 * nt + t];
+                    st->E[d] = f[8 * nt + t];
+                    for (int s = 0; s < st->ns; s++) st->Y[s * st->n3 + d] = f[(9 + s) * nt + t];
+                } else {
+                    rebuild_cell(st, d, IDX(st, i, 2 * bc - 1 - j, k), -1);
+                }
+            }
     /* y back: zero-gradient mirror copy (:684-705) */
     for (int i = bc; i < ni + bc; i++)
         for (int j = nj + bc; j < nj + 2 * bc; j++)
@@ -539,6 +563,32 @@ static void *run_job(void *arg)
                                            dt / (st->z[k] - st->z[k - 1]) * (Q[c] - Q[c - 1]);
                         st->CS[s * n3 + c] = st->CS[s * n3 + c] + rhs;
                     }
+                    update_after_cs(st, c);
+                }
+        } else if (jb->phase == 3) {
+            /* RK stage: CS += RHS alone (the recovery follows the combination) */
+            const double dt = st->dt;
+            for (int j = bc; j < nj + bc; j++)
+                for (int k = bc; k < nk + bc; k++) {
+                    const long c = IDX(st, i, j, k);
+                    const long cx = (long)st->ny * st->nz, cy = st->nz;
+                    for (int s = 0; s < ns + 4; s++) {
+                        const double *F = st->flux[0] + s * n3, *G = st->flux[1] + s * n3, *Q = st->flux[2] + s * n3;
+                        const double rhs = -dt / (st->x[i] - st->x[i - 1]) * (F[c] - F[c - cx]) -
+                                           dt / (st->y[j] - st->y[j - 1]) * (G[c] - G[c - cy]) -
+                                           dt / (st->z[k] - st->z[k - 1]) * (Q[c] - Q[c - 1]);
+                        st->CS[s * n3 + c] = st->CS[s * n3 + c] + rhs;
+                    }
+                }
+        } else if (jb->phase == 4) {
+            /* RK stage combination CS = a CS0 + b CS (Shu-Osher form), then
+             * Update_after_CS */
+            for (int j = bc; j < nj + bc; j++)
+                for (int k = bc; k < nk + bc; k++) {
+                    const long c = IDX(st, i, j, k);
+                    if (st->rk_a != 0)
+                        for (int s = 0; s < ns + 4; s++)
+                            st->CS[s * n3 + c] = st->rk_a * st->cs0[s * n3 + c] + st->rk_b * st->CS[s * n3 + c];
                     update_after_cs(st, c);
                 }
         } else {
@@ -630,6 +680,7 @@ void eo_destroy(eo_state *st)
     for (unsigned q = 0; q < sizeof(bufs) / sizeof(bufs[0]); q++) free(bufs[q]);
     free(st->nchem);
     free(st->inflow);
+    free(st->cs0);
     free(st);
 }
 
@@ -695,6 +746,8 @@ void eo_set_state(eo_state *st, const double *cs, const double *T, const double 
 void eo_boundary(eo_state *st) { boundary_fill(st); }
 
 void eo_set_boundary(eo_state *st, int kind) { st->bc_kind = kind; }
+
+void eo_set_wall(eo_state *st, int first_wall_node) { st->wall_i0 = first_wall_node; }
 
 void eo_set_inflow(eo_state *st, const double *P, const double *T, const double *U, const double *V,
                    const double *W, const double *Y)
@@ -772,14 +825,46 @@ long eo_halo_count(const eo_state *st) { return (long)(7 + st->ns) * st->bc * st
 void eo_halo_pack(eo_state *st, int face, double *msg) { halo_copy(st, face, 1, msg); }
 void eo_halo_unpack(eo_state *st, int face, const double *msg) { halo_copy(st, face, 0, (double *)msg); }
 
+/* The three-stage TVD Runge-Kutta advection of the timestep (Shu and Osher's
+ * SSP-RK3; the reference's TimeAdv::TVD_RK3, src/TimeAdv.cpp:210-221, is an
+ * empty stub): U1 = U0 + dt L(U0), U2 = 3/4 U0 + 1/4 (U1 + dt L(U1)),
+ * U3 = 1/3 U0 + 2/3 (U2 + dt L(U2)), each stage with its own ghost fill and
+ * state recovery; the chemistry then runs once on U3, as after the Euler
+ * stage. */
+static void rk3_advection(eo_state *st)
+{
+    const int bc = st->bc, ni = st->ni;
+    memcpy(st->cs0, st->CS, (size_t)st->n3 * (st->ns + 4) * sizeof(double));
+    static const double a[3] = {0.0, 0.75, 1.0 / 3.0}, b[3] = {1.0, 0.25, 2.0 / 3.0};
+    for (int q = 0; q < 3; q++) {
+        boundary_fill(st);
+        run_phase(st, 0, bc - 1, ni + bc); /* faces */
+        run_phase(st, 3, bc, ni + bc);     /* CS += RHS */
+        st->rk_a = a[q];
+        st->rk_b = b[q];
+        run_phase(st, 4, bc, ni + bc);     /* combination + state recovery */
+    }
+}
+
+void eo_set_scheme(eo_state *st, int scheme)
+{
+    st->scheme = scheme;
+    if (scheme == 1 && !st->cs0)
+        st->cs0 = (double *)calloc((size_t)st->n3 * (st->ns + 4), sizeof(double));
+}
+
 int eo_step(eo_state *st, int nsteps, double dt)
 {
     const int bc = st->bc, ni = st->ni;
     for (int n = 0; n < nsteps; n++) {
         st->dt = dt;
-        boundary_fill(st);
-        run_phase(st, 0, bc - 1, ni + bc); /* faces */
-        run_phase(st, 1, bc, ni + bc);     /* EE update + state recovery */
+        if (st->scheme == 1) {
+            rk3_advection(st);
+        } else {
+            boundary_fill(st);
+            run_phase(st, 0, bc - 1, ni + bc); /* faces */
+            run_phase(st, 1, bc, ni + bc);     /* EE update + state recovery */
+        }
         run_phase(st, 2, bc, ni + bc);     /* chemistry */
         if (st->bad_nchem)
             return -1;

@@ -55,6 +55,10 @@ void eo_set_state(eo_state *st, const double *cs, const double *T, const double 
 /* nsteps reference timesteps at fixed dt. Returns 0, or -1 if a prediction gave
  * Nchem <= 0 (the reference aborts there, src/Reaction.cpp:936-940). */
 int eo_step(eo_state *st, int nsteps, double dt);
+/* Time scheme of eo_step's advection: 0 Euler explicit (the reference's
+ * TimeAdv::EE), 1 the three-stage TVD Runge-Kutta (Shu-Osher SSP-RK3, this
+ * build's; the reference's TimeAdv::TVD_RK3 is an empty stub). */
+void eo_set_scheme(eo_state *st, int scheme);
 
 /* The RSBI ghost fill alone (src/Flowfield.cpp:593-807, face layers). */
 void eo_boundary(eo_state *st);
@@ -75,6 +79,10 @@ void eo_set_exchange(eo_state *st, int x_low, int x_high);
  * the x-low ghosts take these inflow tables (planes of nj * nk interior (j, k)
  * nodes, k fastest; Y: ns planes), with D, H, Gamma, E formed as FieldInitial
  * forms them (src/Flowfield.cpp:226-262). */
+/* ODW: the y-low ghosts of local x nodes below first_wall_node take the
+ * freestream (the first row of the inflow tables) instead of the symmetry
+ * fill; 0 (the default) is the reference's fill. */
+void eo_set_wall(eo_state *st, int first_wall_node);
 void eo_set_inflow(eo_state *st, const double *P, const double *T, const double *U, const double *V,
                    const double *W, const double *Y);
 long eo_halo_count(const eo_state *st);

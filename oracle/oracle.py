@@ -260,6 +260,8 @@ class PortOracle:
             lib.eo_set_boundary.argtypes = [_P, _I]
             lib.eo_set_exchange.argtypes = [_P, _I, _I]
             lib.eo_set_inflow.argtypes = [_P] * 7
+            lib.eo_set_wall.argtypes = [_P, _I]
+            lib.eo_set_scheme.argtypes = [_P, _I]
             lib.eo_halo_count.restype = ctypes.c_long
             lib.eo_halo_count.argtypes = [_P]
             lib.eo_halo_pack.argtypes = [_P, _I, _P]
@@ -327,6 +329,14 @@ class PortOracle:
         """ODW x-low inflow tables over the interior (j, k) nodes: planes (nj, nk), Y (ns, nj, nk)."""
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (P, T, U, V, W, Y)]
         self.lib().eo_set_inflow(self.h, *[a.ctypes.data for a in arrs])
+
+    def set_scheme(self, scheme):
+        """Advection time scheme: "ee" (the reference's) or "rk3" (eo_set_scheme)."""
+        self.lib().eo_set_scheme(self.h, {"ee": 0, "rk3": 1}[scheme])
+
+    def set_wall(self, first_wall_node):
+        """ODW: the y-low wall starts at this local x node (eo_set_wall)."""
+        self.lib().eo_set_wall(self.h, int(first_wall_node))
 
     def set_exchange(self, x_low, x_high):
         """x faces whose ghost nodes come from a neighbouring block (eo_halo_unpack)."""

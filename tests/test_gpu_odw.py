@@ -110,3 +110,49 @@ def test_odw_learned_mixed_runs(gpu):
         s.close()
     l1 = np.abs(out[True] - out[False]).sum(axis=0).mean()
     assert l1 <= 1e-3, l1
+
+
+def test_odw_wedge_tip_inside_the_domain(gpu, port_lib):
+    """The wedge surface starting at an interior x node (eu_set_odw_wall): the
+    y-low ghosts ahead of it take the freestream, behind it the reference's
+    symmetry fill. FP64 strict stiff steps of the Mach 7 / 101.325 kPa / 300 K
+    configuration against the restatement with the same wall start: conserved
+    state within 1e-10, Nchem exact, every y-low ghost layer equal; the shock
+    starts at the tip (no pressure rise ahead of it)."""
+    mo, mech, (x, y, z), _, _ = _case()
+    prim, inflow = cases.odw(x, y, z, mech, input_path=cases.INPUT_ODW_M7)
+    wall = 12
+    port = port_lib(NI, NJ, NK, x, y, z, mo, boundary="odw")
+    port.set_primitive(*prim)
+    port.set_inflow(*inflow)
+    port.set_wall(wall)
+    s = gpu.Solver(NI, NJ, NK, EXT, boundary="odw")
+    s.set_mechanism(mech)
+    s.set_primitive(*prim)
+    s.set_inflow(*inflow)
+    s.set_odw_wall(wall)
+    port.step(25, 1e-8)
+    s.step(25, 1e-8)
+    assert rel_linf(interior(s.get("CS")), interior(port.get("CS"))).max() <= 1e-10
+    assert n_unequal(interior(s.get("Nchem")), interior(port.get("Nchem"))) == 0
+    port.boundary()
+    s.step(0, 1e-8)
+    for f in ["P", "U", "V", "T", "Yi"]:
+        g, r = s.get(f)[:, 2:-2, 0:2, 2:-2], port.get(f)[:, 2:-2, 0:2, 2:-2]
+        assert rel_linf(g, r).max() <= 1e-10, f
+    p = interior(s.get("P"))[0]
+    p0 = 101325.0
+    assert np.abs(p[: wall - 4, :3] / p0 - 1).max() < 1e-6  # the freestream ahead of the tip
+    assert p[wall + 4:, 0].max() > 3 * p0  # the wedge's shock behind it
+    s.close()
+
+
+def test_odw_wall_start_needs_the_inflow_tables(gpu):
+    mo, mech, _, prim, _ = _case()
+    s = gpu.Solver(NI, NJ, NK, EXT, boundary="odw")
+    s.set_mechanism(mech)
+    s.set_primitive(*prim)
+    with pytest.raises(gpu.EU3DError) as e:
+        s.set_odw_wall(5)
+    assert e.value.name == "EU_ERR_NOT_READY"
+    s.close()

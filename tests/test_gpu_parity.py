@@ -84,6 +84,21 @@ def test_shock_bubble_twenty_steps(gpu, arith):
     assert n_unequal(interior(s.get("Nchem")), z["out_Nchem"]) == 0
 
 
+@pytest.mark.parametrize("arith", ["strict", "fast"])
+def test_shock_bubble_hundred_steps(gpu, arith):
+    """The required bound on the 3-D case: 100 steps of the shock-bubble (the
+    shock runs through the whole perturbed sphere) against the reference's
+    own CPU run, relative L-inf <= 1e-9 per conserved variable, Nchem exact."""
+    z = golden("bubble_33x17x17_s100.npz")
+    s = solver_from_golden(gpu, z, arith=arith)
+    st = s.step(int(z["steps"]), float(z["dt"]))
+    assert st["nonfinite"] == 0
+    err = rel_linf(interior(s.get("CS")), z["out_CS"])
+    assert err.max() <= 1e-9, err
+    assert rel_linf(interior(s.get("T")), z["out_T"]).max() <= 1e-9
+    assert n_unequal(interior(s.get("Nchem")), z["out_Nchem"]) == 0
+
+
 def test_larger_grid_against_restatement(gpu, port_lib):
     """A grid the fixtures do not cover, against the pinned C restatement."""
     ni, nj, nk = 49, 25, 25

@@ -91,3 +91,75 @@ def test_dump_of_another_size_is_refused(gpu):
     with pytest.raises(gpu.EU3DError) as e:
         other.read_state(path)
     assert e.value.name == "EU_ERR_INVALID_ARGUMENT"
+
+
+def test_async_dump_is_the_state_at_the_call(gpu):
+    """eu_output_async: the dump holds the state at the call even when steps
+    run before the file is waited for, and its bytes are eu_write_state's."""
+    a, z = bubble(gpu)
+    b, _ = bubble(gpu)
+    dt = float(z["dt"])
+    for s in (a, b):
+        s.step(3, dt)
+    d = tempfile.mkdtemp()
+    a.output_async(os.path.join(d, "async.bin"), "state", iteration=3, num=2, final_time=3 * dt, dt=dt)
+    a.step(4, dt)  # the time loop goes on while the snapshot is written
+    a.output_wait()
+    b.write_state(os.path.join(d, "sync.bin"), iteration=3, num=2, final_time=3 * dt, dt=dt)
+    with open(os.path.join(d, "async.bin"), "rb") as f1, open(os.path.join(d, "sync.bin"), "rb") as f2:
+        assert f1.read() == f2.read()
+    # and the handle that went on stepping is where it should be
+    b.step(4, dt)
+    assert n_unequal(interior(a.get("CS")), interior(b.get("CS"))) == 0
+
+
+def reference_tecplot(x, y, z, fields):
+    """The reference's Tecplot writer (Euler::Output, src/Euler.cpp:1600-1790)
+    restated: header, zone line, then each variable over every haloed node
+    with k outermost and i fastest, one value per line as an ostream writes a
+    double by default (%g)."""
+    nx, ny, nz = len(x), len(y), len(z)
+    lines = ["Variables = X,Y,Z,T,D,P,U,V,Ma,Y1,Y2,Y3,Y4,Y5,Y6,Y7", f"ZONE I={nx}\tJ={ny}\tK={nz}",
+             "datapacking=block"]
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    for a in [X, Y, Z] + fields:
+        lines += ["%g" % v for v in np.transpose(a, (2, 1, 0)).ravel()]
+    return lines
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_tecplot_output_matches_the_reference_writer(gpu, port_lib, precision):
+    """The Tecplot file against the reference writer's format applied to the C
+    restatement's fields after the same steps: identical header and zone lines
+    and node order; values equal to the six significant digits written (FP64
+    strict), or within the mixed-precision bound (1e-4 relative to each
+    variable's largest magnitude)."""
+    import oracle
+    from helpers import golden_mechanism
+    z = golden("bubble_25x13x13_s20.npz")
+    dt = float(z["dt"])
+    s = gpu.Solver(int(z["ni"]), int(z["nj"]), int(z["nk"]), tuple(z["extent"]),
+                   arith="strict" if precision == "fp64" else "fast", precision=precision)
+    s.load_mechanism(cases.MECH_JA919, cases.THERMO)
+    s.set_primitive(*[z[f"prim_{k}"] for k in "PTUVWY"])
+    s.step(6, dt)
+    path = os.path.join(tempfile.mkdtemp(), "Series0_0.dat")
+    s.write_tecplot(path)
+    p = port_lib(int(z["ni"]), int(z["nj"]), int(z["nk"]), z["x"], z["y"], z["z"], golden_mechanism())
+    p.set_primitive(*[z[f"prim_{k}"] for k in "PTUVWY"])
+    p.step(6, dt)
+    fields = [p.get(n)[0] for n in ("T", "D", "P", "U", "V", "Ma")] + list(p.get("Yi")[:7])
+    want = reference_tecplot(z["x"], z["y"], z["z"], fields)
+    got = open(path).read().split("\n")
+    assert got[-1] == "" and len(got) - 1 == len(want)
+    assert got[:3] == want[:3]
+    g = np.array([float(v) for v in got[3:-1]]).reshape(16, -1)
+    w = np.array([float(v) for v in want[3:]]).reshape(16, -1)
+    assert np.array_equal(g[:3], w[:3])  # node coordinates
+    scale = np.abs(w).max(axis=1, keepdims=True)
+    # one unit in the sixth digit (a last-bit difference across a rounding
+    # boundary), or the mixed-precision bound
+    tol = 1.2e-5 if precision == "fp64" else 1e-4
+    assert (np.abs(g - w) <= tol * np.maximum(np.abs(w), 1e-300) + (tol if precision == "mixed" else 0) * scale).all()
+    if precision == "fp64":
+        assert (np.array(got[3:-1]) == np.array(want[3:])).mean() > 0.999  # the same text but for rounding ties

@@ -25,7 +25,8 @@ def port_from_golden(port_lib, z):
     return p
 
 
-@pytest.mark.parametrize("name", ["rsbi_17x13x4_s3.npz", "rsbi_36x18x3_s100.npz", "bubble_25x13x13_s20.npz"])
+@pytest.mark.parametrize("name", ["rsbi_17x13x4_s3.npz", "rsbi_36x18x3_s100.npz", "bubble_25x13x13_s20.npz",
+                                  "bubble_33x17x17_s100.npz"])
 def test_port_matches_golden(port_lib, name):
     z = golden(name)
     p = port_from_golden(port_lib, z)
@@ -183,3 +184,19 @@ def test_odw_ghost_fill_matches_reference(ref_lib, port_lib):
     port.step(3, 2e-8)
     for f in ["CS", "T", "Nchem"]:
         assert n_unequal(interior(port.get(f)), interior(ref.get(f))) == 0, f
+
+
+def test_ns11_mechanism_is_rejected_as_by_the_reference(ref_lib, eu3d_lib, capfd):
+    """H2_JA1119.txt (11 species with Ar and He, 5 third-body rows) is not a
+    file the reference can read: Reaction::ReactionRead splits each
+    stoichiometry row at tabs and calls stoi on every item
+    (src/Reaction.cpp:193-214), and several rows of this file end in a tab
+    followed by spaces and a carriage return, an item stoi rejects. The
+    library's parser rejects it too, with an error code instead of an
+    exception."""
+    with pytest.raises(RuntimeError):
+        ref_lib.from_grid(4, 4, 4, (0.0, 1e-3, 0.0, 1e-3, 0.0, 1e-3), cases.MECH_JA1119, cases.THERMO)
+    assert "stoi" in capfd.readouterr().err
+    with pytest.raises(eu3d_lib.EU3DError) as e:
+        eu3d_lib.parse_mechanism(cases.MECH_JA1119, cases.THERMO)
+    assert e.value.name == "EU_ERR_IO"
