@@ -819,8 +819,10 @@ __global__ void k_to_f32(const double *__restrict__ src, float *__restrict__ dst
 // Post-advection state recovery (Flowfield::Update_after_Adv ->
 // Update_after_CS, src/Flowfield.cpp:1579-1617) followed, in the stiff modes,
 // by the kinetics of react_cell. One thread per interior node.
-template <int NS, int NR, bool kReact, class Rt>
-__global__ void __launch_bounds__(128) k_recover_react(const __grid_constant__ DevMech m, const DevGrid g,
+// MINB: resident 128-thread blocks per SM the register allocation aims at
+// (2: no spills, 8 warps; 3 and 4 trade spills for warps; the autotuner picks).
+template <int NS, int NR, bool kReact, class Rt, int MINB = 2>
+__global__ void __launch_bounds__(128, MINB) k_recover_react(const __grid_constant__ DevMech m, const DevGrid g,
                                                        const DevState st, const double *__restrict__ dt_dev,
                                                        int max_substeps)
 {

@@ -102,10 +102,18 @@ cudaError_t react_t(const LaunchArgs &a, bool react)
     if (!react)
         k_recover_react<NS, NR, false, TableRates<NS, NR>><<<grid, threads, 0, a.stream>>>(*a.mech, g, a.st, a.dt_dev,
                                                                                            a.max_substeps);
-    else if (a.spec == 1 && NS == Mech_JA919::NS && NR == Mech_JA919::NR)
-        k_recover_react<NS, NR, true, Mech_JA919><<<grid, threads, 0, a.stream>>>(*a.mech, g, a.st, a.dt_dev,
-                                                                                a.max_substeps);
-    else
+    else if (a.spec == 1 && NS == Mech_JA919::NS && NR == Mech_JA919::NR) {
+        // register target (autotuned): 2, 3 or 4 resident blocks per SM
+        if (a.recover_minb == 4)
+            k_recover_react<NS, NR, true, Mech_JA919, 4><<<grid, threads, 0, a.stream>>>(*a.mech, g, a.st, a.dt_dev,
+                                                                                       a.max_substeps);
+        else if (a.recover_minb == 3)
+            k_recover_react<NS, NR, true, Mech_JA919, 3><<<grid, threads, 0, a.stream>>>(*a.mech, g, a.st, a.dt_dev,
+                                                                                       a.max_substeps);
+        else
+            k_recover_react<NS, NR, true, Mech_JA919, 2><<<grid, threads, 0, a.stream>>>(*a.mech, g, a.st, a.dt_dev,
+                                                                                       a.max_substeps);
+    } else
         k_recover_react<NS, NR, true, TableRates<NS, NR>><<<grid, threads, 0, a.stream>>>(*a.mech, g, a.st, a.dt_dev,
                                                                                           a.max_substeps);
     return cudaGetLastError();

@@ -1990,6 +1990,8 @@ eu_status eu_autotune(eu_handle *h, int reps, eu_tune_report *report)
                                {h->st.nchem, size_t(n3) * 4}};
     if (h->st.prim32)
         parts.push_back({h->st.prim32, size_t(7 + ns) * n3 * 4});
+    if (h->st.cms) // the stiff kinetics records its sources
+        parts.push_back({h->st.cms, size_t(ns) * n3 * 8});
     size_t total = 0;
     for (const Part &q : parts) total += q.bytes;
     unsigned char *snap = nullptr;
@@ -2048,10 +2050,13 @@ eu_status eu_autotune(eu_handle *h, int reps, eu_tune_report *report)
     };
     restore();
     best = 1e30f;
-    int best_minb = 4;
-    const int minb_learned[] = {3, 4, 5, 6}, minb_other[] = {4};
-    const int *minbs = learned ? minb_learned : minb_other;
-    const int n_minb = learned ? 4 : 1;
+    // register targets: the learned-mode classification (3..6 blocks per SM),
+    // the stiff kinetics (2..4); recovery alone has one
+    const bool stiff = h->cfg.chemistry == EU_CHEM_STIFF;
+    int best_minb = stiff ? 2 : 4;
+    const int minb_learned[] = {3, 4, 5, 6}, minb_stiff[] = {2, 3, 4}, minb_other[] = {4};
+    const int *minbs = learned ? minb_learned : stiff ? minb_stiff : minb_other;
+    const int n_minb = learned ? 4 : stiff ? 3 : 1;
     for (int rb : rb_cand)
         for (int mq = 0; mq < n_minb; ++mq) {
             if (e != cudaSuccess)
@@ -2064,6 +2069,11 @@ eu_status eu_autotune(eu_handle *h, int reps, eu_tune_report *report)
                     if (learned) {
                         cudaError_t r = cudaMemsetAsync(h->lp.counts, 0, 3 * sizeof(int), h->stream);
                         return r == cudaSuccess ? L.recover_classify(a, h->lp) : r;
+                    }
+                    if (stiff) { // the step's kernel: recovery and kinetics (deferred cells' queue emptied)
+                        cudaError_t r = h->st.heavy ? cudaMemsetAsync(h->st.heavy, 0, 2 * sizeof(int), h->stream)
+                                                    : cudaSuccess;
+                        return r == cudaSuccess ? L.recover_react(a, true) : r;
                     }
                     return L.recover_react(a, false);
                 },

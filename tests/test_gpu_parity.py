@@ -26,10 +26,10 @@ FIELDS = ["CS", "T", "E", "P", "D", "U", "V", "W", "H", "Gamma", "Yi", "Nchem", 
           "Cp", "C", "Ma"]
 
 
-def solver_from_golden(eu3d, z, arith="strict", precision="fp64"):
+def solver_from_golden(eu3d, z, arith="strict", precision="fp64", chemistry="stiff"):
     ext = tuple(float(v) for v in z["extent"])
     s = eu3d.Solver(int(z["ni"]), int(z["nj"]), int(z["nk"]), ext, arith=arith, precision=precision,
-                    record_sources=True)
+                    chemistry=chemistry, record_sources=True)
     s.load_mechanism(cases.MECH_JA919, cases.THERMO)
     if "init_CS" in z:
         s.set_state(init_state(z))
@@ -318,3 +318,45 @@ def test_set_conserved_matches_set_state(gpu, precision, tol):
         s.close()
     for a, b in zip(out[0], out[1]):
         assert rel_linf(interior(b), interior(a)).max() <= tol
+
+
+@pytest.mark.parametrize("arith", ["strict", "fast"])
+def test_rk3_against_restatement(gpu, port_lib, arith):
+    """The three-stage TVD Runge-Kutta advection (eu_set_time_scheme) against
+    the C restatement's: 10 steps of the shock-bubble fixture's initial state,
+    conserved state within 1e-10 (strict) or 1e-9 (fast) per variable, Nchem
+    exact; and the scheme changes the result (it is not the Euler step)."""
+    z = golden("bubble_25x13x13_s20.npz")
+    mech = golden_mechanism()
+    port = port_lib(int(z["ni"]), int(z["nj"]), int(z["nk"]), z["x"], z["y"], z["z"], mech)
+    port.set_primitive(*[z[f"prim_{k}"] for k in "PTUVWY"])
+    port.set_scheme("rk3")
+    port.step(10, float(z["dt"]))
+    s = solver_from_golden(gpu, z, arith=arith)
+    s.set_time_scheme("rk3")
+    st = s.step(10, float(z["dt"]))
+    assert st["nonfinite"] == 0
+    want = interior(port.get("CS"))
+    assert rel_linf(interior(s.get("CS")), want).max() <= (1e-10 if arith == "strict" else 1e-9)
+    assert n_unequal(interior(s.get("Nchem")), interior(port.get("Nchem"))) == 0
+    ee = solver_from_golden(gpu, z, arith=arith)
+    ee.step(10, float(z["dt"]))
+    assert rel_linf(interior(ee.get("CS")), want).max() > 1e-6
+
+
+def test_rk3_learned_mixed_stays_close(gpu):
+    """RK3 with the benchmark's learned + mixed step: finite, and its species
+    within L1 1e-3 of the FP64 RK3 run."""
+    import learned
+    z = golden("bubble_25x13x13_s20.npz")
+    a = solver_from_golden(gpu, z)
+    a.set_time_scheme("rk3")
+    b = solver_from_golden(gpu, z, precision="mixed", chemistry="learned", arith="fast")
+    model, gate = learned.load(device=0)
+    learned.attach(b, model, gate)
+    b.set_time_scheme("rk3")
+    a.step(10, float(z["dt"]))
+    st = b.step(10, float(z["dt"]))
+    assert st["nonfinite"] == 0
+    l1 = np.abs(interior(a.get("Yi")) - interior(b.get("Yi"))).sum(axis=0).mean()
+    assert l1 <= 1e-3, l1
