@@ -1188,7 +1188,7 @@ __device__ __forceinline__ void warp_rates(const DevMech &ms, double T, const do
 }
 
 template <int NS, int NR>
-__global__ void __launch_bounds__(128, 1) k_react_heavy(const __grid_constant__ DevMech m, const DevGrid g,
+__global__ void __launch_bounds__(128, 4) k_react_heavy(const __grid_constant__ DevMech m, const DevGrid g,
                                                      const DevState st, const double *__restrict__ dt_dev,
                                                      int max_substeps)
 {

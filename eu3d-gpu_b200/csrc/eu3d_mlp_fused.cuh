@@ -286,15 +286,30 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
                 const float *bias = p.bias[e][l];
                 if (l < p.layers - 1) {
                     for (int c0 = half * 32; c0 < N; c0 += 64) {
+                        // the chunk's biases as vector loads (every lane the same
+                        // address: one broadcast each), issued before the TMEM load
+                        // so their latency overlaps it; N is a multiple of 16, so a
+                        // group of 8 columns is either inside the layer or past it
+                        float4 bv[8];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const int cbase = c0 + j * 8;
+                            if (cbase < N) {
+                                bv[2 * j] = __ldg(reinterpret_cast<const float4 *>(bias + cbase));
+                                bv[2 * j + 1] = __ldg(reinterpret_cast<const float4 *>(bias + cbase + 4));
+                            }
+                        }
                         float v[32];
                         tc::tmem_ld32(trow + c0, v);
 #pragma unroll
                         for (int j = 0; j < 4; ++j) {
                             const int cbase = c0 + j * 8;
                             if (cbase < N) {
+                                const float b8[8] = {bv[2 * j].x,     bv[2 * j].y,     bv[2 * j].z,     bv[2 * j].w,
+                                                     bv[2 * j + 1].x, bv[2 * j + 1].y, bv[2 * j + 1].z, bv[2 * j + 1].w};
                                 __align__(16) __nv_bfloat16 h[8];
 #pragma unroll
-                                for (int q = 0; q < 8; ++q) h[q] = __float2bfloat16_rn(silu_fast(v[j * 8 + q] + bias[cbase + q]));
+                                for (int q = 0; q < 8; ++q) h[q] = __float2bfloat16_rn(silu_fast(v[j * 8 + q] + b8[q]));
                                 *reinterpret_cast<uint4 *>(act + ((cbase / 8) * kFusedRows + lrow) * 16) =
                                     *reinterpret_cast<const uint4 *>(h);
                             }

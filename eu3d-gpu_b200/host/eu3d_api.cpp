@@ -102,6 +102,9 @@ eu_status fail(eu_handle *h, eu_status s, const char *fmt, ...)
 
 eu_status cuda_fail(eu_handle *h, cudaError_t e, const char *what)
 {
+    // a failed call leaves its error as the runtime's last error: clear it, so
+    // the next launch's cudaGetLastError reports that launch, not this call
+    (void)cudaGetLastError();
     if (e == cudaErrorMemoryAllocation)
         return fail(h, EU_ERR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
     return fail(h, EU_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
@@ -1509,7 +1512,7 @@ const char *kDumpPlanes[14] = {"D", "T", "U", "V", "W", "E", "Wav", "Rgas", "Cp"
 // Di (ns), Yi (ns), CS (ns + 4), CMS (ns), then Nchem as n3 ints.
 size_t snap_planes(int kind, int ns)
 {
-    return kind == EU_OUTPUT_TECPLOT ? 6 + kTecplotSpecies : 14 + 4 * size_t(ns) + 4;
+    return kind == EU_OUTPUT_TECPLOT ? 6 + kTecplotSpecies : 14 + 4 * size_t(ns) + 4 + 1; // + the Nchem ints
 }
 
 // One plane of field `name` into dst on the handle's stream (device to device).
@@ -2090,6 +2093,9 @@ eu_status eu_autotune(eu_handle *h, int reps, eu_tune_report *report)
             }
         }
     restore();
+    // the timed kinetics launches counted into the step statistics
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(h->st.counters, 0, kCntCount * sizeof(unsigned long long), h->stream);
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(h->stream);
     cudaFree(snap);
