@@ -656,16 +656,23 @@ __device__ __forceinline__ void muscl(R fm1, R f0, R f1, R f2, R &left, R &right
 template <typename R, bool kStrict>
 __device__ __forceinline__ R muscl_upwind(bool up, R fm1, R f0, R f1, R f2)
 {
+    if constexpr (!kStrict && std::is_same<R, float>::value) {
+        // The side's base u, outer point w and inner point v (up: f0, fm1, f1;
+        // down: f1, f2, f0): the value is u + (u - w)/2 sat((v - u) / ((u - w)
+        // + e)) with e = +1e-12 (up) or -1e-12 (down), one fused multiply-add.
+        // Every term of the down side is the exact negation of the form
+        // f1 - (a/2) sat(A1 / (a + 1e-12)), a = f2 - f1, A1 = f1 - f0
+        // (round-to-nearest is symmetric), so the value is bitwise that form's;
+        // selecting the three points first saves the arithmetic of the side
+        // not taken.
+        const R u = up ? f0 : f1, w = up ? fm1 : f2, v = up ? f1 : f0;
+        const R d = u - w;
+        const R L = __saturatef(div_fast(v - u, d + (up ? R(1e-12) : R(-1e-12))));
+        return fmaf(R(0.5) * d, L, u);
+    }
     const R A1 = f1 - f0;
     const R a = up ? f0 - fm1 : f2 - f1;
-    if constexpr (!kStrict && std::is_same<R, float>::value) {
-        // f0 + (a/2) L or f1 - (a/2) L as one fused multiply-add on the
-        // selected base: the product's sign is exact, so the value is that of
-        // either side's own fused form
-        const R L = __saturatef(div_fast(A1, a + R(1e-12)));
-        const R h = (up ? R(0.5) : R(-0.5)) * a;
-        return fmaf(h, L, up ? f0 : f1);
-    } else {
+    {
         const R t = muscl_slope<R, kStrict>(a, A1);
         return up ? f0 + t : f1 - t;
     }

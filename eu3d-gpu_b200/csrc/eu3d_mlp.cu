@@ -241,7 +241,7 @@ cudaError_t mlp_fused(const FusedMlpParams &p, const float *feat, int ld_feat, i
 {
     if (!fused_supported(p.in_pad, p.width, p.out_pad, p.members, p.layers))
         return cudaErrorInvalidValue;
-    const size_t smem = fused_smem_bytes(p.in_pad, p.width);
+    const size_t smem = fused_smem_bytes(p.in_pad, p.width, p.out_pad, p.layers, p.members);
     static SmemLimit limit; // per device: the largest size set so far
     const cudaError_t e = limit.ensure(k_mlp_fused, smem);
     if (e != cudaSuccess)

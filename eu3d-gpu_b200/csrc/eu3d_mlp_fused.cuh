@@ -50,20 +50,10 @@
 
 namespace eu3d {
 
-constexpr int kFusedStages = 5, kFusedRows = 128, kFusedStreams = 2, kFusedEpiWarps = 8;
+constexpr int kFusedEpiWarps = 8;
 constexpr int kFusedMmaWarp = kFusedStreams * kFusedEpiWarps, kFusedCopyWarp = kFusedMmaWarp + 1;
 constexpr int kFusedThreads = (kFusedCopyWarp + 1) * 32;
 constexpr int kFusedTmemCols = 256 * kFusedStreams;
-
-// Bytes of shared memory the kernel needs for a model.
-// At least 116 KB, so that one CTA (and its 512 TMEM columns) fits per SM.
-inline size_t fused_smem_bytes(int in_pad, int width)
-{
-    const size_t need = size_t(kFusedStages) * width * kFusedSlabK * 2 +
-                        size_t(kFusedStreams) * kFusedRows * (size_t(width) + in_pad) * 2 +
-                        8 * (2 * kFusedStages + 2 * kFusedStreams) + 16;
-    return need > 116 * 1024 ? need : 116 * 1024;
-}
 
 __device__ __forceinline__ int fused_K(const FusedMlpParams &p, int l) { return l == 0 ? p.in_pad : p.width; }
 __device__ __forceinline__ int fused_N(const FusedMlpParams &p, int l)
@@ -113,10 +103,13 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     extern __shared__ __align__(128) unsigned char smem[];
     const uint32_t slot_bytes = uint32_t(p.width) * kFusedSlabK * 2;
     const uint32_t act_bytes = uint32_t(kFusedRows) * p.width * 2, fin_bytes = uint32_t(kFusedRows) * p.in_pad * 2;
+    const uint32_t nbias = uint32_t((p.layers - 1) * p.width + p.out_pad); // fused_bias_floats
+    const uint32_t bias_bytes = (uint32_t(p.members) * nbias * 4 + 15) / 16 * 16;
     unsigned char *ring = smem;
     unsigned char *act0 = ring + kFusedStages * slot_bytes;
     unsigned char *fin0 = act0 + kFusedStreams * act_bytes;
-    uint64_t *full = reinterpret_cast<uint64_t *>(fin0 + kFusedStreams * fin_bytes);
+    float *sbias = reinterpret_cast<float *>(fin0 + kFusedStreams * fin_bytes); // [member][layer][N]
+    uint64_t *full = reinterpret_cast<uint64_t *>(reinterpret_cast<unsigned char *>(sbias) + bias_bytes);
     uint64_t *empty = full + kFusedStages;
     uint64_t *accf = empty + kFusedStages;  // per stream: the layer's MMAs are done
     uint64_t *ready = accf + kFusedStreams; // per stream: A operand written, accumulator read
@@ -150,6 +143,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    // every member's biases into shared memory (read by the epilogues)
+    for (int e = 0; e < p.members; ++e)
+        for (int l = 0, o = e * int(nbias); l < p.layers; o += fused_N(p, l), ++l)
+            for (int c = tid; c < fused_N(p, l); c += kFusedThreads) sbias[o + c] = p.bias[e][l][c];
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
@@ -283,37 +280,38 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
                 }
                 tc::tc_fence_after();
                 const int N = fused_N(p, l);
-                const float *bias = p.bias[e][l];
+                int boff = e * int(nbias);
+                for (int q = 0; q < l; ++q) boff += fused_N(p, q);
+                const float *bias = sbias + boff;
                 if (l < p.layers - 1) {
-                    for (int c0 = half * 32; c0 < N; c0 += 64) {
-                        // the chunk's biases as vector loads (every lane the same
-                        // address: one broadcast each), issued before the TMEM load
-                        // so their latency overlaps it; N is a multiple of 16, so a
-                        // group of 8 columns is either inside the layer or past it
-                        float4 bv[8];
+                    // two 32-column chunks per TMEM wait (columns c0 and c0 + 64);
+                    // N is a multiple of 16, so a group of 8 columns is either
+                    // inside the layer or past it
+                    for (int c0 = half * 32; c0 < N; c0 += 128) {
+                        uint32_t raw[2][32];
+                        tc::tmem_ld32_issue(trow + c0, raw[0]);
+                        if (c0 + 64 < N)
+                            tc::tmem_ld32_issue(trow + c0 + 64, raw[1]);
+                        tc::tmem_ld_wait();
+                        tc::tmem_reg_fence(raw[0]);
+                        tc::tmem_reg_fence(raw[1]);
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const int cbase = c0 + j * 8;
-                            if (cbase < N) {
-                                bv[2 * j] = __ldg(reinterpret_cast<const float4 *>(bias + cbase));
-                                bv[2 * j + 1] = __ldg(reinterpret_cast<const float4 *>(bias + cbase + 4));
+                        for (int u = 0; u < 2; ++u)
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) {
+                                const int cbase = c0 + 64 * u + j * 8;
+                                if (cbase < N) {
+                                    const float4 b0 = *reinterpret_cast<const float4 *>(bias + cbase);
+                                    const float4 b1 = *reinterpret_cast<const float4 *>(bias + cbase + 4);
+                                    const float b8[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+                                    __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+                                    for (int q = 0; q < 8; ++q)
+                                        h[q] = __float2bfloat16_rn(silu_fast(__uint_as_float(raw[u][j * 8 + q]) + b8[q]));
+                                    *reinterpret_cast<uint4 *>(act + ((cbase / 8) * kFusedRows + lrow) * 16) =
+                                        *reinterpret_cast<const uint4 *>(h);
+                                }
                             }
-                        }
-                        float v[32];
-                        tc::tmem_ld32(trow + c0, v);
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const int cbase = c0 + j * 8;
-                            if (cbase < N) {
-                                const float b8[8] = {bv[2 * j].x,     bv[2 * j].y,     bv[2 * j].z,     bv[2 * j].w,
-                                                     bv[2 * j + 1].x, bv[2 * j + 1].y, bv[2 * j + 1].z, bv[2 * j + 1].w};
-                                __align__(16) __nv_bfloat16 h[8];
-#pragma unroll
-                                for (int q = 0; q < 8; ++q) h[q] = __float2bfloat16_rn(silu_fast(v[j * 8 + q] + b8[q]));
-                                *reinterpret_cast<uint4 *>(act + ((cbase / 8) * kFusedRows + lrow) * 16) =
-                                    *reinterpret_cast<const uint4 *>(h);
-                            }
-                        }
                     }
                     tc::fence_proxy_async();
                     arrive_ready();

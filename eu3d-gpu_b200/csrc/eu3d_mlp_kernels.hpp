@@ -10,6 +10,10 @@ namespace eu3d {
 // The fused inference kernel (eu3d_mlp_fused.cuh): model shape, packed weight
 // slabs and per-layer biases.
 constexpr int kFusedMaxMembers = 8, kFusedMaxLayers = 9, kFusedSlabK = 32;
+// weight-ring slots, rows per tile, jobs in flight; the opt-in shared-memory
+// limit of a block on sm_100 (227 KB)
+constexpr int kFusedStages = 5, kFusedRows = 128, kFusedStreams = 2;
+constexpr size_t kFusedMaxSmem = 232448;
 struct FusedMlpParams {
     int members, layers; // layers = hidden + output
     int n_in, in_pad, width, out_pad, n_out;
@@ -19,12 +23,33 @@ struct FusedMlpParams {
     const float *in_shift, *in_scale, *out_shift, *out_scale;
 };
 
+// Biases of one member (every layer's N); the kernel keeps every member's in
+// shared memory.
+inline size_t fused_bias_floats(int width, int out_pad, int layers)
+{
+    return size_t(layers - 1) * width + out_pad;
+}
+
+// Bytes of shared memory the fused kernel needs for a model: the weight ring,
+// each stream's activations and features, the members' biases, the mbarriers.
+// At least 116 KB, so that one block (and its 512 TMEM columns) fits per SM.
+inline size_t fused_smem_bytes(int in_pad, int width, int out_pad, int layers, int members)
+{
+    const size_t bias = (size_t(members) * fused_bias_floats(width, out_pad, layers) * 4 + 15) / 16 * 16;
+    const size_t need = size_t(kFusedStages) * width * kFusedSlabK * 2 +
+                        size_t(kFusedStreams) * size_t(kFusedRows) * (size_t(width) + in_pad) * 2 + bias +
+                        8 * (2 * kFusedStages + 2 * kFusedStreams) + 16;
+    return need > 116 * 1024 ? need : 116 * 1024;
+}
+
 // Shapes the fused kernel takes: every layer's N fits the 256 TMEM columns and
-// the ring slot (sized for width), the input tile fits its buffer.
+// the ring slot (sized for width), the input tile fits its buffer, and all of
+// it fits a block's shared memory.
 inline bool fused_supported(int in_pad, int width, int out_pad, int members, int layers)
 {
     return width % 16 == 0 && width >= 16 && width <= 256 && in_pad <= 64 && out_pad <= width &&
-           members <= kFusedMaxMembers && layers <= kFusedMaxLayers;
+           members >= 1 && members <= kFusedMaxMembers && layers >= 2 && layers <= kFusedMaxLayers &&
+           fused_smem_bytes(in_pad, width, out_pad, layers, members) <= kFusedMaxSmem;
 }
 
 // Predictions of every member for the first `count` rows of feat (count read

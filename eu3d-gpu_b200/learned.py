@@ -67,8 +67,44 @@ def _initial_compositions(rng, n, mw):
     return Y / Y.sum(axis=1, keepdims=True)
 
 
+def front_states(n_max, seed=17, steps=40, dt=2e-8, device=0):
+    """(T, p, Y) of the chemically active cells of igniting blocks (the stiff
+    FP64 step on eu3d_cases.hot_reacting_block variants: 1100-2600 K along x,
+    0.05-2 MPa along y, 0-60 % N2 along z), every step of their ignition:
+    states on the reaction front itself, where the generic trajectories of
+    generate() are thin. At most n_max states, drawn at random."""
+    rng = np.random.default_rng(seed)
+    mech = eu3d.parse_mechanism(cases.MECH_JA919, cases.THERMO)
+    grid = (48, 24, 24)
+    ext = (0.0, 0.012, 0.0, 0.006, 0.0, 0.006)
+    out_T, out_p, out_Y = [], [], []
+    for t_range, p_range in (((1100.0, 2000.0), (5e4, 1e6)), ((1300.0, 2600.0), (1e5, 2e6)),
+                             ((1200.0, 2400.0), (2e5, 5e5))):
+        prim = cases.hot_reacting_block(grid[0] + 4, grid[1] + 4, grid[2] + 4, mech["mw"], mech["ns"],
+                                        t_range=t_range, p_range=p_range)
+        s = eu3d.Solver(*grid, ext, precision="fp64", chemistry="stiff", arith="fast", device=device)
+        s.set_mechanism(mech)
+        s.set_primitive(*prim)
+        for _ in range(steps):
+            s.step(1, dt, stats=False)
+            T = s.get("T")[0, 2:-2, 2:-2, 2:-2].ravel()
+            P = s.get("P")[0, 2:-2, 2:-2, 2:-2].ravel()
+            Y = s.get("Yi")[:, 2:-2, 2:-2, 2:-2].reshape(mech["ns"], -1)
+            radical = Y[list(RADICALS)].sum(0)
+            act = (Y[:N_SPECIES - 1].sum(0) >= FROZEN_Y) & ((T >= FROZEN_T) | (radical >= FROZEN_RADICAL))
+            out_T.append(T[act])
+            out_p.append(P[act])
+            out_Y.append(Y[:, act].T)
+        s.close()
+    T, P, Y = np.concatenate(out_T), np.concatenate(out_p), np.concatenate(out_Y)
+    if T.size > n_max:
+        pick = rng.choice(T.size, n_max, replace=False)
+        T, P, Y = T[pick], P[pick], Y[pick]
+    return T, P, Y
+
+
 def generate(solver, n_traj, n_steps, seed=11, t_range=(300.0, 3500.0), p_range=(5e4, 5e6), dt_range=(1e-9, 3e-7),
-             max_substeps=20000, with_nchem=False):
+             max_substeps=20000, with_nchem=False, init=None):
     """(inputs, targets) as torch CUDA fp32 tensors, up to n_traj * n_steps rows
     (with_nchem: and each row's Nchem, the stiff kinetics' substeps for it).
 
@@ -84,9 +120,13 @@ def generate(solver, n_traj, n_steps, seed=11, t_range=(300.0, 3500.0), p_range=
     mech = solver.mechanism()
     ns = mech["ns"]
     dev = "cuda"
-    T0 = rng.uniform(*t_range, n_traj)
-    p0 = np.exp(rng.uniform(math.log(p_range[0]), math.log(p_range[1]), n_traj))
-    Y0 = _initial_compositions(rng, n_traj, mech["mw"])
+    if init is not None:  # given start states (T, p, Y rows)
+        T0, p0, Y0 = (np.asarray(a, dtype=np.float64) for a in init)
+        n_traj = T0.size
+    else:
+        T0 = rng.uniform(*t_range, n_traj)
+        p0 = np.exp(rng.uniform(math.log(p_range[0]), math.log(p_range[1]), n_traj))
+        Y0 = _initial_compositions(rng, n_traj, mech["mw"])
     T = torch.tensor(T0, device=dev, dtype=torch.float64)
     p = torch.tensor(p0, device=dev, dtype=torch.float64)
     Yp = torch.tensor(np.ascontiguousarray(Y0.T), device=dev, dtype=torch.float64)

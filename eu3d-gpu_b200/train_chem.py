@@ -53,6 +53,9 @@ def main():
     ap.add_argument("--front-only", action="store_true",
                     help="keep the checkpoint's weights and gate; only tighten tau for the front criterion")
     ap.add_argument("--max-shift", type=int, default=0, help="largest reaction-front shift (cells) the gate may cause")
+    ap.add_argument("--front-traj", type=int, default=0,
+                    help="also start this many trajectories from states of igniting blocks (learned.front_states), "
+                         "with dt ~ logU[5e-9, 5e-8] s, the reaction front's own states")
     ap.add_argument("--rows-min-nchem", type=int, default=0,
                     help="train and calibrate only on rows whose Nchem exceeds this (0: every active row). "
                          "With 4 (the rows the default Nchem routing hands to the model) 0.69 M rows remain and "
@@ -68,6 +71,12 @@ def main():
     s = eu3d.Solver(5, 5, 5, (0, 1, 0, 1, 0, 1), max_substeps=20000)
     s.load_mechanism(cases.MECH_JA919, cases.THERMO)
     X, T, N = learned.generate(s, args.traj, args.steps_per_traj, seed=args.seed, with_nchem=True)
+    if args.front_traj > 0:
+        init = learned.front_states(args.front_traj, seed=args.seed + 7)
+        Xf, Tf, Nf = learned.generate(s, 0, args.steps_per_traj // 5 or 1, seed=args.seed + 7, with_nchem=True,
+                                      dt_range=(5e-9, 5e-8), init=init)
+        print(f"{Xf.shape[0]} rows from {init[0].size} front states", flush=True)
+        X, T, N = torch.cat([X, Xf]), torch.cat([T, Tf]), torch.cat([N, Nf])
     s.close()
     act = learned.active_rows(X) & (N > args.rows_min_nchem)
     X, T = X[act].contiguous(), T[act].contiguous()
@@ -87,7 +96,8 @@ def main():
     gate = learned.calibrate(model, scaling, X[va].contiguous(), T[va].contiguous(), target=args.target,
                              bound=bound)
     gate["min_nchem"] = learned.MIN_NCHEM  # the routing the checkpoint is used with
-    meta = {"traj": args.traj, "steps_per_traj": args.steps_per_traj, "train_steps": args.train_steps,
+    meta = {"traj": args.traj, "front_traj": args.front_traj, "steps_per_traj": args.steps_per_traj,
+            "train_steps": args.train_steps,
             "rows_min_nchem": args.rows_min_nchem,
             "batch": args.batch, "lr": args.lr, "seed": args.seed, "samples": n,
             "accepted_fraction": gate["accepted_fraction"], "l1_accepted": gate["l1_accepted"], "tau": gate["tau"]}
