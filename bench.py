@@ -665,21 +665,37 @@ def batch_instances(args, model, gate, local, mech, count=32):
         single_ms.append(r["device_ms"] / args.steps)
         s.close()
     torch.cuda.synchronize()
-    # together: learned + mixed, one graph launch per step
-    solvers = [solver(grid, ext, st, "learned", "mixed") for (grid, ext, st, _) in built]
+    # together: learned + mixed, one graph launch per step; the fallback and
+    # deferred-cell kinetics of all instances as one shared stage, and (for
+    # comparison) inside each instance's branch
     dts = [dt for (_, _, _, dt) in built]
-    b = eu3d.Batch(solvers)
-    b.step(args.warmup, dts)
-    stats, ms = b.step(args.steps, dts)
-    b.close()
-    for s in solvers:
-        s.close()
+    runs = {}
+    for shared in (False, True):
+        solvers = [solver(grid, ext, st, "learned", "mixed") for (grid, ext, st, _) in built]
+        b = eu3d.Batch(solvers)
+        b.set_shared_kinetics(shared)
+        b.step(args.warmup, dts)
+        stats, ms = b.step(args.steps, dts)
+        runs[shared] = (stats, ms, b.launches())
+        b.close()
+        for s in solvers:
+            s.close()
+    stats, ms, (per_step, stage) = runs[True]
+    branch_ms = runs[False][1]
     one_by_one = total * args.steps / (sum(single_ms) * args.steps / 1e3) / 1e6
     together = total * args.steps / (ms / 1e3) / 1e6
     return {"instances": count, "cells": total, "grids": {f"{g[0]}x{g[1]}x{g[2]}": sum(1 for b_ in built if b_[0] == g)
                                                            for g in BATCH_SIZES},
             "learned_mixed_batch": {"value": round(together, 3), "ms_per_step": round(ms / args.steps, 4),
-                                    "launches_per_step": 1,
+                                    "graph_launches_per_step": 1, "kernels_per_step": per_step,
+                                    "shared_kinetics_launches_per_step": stage,
+                                    # launches per stage: the ghost fill, flux, recovery and model
+                                    # stages run once per instance; the fallback and deferred-cell
+                                    # kinetics stages once for the whole batch
+                                    "launches_per_stage": {"per_instance_stages": len(built),
+                                                           "shared_kinetics_stages": stage // 2 if stage else 0},
+                                    "ms_per_step_kinetics_in_branches": round(branch_ms / args.steps, 4),
+                                    "kernels_per_step_kinetics_in_branches": runs[False][2][0],
                                     "learned_cells_last_step": int(sum(st_["learned"] for st_ in stats)),
                                     "max_nchem": int(max(st_["max_nchem"] for st_ in stats))},
             "plain_fp64_one_by_one": {"value": round(one_by_one, 3), "ms_per_step": round(sum(single_ms), 4),
@@ -786,6 +802,7 @@ def our_arm_blocks(args, world, rank, local, dist):
         sp_ = make("stiff", "fp64", "fast")
         if start:
             sp_.step(start, dt, stats=False)
+        ptuned = sp_.autotune(reps=5) if not args.no_autotune else None
         _, pms, _ = timed(sp_)
         y_ref = sp_.get("Yi")
         sp_.close()

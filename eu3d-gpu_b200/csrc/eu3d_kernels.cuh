@@ -1009,6 +1009,69 @@ __global__ void __launch_bounds__(128) k_learned_apply(const __grid_constant__ D
     }
 }
 
+// The stiff kinetics of one queued cell whose recovered state is stored.
+template <int NS, class Rt>
+__device__ __forceinline__ void react_queued(const DevMech &m, const DevState &st, long long n3, long long c,
+                                             double dtm, int max_substeps, int counter)
+{
+    CellState<NS> cell;
+    load_recovered<NS>(st, n3, c, cell);
+    atomicAdd(&st.counters[counter], 1ULL);
+    if (react_or_defer<NS, Rt>(m, st, n3, c, cell, dtm, max_substeps))
+        store_cell<NS>(m, st, n3, c, cell);
+}
+
+// Position `pos` of the batch's queues taken end to end: the instance holding
+// it and the position within that instance's queue (lengths from len(q)).
+template <class Len>
+__device__ __forceinline__ int batch_locate(int n, int pos, Len len, int &local)
+{
+    int q = 0, off = 0;
+    for (; q < n; ++q) {
+        const int l = len(q);
+        if (pos < off + l)
+            break;
+        off += l;
+    }
+    local = pos - off;
+    return q;
+}
+
+// The stiff-fallback queues of every instance of a batch drained by one fixed
+// grid: warps take 32 positions at a time from one counter over the queues
+// taken end to end (the shared reacting-cell work queue), so the cells of all
+// instances are spread over the whole GPU. Per cell the same work as
+// k_react_queue; every instance's statistics go to its own counters.
+template <int NS, class Rt>
+__global__ void __launch_bounds__(128) k_react_queue_batch(const __grid_constant__ DevMech m,
+                                                           const BatchCell *__restrict__ tab, int n, int *next,
+                                                           int max_substeps, int counter)
+{
+    auto len = [&](int q) { return tab[q].count ? *(volatile const int *)tab[q].count : 0; };
+    int total = 0;
+    for (int q = 0; q < n; ++q) total += len(q);
+    if (total == 0)
+        return;
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int base = 0;
+        if (lane == 0)
+            base = atomicAdd(next, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total)
+            break;
+        const int pos = base + lane;
+        if (pos < total) {
+            int local = 0;
+            const int q = batch_locate(n, pos, len, local);
+            if (q < n) {
+                const BatchCell &b = tab[q];
+                react_queued<NS, Rt>(m, b.st, b.n3, b.queue[local], *b.dt, max_substeps, counter);
+            }
+        }
+    }
+}
+
 // The stiff kinetics on a queue of cells whose recovered state is stored.
 template <int NS, class Rt>
 __global__ void __launch_bounds__(128) k_react_queue(const __grid_constant__ DevMech m, const DevGrid g,
@@ -1030,14 +1093,8 @@ __global__ void __launch_bounds__(128) k_react_queue(const __grid_constant__ Dev
         if (base >= nq)
             break;
         const int q = base + lane;
-        if (q < nq) {
-            const long long n3 = g.n3, c = queue[q];
-            CellState<NS> cell;
-            load_recovered<NS>(st, n3, c, cell);
-            atomicAdd(&st.counters[counter], 1ULL);
-            if (react_or_defer<NS, Rt>(m, st, n3, c, cell, *dt_dev, max_substeps))
-                store_cell<NS>(m, st, n3, c, cell);
-        }
+        if (q < nq)
+            react_queued<NS, Rt>(m, st, g.n3, queue[q], *dt_dev, max_substeps, counter);
     }
 }
 
@@ -1187,6 +1244,72 @@ __device__ __forceinline__ void warp_rates(const DevMech &ms, double T, const do
     Wl = ms.mw[sl] * W;
 }
 
+// One deferred cell advanced by a whole warp: lane r evaluates reaction r,
+// lane s owns species s's sums and trapezoid update, every lane rebuilds the
+// state (ms: the mechanism tables in shared memory).
+template <int NS, int NR>
+__device__ __forceinline__ void react_heavy_cell(const DevMech &m, const DevMech &ms, const DevState &st, long long n3,
+                                                 long long c, double dtm, int max_substeps, int lane)
+{
+    CellState<NS> cell;
+    load_recovered<NS>(st, n3, c, cell);
+    double mc[NS], P, Q, W;
+    scaled_concentrations<NS>(m, cell, mc);
+    warp_rates<NS, NR>(ms, cell.T, mc, lane, P, Q, W);
+    // prediction: min over the species lanes, then every lane has Nchem
+    double dt = dtm;
+    if (lane < NS && lane_pick<NS>(cell.Y, lane) >= 1e-6 && W != 0)
+        dt = fmin(dt, fabs(-(lane_pick<NS + 4>(cell.cs, lane) * 1e-3) / W));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dt = fmin(dt, __shfl_xor_sync(0xffffffffu, dt, o));
+    int nchem = 0;
+    if (lane == 0) {
+        nchem = nchem_from_dt(dtm, dt, max_substeps, st.counters);
+        count_nchem(st.counters, nchem);
+    }
+    nchem = __shfl_sync(0xffffffffu, nchem, 0);
+    const double dts = dtm / nchem, half = dts / 2.0;
+    for (int step = 0; step < nchem; ++step) {
+        if (step > 0) {
+            scaled_concentrations<NS>(m, cell, mc);
+            warp_rates<NS, NR>(ms, cell.T, mc, lane, P, Q, W);
+        }
+        if (st.cms && lane < NS)
+            st.cms[lane * n3 + c] = W * 1e3;
+        double nd = 0.0;
+        if (lane < NS) {
+            const double di = lane_pick<NS + 4>(cell.cs, lane) * 1e-3;
+            const double mcl = lane_pick<NS>(mc, lane);
+            const double qv = ms.mw[lane] * Q;
+            const double pv = (mcl == 0) ? 0.0 : P / mcl;
+            nd = ((1.0 - half * pv) * di + dts * qv) / (1.0 + half * pv) * 1e3;
+        }
+        double D = 0.0;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            cell.cs[s] = __shfl_sync(0xffffffffu, nd, s);
+            D += cell.cs[s];
+        }
+        cell.cs[NS + 0] = cell.U * D;
+        cell.cs[NS + 1] = cell.V * D;
+        cell.cs[NS + 2] = cell.W * D;
+        cell.cs[NS + 3] = D * cell.E + 0.5 * (cell.U * cell.U + cell.V * cell.V + cell.W * cell.W) * D;
+        recover_state<NS>(m, cell);
+    }
+    if (lane == 0) {
+        st.nchem[c] = nchem;
+        store_cell<NS>(m, st, n3, c, cell);
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void copy_mech_to_shared(const DevMech &m, DevMech &ms)
+{
+    const int *src = reinterpret_cast<const int *>(&m);
+    int *dst = reinterpret_cast<int *>(&ms);
+    for (int w = threadIdx.x; w < int(sizeof(DevMech) / sizeof(int)); w += blockDim.x) dst[w] = src[w];
+}
+
 template <int NS, int NR>
 __global__ void __launch_bounds__(128, 4) k_react_heavy(const __grid_constant__ DevMech m, const DevGrid g,
                                                      const DevState st, const double *__restrict__ dt_dev,
@@ -1196,15 +1319,10 @@ __global__ void __launch_bounds__(128, 4) k_react_heavy(const __grid_constant__ 
     const int count = st.heavy[0];
     if (count == 0) // no deferred cell this step: skip the table copy
         return;
-    {
-        const int *src = reinterpret_cast<const int *>(&m);
-        int *dst = reinterpret_cast<int *>(&ms);
-        for (int w = threadIdx.x; w < int(sizeof(DevMech) / sizeof(int)); w += blockDim.x) dst[w] = src[w];
-    }
+    copy_mech_to_shared(m, ms);
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const double dtm = *dt_dev;
-    const long long n3 = g.n3;
     for (;;) {
         int q = 0;
         if (lane == 0)
@@ -1212,57 +1330,39 @@ __global__ void __launch_bounds__(128, 4) k_react_heavy(const __grid_constant__ 
         q = __shfl_sync(0xffffffffu, q, 0);
         if (q >= count)
             break;
-        const long long c = st.heavy[2 + q];
-        CellState<NS> cell;
-        load_recovered<NS>(st, n3, c, cell);
-        double mc[NS], P, Q, W;
-        scaled_concentrations<NS>(m, cell, mc);
-        warp_rates<NS, NR>(ms, cell.T, mc, lane, P, Q, W);
-        // prediction: min over the species lanes, then every lane has Nchem
-        double dt = dtm;
-        if (lane < NS && lane_pick<NS>(cell.Y, lane) >= 1e-6 && W != 0)
-            dt = fmin(dt, fabs(-(lane_pick<NS + 4>(cell.cs, lane) * 1e-3) / W));
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) dt = fmin(dt, __shfl_xor_sync(0xffffffffu, dt, o));
-        int nchem = 0;
-        if (lane == 0) {
-            nchem = nchem_from_dt(dtm, dt, max_substeps, st.counters);
-            count_nchem(st.counters, nchem);
+        react_heavy_cell<NS, NR>(m, ms, st, g.n3, st.heavy[2 + q], dtm, max_substeps, lane);
+    }
+}
+
+// The deferred cells of every instance of a batch, their heavy queues taken
+// end to end, drained by one persistent grid (one warp per cell, one counter).
+template <int NS, int NR>
+__global__ void __launch_bounds__(128, 4) k_react_heavy_batch(const __grid_constant__ DevMech m,
+                                                           const BatchCell *__restrict__ tab, int n, int *next,
+                                                           int max_substeps)
+{
+    __shared__ DevMech ms;
+    auto len = [&](int q) { return tab[q].st.heavy ? *(volatile const int *)tab[q].st.heavy : 0; };
+    int total = 0;
+    for (int q = 0; q < n; ++q) total += len(q);
+    if (total == 0)
+        return;
+    copy_mech_to_shared(m, ms);
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int pos = 0;
+        if (lane == 0)
+            pos = atomicAdd(next, 1);
+        pos = __shfl_sync(0xffffffffu, pos, 0);
+        if (pos >= total)
+            break;
+        int local = 0;
+        const int q = batch_locate(n, pos, len, local);
+        if (q < n) {
+            const BatchCell &b = tab[q];
+            react_heavy_cell<NS, NR>(m, ms, b.st, b.n3, b.st.heavy[2 + local], *b.dt, max_substeps, lane);
         }
-        nchem = __shfl_sync(0xffffffffu, nchem, 0);
-        const double dts = dtm / nchem, half = dts / 2.0;
-        for (int step = 0; step < nchem; ++step) {
-            if (step > 0) {
-                scaled_concentrations<NS>(m, cell, mc);
-                warp_rates<NS, NR>(ms, cell.T, mc, lane, P, Q, W);
-            }
-            if (st.cms && lane < NS)
-                st.cms[lane * n3 + c] = W * 1e3;
-            double nd = 0.0;
-            if (lane < NS) {
-                const double di = lane_pick<NS + 4>(cell.cs, lane) * 1e-3;
-                const double mcl = lane_pick<NS>(mc, lane);
-                const double qv = ms.mw[lane] * Q;
-                const double pv = (mcl == 0) ? 0.0 : P / mcl;
-                nd = ((1.0 - half * pv) * di + dts * qv) / (1.0 + half * pv) * 1e3;
-            }
-            double D = 0.0;
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-                cell.cs[s] = __shfl_sync(0xffffffffu, nd, s);
-                D += cell.cs[s];
-            }
-            cell.cs[NS + 0] = cell.U * D;
-            cell.cs[NS + 1] = cell.V * D;
-            cell.cs[NS + 2] = cell.W * D;
-            cell.cs[NS + 3] = D * cell.E + 0.5 * (cell.U * cell.U + cell.V * cell.V + cell.W * cell.W) * D;
-            recover_state<NS>(m, cell);
-        }
-        if (lane == 0) {
-            st.nchem[c] = nchem;
-            store_cell<NS>(m, st, n3, c, cell);
-        }
-        __syncwarp();
     }
 }
 

@@ -230,6 +230,31 @@ cudaError_t heavy_t(const LaunchArgs &a, int blocks)
     return cudaGetLastError();
 }
 
+// The batch's shared kinetics stage: the stiff-fallback queues, then the
+// deferred cells, of every instance in tab[0..n) drained by one fixed grid
+// each (next[0] and next[1] zero at launch). a: any member's arguments (the
+// mechanism, flavour and substep cap are the same over the table).
+template <int NS, int NR>
+cudaError_t react_queue_batch_t(const LaunchArgs &a, const BatchCell *tab, int n, int *next, int counter)
+{
+    const dim3 grid(queue_grid(a, 4));
+    if (a.spec == 1 && NS == Mech_JA919::NS && NR == Mech_JA919::NR)
+        k_react_queue_batch<NS, Mech_JA919><<<grid, 128, 0, a.stream>>>(*a.mech, tab, n, next, a.max_substeps,
+                                                                        counter);
+    else
+        k_react_queue_batch<NS, TableRates<NS, NR>><<<grid, 128, 0, a.stream>>>(*a.mech, tab, n, next,
+                                                                                a.max_substeps, counter);
+    return cudaGetLastError();
+}
+
+template <int NS, int NR>
+cudaError_t heavy_batch_t(const LaunchArgs &a, const BatchCell *tab, int n, int *next, int blocks)
+{
+    k_react_heavy_batch<NS, NR><<<dim3(unsigned(blocks)), 128, 0, a.stream>>>(*a.mech, tab, n, next + 1,
+                                                                               a.max_substeps);
+    return cudaGetLastError();
+}
+
 } // namespace
 
 // Supported (NS, NR): the repository mechanism H2_JA919 (9 species, 19
@@ -275,6 +300,14 @@ cudaError_t launch_chem_samples(const LaunchArgs &a, long long n, double *cs, do
 }
 
 cudaError_t launch_react_heavy(const LaunchArgs &a, int blocks) { EU3D_DISPATCH(heavy_t, a, blocks) }
+cudaError_t launch_react_queue_batch(const LaunchArgs &a, const BatchCell *tab, int n, int *next, int counter)
+{
+    EU3D_DISPATCH(react_queue_batch_t, a, tab, n, next, counter)
+}
+cudaError_t launch_react_heavy_batch(const LaunchArgs &a, const BatchCell *tab, int n, int *next, int blocks)
+{
+    EU3D_DISPATCH(heavy_batch_t, a, tab, n, next, blocks)
+}
 
 cudaError_t launch_cfl(const LaunchArgs &a, double cfl, unsigned long long *slot, double *time)
 {
@@ -326,7 +359,8 @@ cudaError_t launch_set_value(double *dst, double v, cudaStream_t s)
 const Launchers launchers = {&launch_boundary,         &launch_flux_update,      &launch_recover_react,
                              &launch_derived,          &launch_recover_classify, &launch_learned_features,
                              &launch_learned_apply,    &launch_react_queue,      &launch_react_heavy,
-                             &launch_materialize,      &launch_learned_route};
+                             &launch_materialize,      &launch_learned_route,    &launch_react_queue_batch,
+                             &launch_react_heavy_batch};
 
 #undef EU3D_DISPATCH
 

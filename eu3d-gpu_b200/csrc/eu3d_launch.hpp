@@ -40,6 +40,9 @@ struct Launchers {
     cudaError_t (*react_heavy)(const LaunchArgs &a, int blocks);
     cudaError_t (*materialize)(const LaunchArgs &a);
     cudaError_t (*learned_route)(const LaunchArgs &a, const LearnedParams &lp);
+    // a batch's shared kinetics stage over the instances of tab[0..n)
+    cudaError_t (*react_queue_batch)(const LaunchArgs &a, const BatchCell *tab, int n, int *next, int counter);
+    cudaError_t (*react_heavy_batch)(const LaunchArgs &a, const BatchCell *tab, int n, int *next, int blocks);
 };
 
 #define EU3D_DECLARE_LAUNCHERS(NSP)                                                                \
@@ -61,6 +64,10 @@ struct Launchers {
     cudaError_t launch_chem_samples(const LaunchArgs &a, long long n, double *cs, double *T,       \
                                     double *E, const double *dt, int *nchem);                      \
     cudaError_t launch_react_heavy(const LaunchArgs &a, int blocks);                               \
+    cudaError_t launch_react_queue_batch(const LaunchArgs &a, const BatchCell *tab, int n, int *next, \
+                                         int counter);                                             \
+    cudaError_t launch_react_heavy_batch(const LaunchArgs &a, const BatchCell *tab, int n, int *next, \
+                                         int blocks);                                              \
     cudaError_t launch_materialize(const LaunchArgs &a);                                           \
     cudaError_t launch_to_f32(const double *src, float *dst, long long n, cudaStream_t s);          \
     cudaError_t launch_halo(const LaunchArgs &a, int nf, int face, bool pack, void *msg);           \

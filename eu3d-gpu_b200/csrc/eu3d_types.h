@@ -93,6 +93,17 @@ enum CounterIdx {
     kCntCount = 8
 };
 
+// One instance of a batch in the batch's shared kinetics stage: its state, its
+// dt, and its stiff-fallback queue (learned mode; null otherwise). The
+// deferred cells are st.heavy's (null: none).
+struct BatchCell {
+    DevState st;
+    long long n3;
+    const double *dt;
+    const int *queue; // cell indices
+    const int *count; // queue length (count[0])
+};
+
 // Parameters and buffers of the learned-chemistry step (set by eu_set_learned).
 struct LearnedParams {
     float *feat;           // [queue capacity x (3 + NS)] fp32 model inputs

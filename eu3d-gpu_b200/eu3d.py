@@ -153,7 +153,10 @@ def library():
         lib.eu_batch_destroy.argtypes = [_P]
         lib.eu_batch_last_error.argtypes = [_P]
         lib.eu_batch_last_error.restype = ctypes.c_char_p
-        for fn in ("eu_batch_create", "eu_batch_step", "eu_batch_destroy"):
+        lib.eu_batch_set_shared_kinetics.argtypes = [_P, _I]
+        lib.eu_batch_launches.argtypes = [_P, ctypes.POINTER(_I), ctypes.POINTER(_I)]
+        for fn in ("eu_batch_create", "eu_batch_step", "eu_batch_destroy", "eu_batch_set_shared_kinetics",
+                   "eu_batch_launches"):
             getattr(lib, fn).restype = _I
         lib.eu_set_conserved.argtypes = [_P] * 4
         lib.eu_set_conserved.restype = _I
@@ -502,6 +505,22 @@ class Batch:
         if st:
             raise EU3DError(st, library().eu_batch_last_error(self.h).decode())
         return [s.as_dict() for s in stats], ms.value
+
+    def set_shared_kinetics(self, on):
+        """eu_batch_set_shared_kinetics: the fallback and deferred-cell kinetics
+        of all instances as one shared stage (True, the default) or inside
+        each instance's branch."""
+        st = library().eu_batch_set_shared_kinetics(self.h, int(bool(on)))
+        if st:
+            raise EU3DError(st, "eu_batch_set_shared_kinetics")
+
+    def launches(self):
+        """(kernel launches per step, of which the shared kinetics stage's)."""
+        per, shared = ctypes.c_int(), ctypes.c_int()
+        st = library().eu_batch_launches(self.h, ctypes.byref(per), ctypes.byref(shared))
+        if st:
+            raise EU3DError(st, "eu_batch_launches")
+        return per.value, shared.value
 
     def close(self):
         if getattr(self, "h", None):

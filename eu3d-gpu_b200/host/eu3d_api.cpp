@@ -65,6 +65,8 @@ struct eu_handle {
     int graph_launches = 0;
     bool graph_dirty = true;
     double graph_cfl = 0;   // the CFL number the captured step sets its dt from (0: a fixed dt)
+    bool graph_shared_tail = false; // captured for a batch: the stiff-fallback and deferred-cell
+                                    // kinetics left to the batch's shared stage
     unsigned graph_gen = 0; // captures so far (batches rebuild when it changes)
     // launch shapes picked by eu_autotune (0: defaults)
     int flux_ci = 0, recover_block = 0, recover_minb = 0;
@@ -831,7 +833,7 @@ void element_projector(const MechanismTables &m, double (&P)[kMaxS][kMaxS])
 // fused inference kernel nothing here waits on the host, so the phase can be
 // captured in the step's graph. Otherwise (a model shape without the fused
 // kernel) the queue length is read back to size the layer-wise GEMMs.
-eu_status learned_chemistry(eu_handle *h, const LaunchArgs &a, const Launchers &L, int *launches)
+eu_status learned_chemistry(eu_handle *h, const LaunchArgs &a, const Launchers &L, int *launches, bool fallback)
 {
     LearnedParams lp = h->lp;
     const int ns = h->mech.ns;
@@ -869,15 +871,20 @@ eu_status learned_chemistry(eu_handle *h, const LaunchArgs &a, const Launchers &
         }
     }
     CK(h, L.learned_apply(a, lp));
-    CK(h, L.react_queue(a, lp.fallback, lp.counts + 1, kCntFallback));
-    *launches += 2;
+    ++*launches;
+    if (fallback) {
+        CK(h, L.react_queue(a, lp.fallback, lp.counts + 1, kCntFallback));
+        ++*launches;
+    }
     return EU_OK;
 }
 
 // The launches of one timestep on h->stream (run eagerly or recorded into the
 // step's graph). phase (profile mode) receives per-phase event times.
+// shared_tail: leave the stiff-fallback queue and the deferred cells to a
+// batch's shared kinetics stage (their queues are filled, not drained).
 eu_status step_launches(eu_handle *h, const LaunchArgs &a, const Launchers &L, bool prof, int *launches,
-                        double cfl = 0)
+                        double cfl = 0, bool shared_tail = false)
 {
     const bool react = h->cfg.chemistry == EU_CHEM_STIFF;
     const bool learned = h->cfg.chemistry == EU_CHEM_LEARNED;
@@ -923,14 +930,14 @@ eu_status step_launches(eu_handle *h, const LaunchArgs &a, const Launchers &L, b
     if (heavy)
         CK(h, cudaMemsetAsync(h->st.heavy, 0, 2 * sizeof(int), h->stream));
     if (learned) {
-        eu_status ls = learned_chemistry(h, a, L, launches);
+        eu_status ls = learned_chemistry(h, a, L, launches, !shared_tail);
         if (ls != EU_OK)
             return ls;
     } else {
         CK(h, L.recover_react(a, react));
         ++*launches;
     }
-    if (heavy) { // warp-per-cell kinetics of the cells deferred above
+    if (heavy && !shared_tail) { // warp-per-cell kinetics of the cells deferred above
         CK(h, L.react_heavy(a, h->heavy_blocks));
         ++*launches;
     }
@@ -940,12 +947,13 @@ eu_status step_launches(eu_handle *h, const LaunchArgs &a, const Launchers &L, b
 }
 
 // Records one timestep into h->graph and instantiates it.
-eu_status capture_step(eu_handle *h, const LaunchArgs &a, const Launchers &L, double cfl = 0)
+eu_status capture_step(eu_handle *h, const LaunchArgs &a, const Launchers &L, double cfl = 0,
+                       bool shared_tail = false)
 {
     drop_graph(h);
     int launches = 0;
     CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    eu_status s = step_launches(h, a, L, false, &launches, cfl);
+    eu_status s = step_launches(h, a, L, false, &launches, cfl, shared_tail);
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     if (s != EU_OK) {
@@ -960,6 +968,7 @@ eu_status capture_step(eu_handle *h, const LaunchArgs &a, const Launchers &L, do
     h->graph_launches = launches;
     h->graph_dirty = false;
     h->graph_cfl = cfl;
+    h->graph_shared_tail = shared_tail;
     ++h->graph_gen;
     return EU_OK;
 }
@@ -1188,7 +1197,7 @@ eu_status step_impl(eu_handle *h, int nsteps, double dt, double cfl, eu_step_sta
     if (h->st.prim32 && nsteps > 0)
         h->prim_stale = true;
     int n = 0;
-    if (graphs && nsteps > 0 && (h->graph_dirty || !h->graph_exec || h->graph_cfl != cfl)) {
+    if (graphs && nsteps > 0 && (h->graph_dirty || !h->graph_exec || h->graph_cfl != cfl || h->graph_shared_tail)) {
         // the first step runs eagerly (one-time kernel attribute set-up), then
         // the step is captured
         eu_status s = step_launches(h, a, L, false, &launches, cfl);
@@ -1762,9 +1771,25 @@ eu_status eu_device_info(const eu_handle *h, void **stream, size_t *device_bytes
 // Several handles on one device advanced together: one CUDA graph whose
 // independent branches are the instances' captured timesteps, launched once
 // per step on the batch's own stream, so the kernels of different instances
-// overlap on the GPU. Each instance keeps its own buffers, queues and
+// overlap on the GPU. The kinetics of the cells the instances leave to the
+// stiff integrator after their own recovery (the learned mode's fallback
+// queue, the deferred cells of the warp-per-cell kinetics) form one shared
+// stage after every branch: one fixed grid drains the fallback queues of all
+// instances taken end to end, then one persistent grid their deferred cells,
+// so the reacting cells of all instances spread over the whole GPU whatever
+// instance they sit in. Each instance keeps its own buffers, queues and
 // statistics.
 struct eu_batch {
+    // instances of one flavour, mechanism and substep cap share one launch
+    // per kinetics stage; their table entries are contiguous
+    struct Group {
+        LaunchArgs a;           // the first member's (mechanism, flavour, stream replaced)
+        const Launchers *L;
+        int first = 0, count = 0;
+        bool fallback = false;  // some member has a stiff-fallback queue
+        bool heavy = false;     // some member defers cells
+        int heavy_blocks = 0;
+    };
     std::vector<eu_handle *> hs;
     std::vector<unsigned> gens;
     int device = 0;
@@ -1773,6 +1798,12 @@ struct eu_batch {
     std::vector<cudaEvent_t> joins; // one per instance
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    bool shared = true;              // eu_batch_set_shared_kinetics
+    std::vector<Group> groups;
+    BatchCell *d_tab = nullptr;      // [instances] (members of the groups, in group order)
+    int *d_next = nullptr;           // [2 per group]: fallback and deferred-cell positions taken
+    int shared_launches = 0;         // kernels of the shared stage per step
+    int launches = 0;                // kernels per step, the instances' and the shared stage's
     std::string err;
 };
 
@@ -1805,6 +1836,94 @@ void drop_batch_graph(eu_batch *b)
         cudaGraphDestroy(b->graph);
     b->exec = nullptr;
     b->graph = nullptr;
+    b->groups.clear();
+}
+
+// Whether an instance leaves kinetics to the shared stage.
+bool needs_shared_stage(const eu_handle *h)
+{
+    const bool learned = h->cfg.chemistry == EU_CHEM_LEARNED;
+    return learned || (h->st.heavy && h->cfg.chemistry == EU_CHEM_STIFF);
+}
+
+// The shared kinetics stage: the groups' table on the device, then the
+// stage's launches recorded into `out` (zeroing the positions taken first).
+eu_status build_shared_stage(eu_batch *b, cudaGraph_t *out)
+{
+    *out = nullptr;
+    std::vector<BatchCell> tab;
+    std::vector<int> done(b->hs.size(), 0);
+    for (size_t i = 0; i < b->hs.size(); ++i) {
+        eu_handle *h = b->hs[i];
+        if (done[i] || !needs_shared_stage(h))
+            continue;
+        eu_batch::Group grp;
+        grp.a = launch_args(h);
+        grp.L = &flavour(h);
+        grp.first = int(tab.size());
+        grp.heavy_blocks = h->heavy_blocks;
+        for (size_t j = i; j < b->hs.size(); ++j) {
+            eu_handle *o = b->hs[j];
+            if (done[j] || !needs_shared_stage(o) || &flavour(o) != grp.L || o->spec != h->spec ||
+                launch_args(o).max_substeps != grp.a.max_substeps ||
+                std::memcmp(&o->dmech, &h->dmech, sizeof(DevMech)) != 0)
+                continue;
+            done[j] = 1;
+            BatchCell c{};
+            c.st = o->st;
+            c.n3 = o->g.n3;
+            c.dt = o->d_dt;
+            if (o->cfg.chemistry == EU_CHEM_LEARNED) {
+                c.queue = o->lp.fallback;
+                c.count = o->lp.counts + 1;
+                grp.fallback = true;
+            }
+            if (o->st.heavy)
+                grp.heavy = true;
+            else
+                c.st.heavy = nullptr;
+            tab.push_back(c);
+        }
+        grp.count = int(tab.size()) - grp.first;
+        b->groups.push_back(grp);
+    }
+    b->shared_launches = 0;
+    if (b->groups.empty())
+        return EU_OK;
+    if (b->d_tab)
+        cudaFree(b->d_tab);
+    if (b->d_next)
+        cudaFree(b->d_next);
+    b->d_tab = nullptr;
+    b->d_next = nullptr;
+    BCK(b, cudaMalloc(&b->d_tab, tab.size() * sizeof(BatchCell)));
+    BCK(b, cudaMalloc(&b->d_next, b->groups.size() * 2 * sizeof(int)));
+    BCK(b, cudaMemcpyAsync(b->d_tab, tab.data(), tab.size() * sizeof(BatchCell), cudaMemcpyHostToDevice, b->stream));
+    BCK(b, cudaStreamSynchronize(b->stream));
+    BCK(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaMemsetAsync(b->d_next, 0, b->groups.size() * 2 * sizeof(int), b->stream);
+    for (size_t q = 0; q < b->groups.size() && e == cudaSuccess; ++q) {
+        eu_batch::Group &grp = b->groups[q];
+        grp.a.stream = b->stream;
+        const BatchCell *t = b->d_tab + grp.first;
+        int *next = b->d_next + 2 * q;
+        if (grp.fallback && (e = grp.L->react_queue_batch(grp.a, t, grp.count, next, kCntFallback)) == cudaSuccess)
+            ++b->shared_launches;
+        if (e == cudaSuccess && grp.heavy &&
+            (e = grp.L->react_heavy_batch(grp.a, t, grp.count, next, grp.heavy_blocks)) == cudaSuccess)
+            ++b->shared_launches;
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(b->stream, &g);
+    if (e != cudaSuccess || ee != cudaSuccess) {
+        if (g)
+            cudaGraphDestroy(g);
+        const cudaError_t bad = e != cudaSuccess ? e : ee;
+        cudaGetLastError();
+        return bfail(b, EU_ERR_CUDA, "shared kinetics stage: %s", cudaGetErrorString(bad));
+    }
+    *out = g;
+    return EU_OK;
 }
 
 } // namespace
@@ -1851,6 +1970,8 @@ eu_status eu_batch_destroy(eu_batch *b)
     if (b->stream)
         cudaStreamSynchronize(b->stream);
     drop_batch_graph(b);
+    if (b->d_tab) cudaFree(b->d_tab);
+    if (b->d_next) cudaFree(b->d_next);
     for (cudaEvent_t e : b->joins)
         if (e) cudaEventDestroy(e);
     if (b->ev0) cudaEventDestroy(b->ev0);
@@ -1861,6 +1982,32 @@ eu_status eu_batch_destroy(eu_batch *b)
 }
 
 const char *eu_batch_last_error(const eu_batch *b) { return b ? b->err.c_str() : kNoHandle; }
+
+eu_status eu_batch_set_shared_kinetics(eu_batch *b, int on)
+{
+    if (!b)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (b->shared != (on != 0)) {
+        cudaSetDevice(b->device);
+        cudaStreamSynchronize(b->stream);
+        drop_batch_graph(b);
+        b->shared = on != 0;
+    }
+    return EU_OK;
+}
+
+eu_status eu_batch_launches(const eu_batch *b, int *per_step, int *shared_stage)
+{
+    if (!b)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (!b->exec)
+        return EU_ERR_NOT_READY;
+    if (per_step)
+        *per_step = b->launches;
+    if (shared_stage)
+        *shared_stage = b->shared_launches;
+    return EU_OK;
+}
 
 eu_status eu_batch_step(eu_batch *b, int nsteps, const double *dt, eu_step_stats *stats, double *device_ms)
 {
@@ -1877,8 +2024,9 @@ eu_status eu_batch_step(eu_batch *b, int nsteps, const double *dt, eu_step_stats
             return bfail(b, EU_ERR_NOT_READY, "instance %d: mechanism and state must be set", i);
         if (h->cfg.chemistry == EU_CHEM_LEARNED && (!h->model || !mlp_has_fused(h->model)))
             return bfail(b, EU_ERR_UNSUPPORTED, "instance %d: learned chemistry needs a model with the fused kernel", i);
-        if (h->graph_dirty || !h->graph_exec || h->graph_cfl != 0) {
-            const eu_status s = capture_step(h, launch_args(h), flavour(h));
+        const bool tail = b->shared && needs_shared_stage(h);
+        if (h->graph_dirty || !h->graph_exec || h->graph_cfl != 0 || h->graph_shared_tail != tail) {
+            const eu_status s = capture_step(h, launch_args(h), flavour(h), 0, tail);
             if (s != EU_OK)
                 return bfail(b, s, "instance %d: %s", i, h->err.c_str());
         }
@@ -1887,10 +2035,26 @@ eu_status eu_batch_step(eu_batch *b, int nsteps, const double *dt, eu_step_stats
     if (rebuild) {
         drop_batch_graph(b);
         BCK(b, cudaGraphCreate(&b->graph, 0));
+        std::vector<cudaGraphNode_t> nodes(n);
+        b->launches = 0;
         for (int i = 0; i < n; ++i) {
-            cudaGraphNode_t node;
-            BCK(b, cudaGraphAddChildGraphNode(&node, b->graph, nullptr, 0, b->hs[i]->graph));
+            BCK(b, cudaGraphAddChildGraphNode(&nodes[i], b->graph, nullptr, 0, b->hs[i]->graph));
             b->gens[i] = b->hs[i]->graph_gen;
+            b->launches += b->hs[i]->graph_launches;
+        }
+        b->shared_launches = 0;
+        if (b->shared) {
+            cudaGraph_t stage = nullptr;
+            const eu_status s = build_shared_stage(b, &stage);
+            if (s != EU_OK)
+                return s;
+            if (stage) {
+                cudaGraphNode_t node;
+                const cudaError_t e = cudaGraphAddChildGraphNode(&node, b->graph, nodes.data(), nodes.size(), stage);
+                cudaGraphDestroy(stage); // the node holds its own copy
+                BCK(b, e);
+                b->launches += b->shared_launches;
+            }
         }
         BCK(b, cudaGraphInstantiate(&b->exec, b->graph, 0));
     }

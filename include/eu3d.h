@@ -496,6 +496,18 @@ eu_status eu_batch_create(eu_handle *const *handles, int count, eu_batch **out);
 eu_status eu_batch_step(eu_batch *b, int nsteps, const double *dt, eu_step_stats *stats, double *device_ms);
 const char *eu_batch_last_error(const eu_batch *b);
 eu_status eu_batch_destroy(eu_batch *b);
+/* The kinetics the instances leave to the stiff integrator after their own
+ * recovery (the learned mode's fallback queue, the cells deferred to the
+ * warp-per-cell kinetics) run by default as one shared stage after every
+ * instance's branch: one launch drains the fallback queues of all instances
+ * of one flavour and mechanism taken end to end, one persistent launch their
+ * deferred cells. on = 0 keeps those launches inside each instance's branch
+ * instead. Results are the same either way (every cell's kinetics is
+ * independent of the others). */
+eu_status eu_batch_set_shared_kinetics(eu_batch *b, int on);
+/* Kernel launches per batch step (after the first eu_batch_step): all of
+ * them, and those of the shared kinetics stage. */
+eu_status eu_batch_launches(const eu_batch *b, int *per_step, int *shared_stage);
 
 #ifdef __cplusplus
 }

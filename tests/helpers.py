@@ -36,6 +36,20 @@ def rel_linf(a, ref):
     return np.where(den > 0, num / np.where(den > 0, den, 1), num)
 
 
+def cs_rel_linf(a, ref):
+    """rel_linf over the conserved planes (species densities, then rho*u,
+    rho*v, rho*w, E) with the three momentum planes measured against the
+    largest momentum magnitude: in a flow uniform along z, rho*w is rounding
+    noise (1e-14 against 1e3) whose own relative error says nothing."""
+    e = rel_linf(a, ref)
+    ns = a.shape[0] - 4
+    mom = slice(ns, ns + 3)
+    den = np.abs(ref[mom]).max()
+    if den > 0:
+        e[mom] = np.abs(a[mom] - ref[mom]).reshape(3, -1).max(axis=1) / den
+    return e
+
+
 def n_unequal(a, b):
     """Elements that differ in value (NaN equals NaN; -0 equals +0)."""
     a, b = np.asarray(a), np.asarray(b)

@@ -164,26 +164,32 @@ def test_graph_replay_equals_eager_launches(gpu, chemistry, precision):
         assert n_unequal(a, b) == 0
 
 
-def test_batch_of_uneven_instances_equals_one_by_one(gpu):
-    """A batch of instances of different sizes and modes (stiff FP64, learned +
-    mixed, frozen) advanced by one graph launch per step gives each instance
-    bitwise the state and statistics it reaches stepping alone, and the
-    handles stay usable on their own between batch calls."""
+@pytest.mark.parametrize("shared", [True, False])
+def test_batch_of_uneven_instances_equals_one_by_one(gpu, shared):
+    """A batch of instances of different sizes and modes (stiff FP64, stiff
+    mixed, learned + mixed with and without the Nchem routing, frozen)
+    advanced by one graph launch per step gives each instance bitwise the
+    state and statistics it reaches stepping alone, with the fallback and
+    deferred-cell kinetics of all instances as one shared stage (one launch
+    per kinetics stage for the instances of one flavour) or inside each
+    instance's branch; the handles stay usable on their own between batch
+    calls."""
     import learned
     model, gate = learned.load()
     mech = gpu.parse_mechanism(cases.MECH_JA919, cases.THERMO)
-    specs = [((24, 8, 8), "stiff", "fp64", 2e-8), ((16, 12, 8), "learned", "mixed", 3e-8),
-             ((20, 6, 10), "frozen", "mixed", 2e-8), ((8, 8, 8), "learned", "fp64", 1e-8)]
+    specs = [((24, 8, 8), "stiff", "fp64", 2e-8, 0), ((16, 12, 8), "learned", "mixed", 3e-8, 0),
+             ((20, 6, 10), "frozen", "mixed", 2e-8, 0), ((8, 8, 8), "learned", "fp64", 1e-8, 0),
+             ((20, 10, 8), "stiff", "mixed", 3e-8, 0), ((12, 12, 12), "learned", "mixed", 3e-8, None)]
 
     def make():
         out = []
-        for (ni, nj, nk), chem, prec, _ in specs:
+        for (ni, nj, nk), chem, prec, _, min_nchem in specs:
             s = gpu.Solver(ni, nj, nk, (0.0, ni * 1e-3, 0.0, nj * 1e-3, 0.0, nk * 1e-3), chemistry=chem,
                            precision=prec, arith="fast")
             s.set_mechanism(mech)
             s.set_primitive(*cases.hot_reacting_block(ni + 4, nj + 4, nk + 4, mech["mw"], mech["ns"]))
-            if chem == "learned":  # every active cell to the model
-                learned.attach(s, model, dict(gate, min_nchem=0))
+            if chem == "learned":  # min_nchem 0: every active cell to the model; None: routed
+                learned.attach(s, model, gate if min_nchem is None else dict(gate, min_nchem=min_nchem))
             out.append(s)
         return out
 
@@ -193,11 +199,20 @@ def test_batch_of_uneven_instances_equals_one_by_one(gpu):
         s.step(1, spec[3])
     together = make()
     b = gpu.Batch(together)
+    b.set_shared_kinetics(shared)
     stats, ms = b.step(3, [spec[3] for spec in specs])
     assert ms > 0
+    per_step, stage = b.launches()
+    # shared: the two learned mixed instances drain their fallback queues in
+    # one launch and, with the stiff mixed one, their deferred cells in
+    # another; the learned FP64 instance (another flavour, no deferral) has
+    # its own fallback launch
+    assert stage == (3 if shared else 0), stage
+    assert per_step > stage
     for s, spec in zip(together, specs):  # on their own between batch calls
         s.step(1, spec[3])
     keep = ("max_nchem", "sum_nchem", "learned", "fallback")
+    assert sum(st["fallback"] for st in ref_stats) > 0
     for got, want in zip(stats, ref_stats):
         assert {k: got[k] for k in keep} == {k: want[k] for k in keep}
     for a, c in zip(alone, together):

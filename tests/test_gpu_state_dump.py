@@ -123,8 +123,16 @@ def reference_tecplot(x, y, z, fields):
              "datapacking=block"]
     X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
     for a in [X, Y, Z] + fields:
-        lines += ["%g" % v for v in np.transpose(a, (2, 1, 0)).ravel()]
+        lines += [format_g(v) for v in np.transpose(a, (2, 1, 0)).ravel()]
     return lines
+
+
+def format_g(v):
+    """One double as C's printf("%g") writes it on Linux: a NaN keeps its sign
+    ("-nan" for the sign bit set), which Python's own %g drops."""
+    if np.isnan(v):
+        return "-nan" if np.signbit(v) else "nan"
+    return "%g" % v
 
 
 def test_tecplot_output_matches_the_reference_writer(gpu, port_lib):
@@ -153,7 +161,10 @@ def test_tecplot_output_matches_the_reference_writer(gpu, port_lib):
     g = np.array([float(v) for v in got[3:-1]]).reshape(16, -1)
     w = np.array([float(v) for v in want[3:]]).reshape(16, -1)
     assert np.array_equal(g[:3], w[:3])  # node coordinates
-    assert (np.abs(g - w) <= 1.2e-5 * np.abs(w)).all()
+    # corner halo nodes that no boundary pass fills hold 0/0 in both codes
+    assert np.array_equal(np.isnan(g), np.isnan(w))
+    ok = np.isnan(w) | (np.abs(g - w) <= 1.2e-5 * np.abs(w))
+    assert ok.all()
     assert (np.array(got[3:-1]) == np.array(want[3:])).mean() > 0.999
 
 
