@@ -822,28 +822,30 @@ def our_arm_blocks(args, world, rank, local, dist):
     per_kernel = {n: round(phase[q], 4) for q, n in enumerate(names)}
     roofline = flux_roofline(phase, 1, ncell, args.precision)
 
-    # end to end through the public API with host buffers (state up once, the
-    # exchanged steps each synchronous, the conserved state down at the end)
+    # end to end through the public API with host buffers: the configured run
+    # (each block's initial state up once, the exchanged steps each synchronous,
+    # the conserved state down at the end)
     pinned = {}
     for k in ("CS", "T", "E"):
-        src = window_state[k] if k == "CS" else window_state[k][None]
+        src = sd[k] if k == "CS" else sd[k][None]
         t = torch.empty(src.shape, dtype=torch.float64, pin_memory=True)
         t.numpy()[...] = src
         pinned[k] = t.numpy()
-    cs_host = torch.empty(window_state["CS"].shape, dtype=torch.float64, pin_memory=True).numpy()
+    cs_host = torch.empty(sd["CS"].shape, dtype=torch.float64, pin_memory=True).numpy()
     se = make(args.chem, args.precision, args.arith, state=window_state)
     se.step(args.warmup, dt, stats=False)
     se.sync()
+    e2e_steps = max(getattr(args, "total_steps", TOTAL_STEPS), start + args.warmup + args.steps)
     barrier(dist, device)
     t0 = time.perf_counter()
     se.set_conserved(pinned["CS"], pinned["T"], pinned["E"])
-    for _ in range(args.steps):
+    for _ in range(e2e_steps):
         se.step(1, dt, stats=True)
     cs_out = se.get("CS", out=cs_host)
     e2e_s = reduce_max(dist, time.perf_counter() - t0, device)
-    e2e_value = ncell * args.steps * world / e2e_s / 1e6
-    h2d = sum(v.nbytes for v in pinned.values()) / args.steps + 8
-    d2h = cs_out.nbytes / args.steps + 96
+    e2e_value = ncell * e2e_steps * world / e2e_s / 1e6
+    h2d = sum(v.nbytes for v in pinned.values()) / e2e_steps + 8
+    d2h = cs_out.nbytes / e2e_steps + 96
     se.close()
 
     if rank == 0:
@@ -867,7 +869,7 @@ def our_arm_blocks(args, world, rank, local, dist):
                 "learned_cells": stats["learned"], "fallback_cells": stats["fallback"],
                 "clocks": clocks,
                 "e2e": {"value": round(e2e_value, 3), "unit": "Mcell-steps/s",
-                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
                 # the step's kernels plus one halo pack and unpack per neighbour face
                 "gpu_launches": (stats["launches"] + 2 * faces) * args.steps,
                 "cpu_baseline": None}
@@ -1018,31 +1020,34 @@ def our_arm(args):
     sp.close()
     roofline = flux_roofline(phase, args.steps, ncell, args.precision)
 
-    # -- end to end through the public API with host buffers, on the window state -------------
-    # the conserved state (CS, T, E) is what a step needs; eu_set_conserved forms
-    # the primitives on the device as the step's recovery does
+    # -- end to end through the public API with host buffers: the configured run --------------
+    # the whole run a user makes: the initial conserved state (CS, T, E) from
+    # pinned host memory (eu_set_conserved forms the primitives on the device as
+    # the step's recovery does), run_end steps each reading its health counters
+    # back to the host, the final conserved state read back
     pinned = {}
     for k in ("CS", "T", "E"):
-        src = window_state[k] if k == "CS" else window_state[k][None]
+        src = sd[k] if k == "CS" else sd[k][None]
         t = torch.empty(src.shape, dtype=torch.float64, pin_memory=True)
         t.numpy()[...] = src
         pinned[k] = t.numpy()
-    cs_host = torch.empty(window_state["CS"].shape, dtype=torch.float64, pin_memory=True).numpy()
+    cs_host = torch.empty(sd["CS"].shape, dtype=torch.float64, pin_memory=True).numpy()
     se = make_solver(args.chem, args.precision, args.arith, state=window_state)
-    se.step(args.warmup, dt)
+    se.step(args.warmup, dt)  # first capture and attribute set-up, then the run from the initial state
+    e2e_steps = max(run_end, args.steps)
     barrier(dist, device)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     se.set_conserved(pinned["CS"], pinned["T"], pinned["E"])
-    for _ in range(args.steps):
+    for _ in range(e2e_steps):
         se.step(1, dt)  # synchronous: reads the step's health counters back
     cs = se.get("CS", out=cs_host)
     torch.cuda.synchronize()
     e2e_s = reduce_max(dist, time.perf_counter() - t0, device)
-    e2e_value = ncell * args.steps * world / e2e_s / 1e6
+    e2e_value = ncell * e2e_steps * world / e2e_s / 1e6
     state_bytes = sum(v.nbytes for v in pinned.values())
-    h2d = state_bytes / args.steps + 8
-    d2h = cs.nbytes / args.steps + 96
+    h2d = state_bytes / e2e_steps + 8
+    d2h = cs.nbytes / e2e_steps + 96
     se.close()
 
     cpu = None
@@ -1084,7 +1089,12 @@ def our_arm(args):
                 "nchem_histogram_window_end": nchem_histogram(end_fast["Nchem"]),
                 "clocks": clocks,
                 "e2e": {"value": round(e2e_value, 3), "unit": "Mcell-steps/s",
-                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                        "steps": e2e_steps,
+                        "what": "the configured run through the C-ABI from host buffers: the initial conserved "
+                                "state uploaded from pinned memory, every step synchronous with its health "
+                                "counters read back, the final conserved state downloaded; bytes per step "
+                                "are the run's copies over its steps"},
                 "gpu_launches": stats["launches"],
                 "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)

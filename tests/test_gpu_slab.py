@@ -332,7 +332,7 @@ def _bench_rank(rank, ranks, port, out):
     torch.cuda.set_device(0)
     dist.init_process_group("gloo", rank=rank, world_size=ranks, timeout=timedelta(seconds=300))
     args = argparse.Namespace(grid=[33, 17, 17], chem="learned", precision="mixed", arith="fast", steps=2, warmup=3,
-                              no_autotune=False, window_start=5)
+                              no_autotune=False, window_start=5, total_steps=12)
     buf = io.StringIO()
     with contextlib.redirect_stdout(buf):
         rc = bench.our_arm_blocks(args, ranks, rank, 0, dist)
