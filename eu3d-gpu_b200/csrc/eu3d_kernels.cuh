@@ -1310,6 +1310,28 @@ __device__ __forceinline__ void copy_mech_to_shared(const DevMech &m, DevMech &m
     for (int w = threadIdx.x; w < int(sizeof(DevMech) / sizeof(int)); w += blockDim.x) dst[w] = src[w];
 }
 
+// The order in which the warps of a persistent grid take deferred cells:
+// position p of n is entry p * s mod n, s near 0.618 n and coprime with n (a
+// bijection of [0, n)). The queue holds the cells in about the order the
+// recovery met them, so neighbouring cells, whose stiffness is alike, sit
+// next to each other; the warps that start together belong to few blocks,
+// and without the scatter the stiffest cells would share a few SMs.
+__device__ __forceinline__ long long scatter_stride(long long n)
+{
+    long long s = static_cast<long long>(0.6180339887498949 * double(n)) | 1;
+    for (;;) {
+        long long a = s, b = n;
+        while (b != 0) {
+            const long long t = a % b;
+            a = b;
+            b = t;
+        }
+        if (a == 1)
+            return s;
+        s += 2;
+    }
+}
+
 template <int NS, int NR>
 __global__ void __launch_bounds__(128, 4) k_react_heavy(const __grid_constant__ DevMech m, const DevGrid g,
                                                      const DevState st, const double *__restrict__ dt_dev,
@@ -1323,6 +1345,7 @@ __global__ void __launch_bounds__(128, 4) k_react_heavy(const __grid_constant__ 
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const double dtm = *dt_dev;
+    const long long stride = scatter_stride(count);
     for (;;) {
         int q = 0;
         if (lane == 0)
@@ -1330,7 +1353,8 @@ __global__ void __launch_bounds__(128, 4) k_react_heavy(const __grid_constant__ 
         q = __shfl_sync(0xffffffffu, q, 0);
         if (q >= count)
             break;
-        react_heavy_cell<NS, NR>(m, ms, st, g.n3, st.heavy[2 + q], dtm, max_substeps, lane);
+        const int e = int((q * stride) % count);
+        react_heavy_cell<NS, NR>(m, ms, st, g.n3, st.heavy[2 + e], dtm, max_substeps, lane);
     }
 }
 
@@ -1350,6 +1374,7 @@ __global__ void __launch_bounds__(128, 4) k_react_heavy_batch(const __grid_const
     copy_mech_to_shared(m, ms);
     __syncthreads();
     const int lane = threadIdx.x & 31;
+    const long long stride = scatter_stride(total);
     for (;;) {
         int pos = 0;
         if (lane == 0)
@@ -1358,7 +1383,7 @@ __global__ void __launch_bounds__(128, 4) k_react_heavy_batch(const __grid_const
         if (pos >= total)
             break;
         int local = 0;
-        const int q = batch_locate(n, pos, len, local);
+        const int q = batch_locate(n, int((pos * stride) % total), len, local);
         if (q < n) {
             const BatchCell &b = tab[q];
             react_heavy_cell<NS, NR>(m, ms, b.st, b.n3, b.st.heavy[2 + local], *b.dt, max_substeps, lane);

@@ -15,8 +15,11 @@ and each step draws dt ~ logU[1e-9, 3e-7] s. All tensors stay on the GPU
 """
 from __future__ import annotations
 
+import ast
+import json
 import math
 import os
+import re
 
 import numpy as np
 
@@ -263,7 +266,17 @@ def save(path, model, scaling, gate, meta=None):
              **scaling, tau=gate["tau"], box_lo=gate["box_lo"], box_hi=gate["box_hi"], out_eps=gate["out_eps"],
              out_bound=gate["out_bound"],
              frozen=np.array([FROZEN_Y, FROZEN_T, FROZEN_RADICAL]), min_nchem=np.array(gate.get("min_nchem", 0)),
-             meta=np.array(repr(meta or {})))
+             meta=np.array(json.dumps(meta or {})))
+
+
+def load_meta(z):
+    """The training record of a checkpoint (JSON; older ones hold a Python
+    literal)."""
+    text = str(z["meta"])
+    try:
+        return dict(json.loads(text))
+    except ValueError:  # a Python repr: inf and nan are bare names there
+        return dict(ast.literal_eval(re.sub(r"\bnan\b", "None", re.sub(r"\binf\b", "1e999", text))))
 
 
 def load(path=CHECKPOINT, device=0):

@@ -22,7 +22,6 @@ Seeded; the whole run takes about ten minutes on a B200 (six of them training).
 from __future__ import annotations
 
 import argparse
-import ast
 import json
 import os
 import sys
@@ -78,7 +77,11 @@ def main():
         print(f"{Xf.shape[0]} rows from {init[0].size} front states", flush=True)
         X, T, N = torch.cat([X, Xf]), torch.cat([T, Tf]), torch.cat([N, Nf])
     s.close()
-    act = learned.active_rows(X) & (N > args.rows_min_nchem)
+    # rows whose inputs or changes are not finite (a state the stiff kinetics
+    # could not advance) would turn the scaling and every loss into NaN
+    finite = torch.isfinite(X).all(1) & torch.isfinite(T).all(1) & torch.isfinite(learned.to_model_space(T)).all(1)
+    print(f"{int((~finite).sum())} rows with non-finite inputs or changes dropped", flush=True)
+    act = learned.active_rows(X) & (N > args.rows_min_nchem) & finite
     X, T = X[act].contiguous(), T[act].contiguous()
     n = X.shape[0]
     g = torch.Generator(device="cuda")
@@ -126,7 +129,7 @@ def calibrate_only(args):
     scaling = {k: z[k] for k in ("in_shift", "in_scale", "out_shift", "out_scale")}
     bound = old["out_bound"]
     gate = learned.calibrate(model, scaling, X, T, target=args.target, eps=old["out_eps"], bound=bound)
-    meta = dict(ast.literal_eval(str(z["meta"])))
+    meta = learned.load_meta(z)
     meta.update(calibrated_on=int(learned.active_rows(X).sum()), target=args.target, tau=gate["tau"],
                 accepted_fraction=gate["accepted_fraction"], l1_accepted=gate["l1_accepted"])
     learned.save(args.out, model, scaling, gate, meta)
@@ -144,7 +147,7 @@ def front_only(args):
     z = np.load(args.out)
     scaling = {k: z[k] for k in ("in_shift", "in_scale", "out_shift", "out_scale")}
     tight, shift = learned.tighten_for_front(model, gate, max_shift=args.max_shift, log=lambda m: print(m, flush=True))
-    meta = dict(ast.literal_eval(str(z["meta"])))
+    meta = learned.load_meta(z)
     meta.update(tau=tight["tau"], tau_per_step_l1=gate["tau"], front_shift_validation=shift)
     learned.save(args.out, model, scaling, tight, meta)
     print(json.dumps(meta), flush=True)

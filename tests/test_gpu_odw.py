@@ -136,11 +136,15 @@ def test_odw_wedge_tip_inside_the_domain(gpu, port_lib):
     s.step(25, 1e-8)
     assert cs_rel_linf(interior(s.get("CS")), interior(port.get("CS"))).max() <= 1e-10
     assert n_unequal(interior(s.get("Nchem")), interior(port.get("Nchem"))) == 0
-    port.boundary()
-    s.step(0, 1e-8)
-    for f in ["P", "U", "V", "T", "Yi"]:
-        g, r = s.get(f)[:, 2:-2, 0:2, 2:-2], port.get(f)[:, 2:-2, 0:2, 2:-2]
-        assert rel_linf(g, r).max() <= 1e-10, f
+    # the y-low ghosts of the primitives the flux reads, as both codes' last
+    # fill left them (from the state at the start of the last step)
+    ylow = (slice(None), slice(2, -2), slice(0, 2), slice(2, -2))
+    speed = np.abs(port.get("U")[ylow]).max()
+    for f in ["P", "D", "U", "V", "W", "H", "Gamma", "Yi"]:
+        g, r = s.get(f)[ylow], port.get(f)[ylow]
+        # W is rounding noise in this z-uniform flow: measured against the speed
+        err = np.abs(g - r).max() / speed if f == "W" else rel_linf(g, r).max()
+        assert err <= 1e-10, (f, err)
     p = interior(s.get("P"))[0]
     p0 = 101325.0
     assert np.abs(p[: wall - 4, :3] / p0 - 1).max() < 1e-6  # the freestream ahead of the tip
