@@ -84,6 +84,23 @@ __device__ __forceinline__ TPow make_tpow(double T, bool need_log)
     return p;
 }
 
+// The powers of T with 1/T and log T already known (a caller that carries
+// them from the temperature Newton).
+__device__ __forceinline__ TPow make_tpow_known(double T, double inv, double lnT)
+{
+    TPow p;
+    p.T = T;
+    p.low = T < kThermoSwitch;
+    p.inv = inv;
+    p.inv2 = inv * inv;
+    p.t2 = T * T;
+    p.t3 = p.t2 * T;
+    p.t4 = p.t3 * T;
+    p.t5 = p.t4 * T;
+    p.lnT = lnT;
+    return p;
+}
+
 // Coefficient k of species s in the range of p. kRange 1 / 2: the low / high
 // range fixed at compile time, so the value is an operand of the kernel's
 // constant bank; 0: chosen per thread, a load whose address differs between
@@ -308,6 +325,74 @@ __device__ __forceinline__ double newton_temperature(const DevMech &m, double T,
     ThermoCache<NS> tc;
     return newton_temperature<NS>(m, T, E, Y, tc);
 }
+
+// log(1 + x) for |x| <= 2^-6 by its series to x^9 (truncation below 2^-57 |x|):
+// the change of log T between Newton iterates without a logarithm.
+__device__ __forceinline__ double log1p_small(double x)
+{
+    double s = 1.0 / 9.0;
+    s = fma(s, x, -1.0 / 8.0);
+    s = fma(s, x, 1.0 / 7.0);
+    s = fma(s, x, -1.0 / 6.0);
+    s = fma(s, x, 1.0 / 5.0);
+    s = fma(s, x, -1.0 / 4.0);
+    s = fma(s, x, 1.0 / 3.0);
+    s = fma(s, x, -1.0 / 2.0);
+    s = fma(s, x, 1.0);
+    return s * x;
+}
+
+// log T1 from log T0 and x = (T1 - T0) / T0.
+__device__ __forceinline__ double advance_log(double ln0, double x, double T1)
+{
+    return fabs(x) <= 0x1p-6 ? ln0 + log1p_small(x) : log(T1);
+}
+
+// The Newton above for a caller that carries 1/T and log T from one solve to
+// the next (the warp-per-cell kinetics: every substep's rates and rebuild
+// start from the last rebuild's temperature). On entry inv and lnT are those
+// of T; each iterate's log comes from the previous one's (advance_log), not
+// from a logarithm; on return they are those of the result. Same iterates as
+// the Newton above to within rounding.
+template <int NS>
+__device__ __forceinline__ double newton_temperature_carry(const DevMech &m, double T, double E, const double (&Y)[NS],
+                                                           ThermoCache<NS> &tc, double &inv, double &lnT)
+{
+    double rsum = 0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) rsum += Y[s] * m.ri[s];
+    const double e_scaled = E * 1e-3;
+    bool &low = tc.low;
+    MixPoly<NS> &c = tc.c;
+    low = T < kThermoSwitch;
+    mix_poly<NS>(m, Y, low, c);
+    double T0 = T, inv0 = inv, ln0 = lnT, T_temp = T;
+    for (int count = 0; count < 10; ++count) {
+        if (count > 0) {
+            const double x = (T_temp - T0) * inv0;
+            ln0 = advance_log(ln0, x, T_temp);
+            T0 = T_temp;
+            inv0 = rcp_nr(T0);
+        }
+        const bool l = T0 < kThermoSwitch;
+        if (l != low) {
+            low = l;
+            mix_poly<NS>(m, Y, low, c);
+        }
+        const double h = fma(T0, fma(T0, fma(T0, fma(T0, fma(T0, c.h6, c.h5), c.h4), c.h3), c.a2), c.a7) -
+                         c.a0 * inv0 + c.a1 * ln0;
+        const double cp = fma(T0, fma(T0, fma(T0, fma(T0, c.a6, c.a5), c.a4), c.a3), c.a2) +
+                          inv0 * fma(c.a0, inv0, c.a1);
+        const double temp1 = (h - e_scaled) - rsum * T0;
+        const double temp2 = cp - rsum;
+        T_temp = T0 - div_fast(temp1, temp2);
+        if (fabs(T_temp - T0) < 1e-6)
+            break;
+    }
+    lnT = advance_log(ln0, (T_temp - T0) * inv0, T_temp);
+    inv = rcp_nr(T_temp);
+    return T_temp;
+}
 #endif
 
 // Per-cell flow state kept in registers by the recovery / kinetics kernel.
@@ -356,6 +441,27 @@ __device__ __forceinline__ void recover_state(const DevMech &m, CellState<NS> &c
     ThermoCache<NS> tcache;
     recover_state<NS>(m, c, tcache);
 }
+
+#ifndef EU_EXACT_CHEM
+// recover_state with 1/T and log T carried (newton_temperature_carry).
+template <int NS>
+__device__ __forceinline__ void recover_state_carry(const DevMech &m, CellState<NS> &c, double &inv, double &lnT)
+{
+    double D = 0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) D += c.cs[s];
+    const double invD = rcp_nr(D);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) c.Y[s] = c.cs[s] * invD;
+    c.D = D;
+    ThermoCache<NS> tcache;
+    c.T = newton_temperature_carry<NS>(m, c.T, c.E, c.Y, tcache, inv, lnT);
+    c.U = c.cs[NS + 0] * invD;
+    c.V = c.cs[NS + 1] * invD;
+    c.W = c.cs[NS + 2] * invD;
+    c.E = (c.cs[NS + 3] - 0.5 * D * (c.U * c.U + c.V * c.V + c.W * c.W)) * invD;
+}
+#endif
 
 // P, H, Gamma of Update_after_CS (src/Flowfield.cpp:1606-1614). tcache: the
 // recovery's thermo sums for this state, or null.

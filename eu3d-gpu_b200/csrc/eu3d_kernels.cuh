@@ -1188,18 +1188,19 @@ __device__ __forceinline__ double lane_pick(const double (&v)[NS], int lane)
 // lane s < NS holds P_s, Q_s and W_s (W with the molecular weight applied).
 // Every lane runs every loop (lanes past NR evaluate reaction 0 and drop it)
 // so the shuffles stay convergent.
+// inv, lnT: 1/T and log T (carried from the last rebuild's Newton).
 template <int NS, int NR>
-__device__ __forceinline__ void warp_rates(const DevMech &ms, double T, const double (&mc)[NS], int lane, double &Pl,
-                                           double &Ql, double &Wl)
+__device__ __forceinline__ void warp_rates(const DevMech &ms, double T, double inv, double lnT, const double (&mc)[NS],
+                                           int lane, double &Pl, double &Ql, double &Wl)
 {
     static_assert(NR <= 32 && NS <= 32, "one lane per reaction and per species");
-    const TPow p = make_tpow(T, true);
-    const double invRT = 1.0 / (kRUniv * T);
+    const TPow p = make_tpow_known(T, inv, lnT);
+    const double invRT = inv * (1.0 / kRUniv);
     const int sl = lane < NS ? lane : 0;
     const double egl = exp((h_species<NS>(ms, p, kRUniv, sl) - s_species<NS>(ms, p, kRUniv, sl) * T) * invRT);
     const double iegl = rcp_nr(egl);
     const int r = lane < NR ? lane : 0;
-    const double invRuT = 1.0 / (kRuCal * T);
+    const double invRuT = inv * (1.0 / kRuCal);
     const double rt_p0 = (kRUniv * T) / (kP0 * 1e-6);
     const double p0_rt = rcp_nr(rt_p0);
     double rrf = 1.0, rrb = 1.0, kc_inv = 1.0, rtb = 0.0;
@@ -1253,9 +1254,12 @@ __device__ __forceinline__ void react_heavy_cell(const DevMech &m, const DevMech
 {
     CellState<NS> cell;
     load_recovered<NS>(st, n3, c, cell);
+    // 1/T and log T of the current temperature, carried through the substeps
+    // by the rebuild's Newton
+    double inv = rcp_nr(cell.T), lnT = log(cell.T);
     double mc[NS], P, Q, W;
     scaled_concentrations<NS>(m, cell, mc);
-    warp_rates<NS, NR>(ms, cell.T, mc, lane, P, Q, W);
+    warp_rates<NS, NR>(ms, cell.T, inv, lnT, mc, lane, P, Q, W);
     // prediction: min over the species lanes, then every lane has Nchem
     double dt = dtm;
     if (lane < NS && lane_pick<NS>(cell.Y, lane) >= 1e-6 && W != 0)
@@ -1272,7 +1276,7 @@ __device__ __forceinline__ void react_heavy_cell(const DevMech &m, const DevMech
     for (int step = 0; step < nchem; ++step) {
         if (step > 0) {
             scaled_concentrations<NS>(m, cell, mc);
-            warp_rates<NS, NR>(ms, cell.T, mc, lane, P, Q, W);
+            warp_rates<NS, NR>(ms, cell.T, inv, lnT, mc, lane, P, Q, W);
         }
         if (st.cms && lane < NS)
             st.cms[lane * n3 + c] = W * 1e3;
@@ -1281,8 +1285,14 @@ __device__ __forceinline__ void react_heavy_cell(const DevMech &m, const DevMech
             const double di = lane_pick<NS + 4>(cell.cs, lane) * 1e-3;
             const double mcl = lane_pick<NS>(mc, lane);
             const double qv = ms.mw[lane] * Q;
+#ifdef EU_EXACT_CHEM
             const double pv = (mcl == 0) ? 0.0 : P / mcl;
             nd = ((1.0 - half * pv) * di + dts * qv) / (1.0 + half * pv) * 1e3;
+#else
+            // refined reciprocals instead of IEEE divisions (1 + half pv >= 1)
+            const double pv = (mcl == 0) ? 0.0 : P * rcp_nr(mcl);
+            nd = ((1.0 - half * pv) * di + dts * qv) * rcp_nr(1.0 + half * pv) * 1e3;
+#endif
         }
         double D = 0.0;
 #pragma unroll
@@ -1294,7 +1304,13 @@ __device__ __forceinline__ void react_heavy_cell(const DevMech &m, const DevMech
         cell.cs[NS + 1] = cell.V * D;
         cell.cs[NS + 2] = cell.W * D;
         cell.cs[NS + 3] = D * cell.E + 0.5 * (cell.U * cell.U + cell.V * cell.V + cell.W * cell.W) * D;
+#ifdef EU_EXACT_CHEM
         recover_state<NS>(m, cell);
+        inv = 1.0 / cell.T;
+        lnT = log(cell.T);
+#else
+        recover_state_carry<NS>(m, cell, inv, lnT);
+#endif
     }
     if (lane == 0) {
         st.nchem[c] = nchem;
@@ -1333,7 +1349,7 @@ __device__ __forceinline__ long long scatter_stride(long long n)
 }
 
 template <int NS, int NR>
-__global__ void __launch_bounds__(128, 4) k_react_heavy(const __grid_constant__ DevMech m, const DevGrid g,
+__global__ void __launch_bounds__(128, 3) k_react_heavy(const __grid_constant__ DevMech m, const DevGrid g,
                                                      const DevState st, const double *__restrict__ dt_dev,
                                                      int max_substeps)
 {
@@ -1361,7 +1377,7 @@ __global__ void __launch_bounds__(128, 4) k_react_heavy(const __grid_constant__ 
 // The deferred cells of every instance of a batch, their heavy queues taken
 // end to end, drained by one persistent grid (one warp per cell, one counter).
 template <int NS, int NR>
-__global__ void __launch_bounds__(128, 4) k_react_heavy_batch(const __grid_constant__ DevMech m,
+__global__ void __launch_bounds__(128, 3) k_react_heavy_batch(const __grid_constant__ DevMech m,
                                                            const BatchCell *__restrict__ tab, int n, int *next,
                                                            int max_substeps)
 {

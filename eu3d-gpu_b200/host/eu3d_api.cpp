@@ -459,7 +459,7 @@ eu_status eu_create(const eu_config *cfg, eu_handle **out)
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg->device) != cudaSuccess || sms < 1)
         sms = 1;
-    h->heavy_blocks = 4 * sms; // 4 blocks of 4 warps per SM, each warp a cell at a time
+    h->heavy_blocks = 3 * sms; // 3 blocks of 4 warps per SM (its register target), each warp a cell at a time
     h->sms = sms;
     eu_status s;
     if ((s = dalloc(h, &h->d_xyz, size_t(h->nx + h->ny + h->nz))) != EU_OK ||
