@@ -1184,73 +1184,147 @@ __device__ __forceinline__ double lane_pick(const double (&v)[NS], int lane)
     return r;
 }
 
-// Fast-form rates (the mixed flavour's eval_rates) across a warp. On return
-// lane s < NS holds P_s, Q_s and W_s (W with the molecular weight applied).
-// Every lane runs every loop (lanes past NR evaluate reaction 0 and drop it)
-// so the shuffles stay convergent.
-// inv, lnT: 1/T and log T (carried from the last rebuild's Newton).
+// Per-lane constants of the warp-per-cell kinetics, read once per warp from
+// the mechanism tables: lane r's reaction (r < NR; others repeat reaction 0)
+// and lane s's species (s < NS; others repeat species 0).
 template <int NS, int NR>
-__device__ __forceinline__ void warp_rates(const DevMech &ms, double T, double inv, double lnT, const double (&mc)[NS],
-                                           int lane, double &Pl, double &Ql, double &Wl)
+struct HeavyLane {
+    double af, bf, eaf, xr, mw;
+};
+
+template <int NS, int NR>
+__device__ __forceinline__ HeavyLane<NS, NR> heavy_lane(const DevMech &m, int lane)
 {
     static_assert(NR <= 32 && NS <= 32, "one lane per reaction and per species");
+    HeavyLane<NS, NR> h;
+    const int r = lane < NR ? lane : 0, sl = lane < NS ? lane : 0;
+    h.af = m.af[r];
+    h.bf = m.bf[r];
+    h.eaf = m.eaf[r];
+    h.xr = m.xr[r];
+    h.mw = m.mw[sl];
+    return h;
+}
+
+// The mechanism's sparse structure for the warp-per-cell kinetics, built once
+// per block, every array [entry][lane] so that a warp reads 32 consecutive
+// elements. Lane r's reaction (lanes past NR repeat reaction 0) lists the
+// species it involves, ascending: rent = s | nu' << 4 | nu'' << 6, then
+// entries with nu' = nu'' = 0 (factors of exactly 1). Lane s's species (lanes
+// past NS repeat species 0) lists the reactions it takes part in, ascending:
+// sent = q with its coefficients as doubles in sbv, sfv, then entries of
+// reaction slot 31, whose rates are zero (addends of exactly 0). So the
+// loops run a fixed count without branches and the products and sums are
+// the per-thread form's, whose other terms are factors of 1 and addends of
+// 0. tb: third-body efficiencies [s][r]; imw: 1e-3 / W_s.
+template <int NS, int NR>
+struct HeavyTablesT {
+    static_assert(NR < 32, "slot 31 holds zero rates");
+    double tb[NS][32];
+    double sbv[NR][32], sfv[NR][32];
+    double imw[NS];
+    unsigned char rent[NS][32], sent[NR][32];
+};
+
+// A warp's exchange buffers in shared memory: the species' exp(g) and
+// exp(-g), the reactions' forward and backward rates and third-body sums.
+struct HeavyScratch {
+    double eg[32], ieg[32], fwd[32], bwd[32], rtb[32], mc[32];
+};
+
+// Fast-form rates (the mixed flavour's eval_rates) across a warp. On return
+// lane s < NS holds P_s, Q_s and W_s (W with the molecular weight applied).
+// The species' Gibbs exponentials and the reactions' rates change hands
+// through the warp's shared buffers (one store each, broadcast loads); a
+// reaction lane reads its coefficients from the transposed tables (tt), a
+// species lane from the mechanism's (ms): the arithmetic and its order are
+// the per-thread form's. inv, lnT: 1/T and log T (carried from the last
+// rebuild's Newton).
+template <int NS, int NR>
+__device__ __forceinline__ void warp_rates(const DevMech &ms, const HeavyLane<NS, NR> &hl,
+                                           const HeavyTablesT<NS, NR> &tt, HeavyScratch &x, double T, double inv,
+                                           double lnT, const double (&mc)[NS], int lane, double &Pl, double &Ql,
+                                           double &Wl)
+{
     const TPow p = make_tpow_known(T, inv, lnT);
     const double invRT = inv * (1.0 / kRUniv);
     const int sl = lane < NS ? lane : 0;
     const double egl = exp((h_species<NS>(ms, p, kRUniv, sl) - s_species<NS>(ms, p, kRUniv, sl) * T) * invRT);
-    const double iegl = rcp_nr(egl);
-    const int r = lane < NR ? lane : 0;
+    x.eg[lane] = egl;
+    x.ieg[lane] = rcp_nr(egl);
+    x.mc[lane] = lane_pick<NS>(mc, sl);
     const double invRuT = inv * (1.0 / kRuCal);
     const double rt_p0 = (kRUniv * T) / (kP0 * 1e-6);
     const double p0_rt = rcp_nr(rt_p0);
     double rrf = 1.0, rrb = 1.0, kc_inv = 1.0, rtb = 0.0;
-    const double b = ms.bf[r];
+    const double b = hl.bf;
     double kf;
-    if (ms.eaf[r] == 0.0 && (b == 0.0 || b == 1.0 || b == -1.0 || b == -2.0))
-        kf = ms.af[r] * (b == 0.0 ? 1.0 : b == 1.0 ? T : b == -1.0 ? p.inv : p.inv2);
+    if (hl.eaf == 0.0 && (b == 0.0 || b == 1.0 || b == -1.0 || b == -2.0))
+        kf = hl.af * (b == 0.0 ? 1.0 : b == 1.0 ? T : b == -1.0 ? p.inv : p.inv2);
     else
-        kf = ms.af[r] * exp(b * p.lnT - ms.eaf[r] * invRuT);
+        kf = hl.af * exp(b * p.lnT - hl.eaf * invRuT);
 #pragma unroll
-    for (int s = 0; s < NS; ++s) {
-        const double eg = __shfl_sync(0xffffffffu, egl, s), ieg = __shfl_sync(0xffffffffu, iegl, s);
-        const double f = ms.sf[r][s], bb = ms.sb[r][s];
-        rrf *= (f == 0.0 ? 1.0 : (f == 1.0 ? mc[s] : mc[s] * mc[s]));
-        rrb *= (bb == 0.0 ? 1.0 : (bb == 1.0 ? mc[s] : mc[s] * mc[s]));
-        const double d = bb - f;
-        kc_inv *= (d == 0.0 ? 1.0 : d == 1.0 ? eg : d == -1.0 ? ieg : d == 2.0 ? eg * eg : ieg * ieg);
-        rtb += mc[s] * ms.tb[r][s];
+    for (int s = 0; s < NS; ++s) rtb += mc[s] * tt.tb[s][lane];
+    __syncwarp();
+    // a fixed count without branches: every entry's loads issue together
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+        const unsigned e = tt.rent[i][lane];
+        const int s = int(e & 15u), fi = int((e >> 4) & 3u), bi = int(e >> 6);
+        const double m = x.mc[s], eg = x.eg[s], ieg = x.ieg[s];
+        rrf *= (fi == 0 ? 1.0 : (fi == 1 ? m : m * m));
+        rrb *= (bi == 0 ? 1.0 : (bi == 1 ? m : m * m));
+        const int d = bi - fi;
+        kc_inv *= (d == 0 ? 1.0 : d == 1 ? eg : d == -1 ? ieg : d == 2 ? eg * eg : ieg * ieg);
     }
-    const double Xr = ms.xr[r];
+    const double Xr = hl.xr;
     kc_inv *= (Xr == 0.0 ? 1.0 : Xr == 1.0 ? rt_p0 : p0_rt);
     if (rtb == 0.0)
         rtb = 1.0;
-    const double fwd = kf * rrf, bwd = kf * kc_inv * rrb;
+    const bool real = lane < NR; // slot 31 (and every slot past NR) holds zero rates
+    x.fwd[lane] = real ? kf * rrf : 0.0;
+    x.bwd[lane] = real ? kf * kc_inv * rrb : 0.0;
+    x.rtb[lane] = real ? rtb : 0.0;
+    __syncwarp();
     double P = 0.0, Q = 0.0, W = 0.0;
-    // unrolled: the shuffles of all reactions issue ahead of the sums, so a
-    // substep's latency is not NR shuffle round trips
 #pragma unroll
-    for (int q = 0; q < NR; ++q) {
-        const double fr = __shfl_sync(0xffffffffu, fwd, q);
-        const double br = __shfl_sync(0xffffffffu, bwd, q);
-        const double tr = __shfl_sync(0xffffffffu, rtb, q);
-        const double bb = ms.sb[q][sl], f = ms.sf[q][sl];
-        if (bb != 0.0 || f != 0.0) {
-            W += (bb - f) * tr * (fr - br);
-            Q += (bb * fr + f * br) * tr;
-            P += (bb * br + f * fr) * tr;
-        }
+    for (int i = 0; i < NR; ++i) {
+        const int q = tt.sent[i][lane];
+        const double bb = tt.sbv[i][lane], f = tt.sfv[i][lane];
+        const double fr = x.fwd[q], br = x.bwd[q], tr = x.rtb[q];
+        W += (bb - f) * tr * (fr - br);
+        Q += (bb * fr + f * br) * tr;
+        P += (bb * br + f * fr) * tr;
     }
+    __syncwarp(); // the buffers are free for the next evaluation
     Pl = P;
     Ql = Q;
-    Wl = ms.mw[sl] * W;
+    Wl = hl.mw * W;
+}
+
+// The scaled concentrations of a deferred cell: one multiplication by
+// 1e-3 / W_s per species instead of a division (within rounding of
+// scaled_concentrations).
+template <int NS, int NR>
+__device__ __forceinline__ void heavy_concentrations(const DevMech &m, const HeavyTablesT<NS, NR> &tt,
+                                                     const CellState<NS> &c, double (&mc)[NS])
+{
+#ifdef EU_EXACT_CHEM
+    scaled_concentrations<NS>(m, c, mc);
+#else
+#pragma unroll
+    for (int s = 0; s < NS; ++s) mc[s] = c.cs[s] * tt.imw[s];
+#endif
 }
 
 // One deferred cell advanced by a whole warp: lane r evaluates reaction r,
 // lane s owns species s's sums and trapezoid update, every lane rebuilds the
-// state (ms: the mechanism tables in shared memory).
+// state (ms: the mechanism tables in shared memory; hl, tt, x: see
+// warp_rates).
 template <int NS, int NR>
-__device__ __forceinline__ void react_heavy_cell(const DevMech &m, const DevMech &ms, const DevState &st, long long n3,
-                                                 long long c, double dtm, int max_substeps, int lane)
+__device__ __forceinline__ void react_heavy_cell(const DevMech &m, const DevMech &ms, const HeavyLane<NS, NR> &hl,
+                                                 const HeavyTablesT<NS, NR> &tt, HeavyScratch &x, const DevState &st,
+                                                 long long n3, long long c, double dtm, int max_substeps, int lane)
 {
     CellState<NS> cell;
     load_recovered<NS>(st, n3, c, cell);
@@ -1258,8 +1332,8 @@ __device__ __forceinline__ void react_heavy_cell(const DevMech &m, const DevMech
     // by the rebuild's Newton
     double inv = rcp_nr(cell.T), lnT = log(cell.T);
     double mc[NS], P, Q, W;
-    scaled_concentrations<NS>(m, cell, mc);
-    warp_rates<NS, NR>(ms, cell.T, inv, lnT, mc, lane, P, Q, W);
+    heavy_concentrations<NS, NR>(m, tt, cell, mc);
+    warp_rates<NS, NR>(ms, hl, tt, x, cell.T, inv, lnT, mc, lane, P, Q, W);
     // prediction: min over the species lanes, then every lane has Nchem
     double dt = dtm;
     if (lane < NS && lane_pick<NS>(cell.Y, lane) >= 1e-6 && W != 0)
@@ -1275,8 +1349,8 @@ __device__ __forceinline__ void react_heavy_cell(const DevMech &m, const DevMech
     const double dts = dtm / nchem, half = dts / 2.0;
     for (int step = 0; step < nchem; ++step) {
         if (step > 0) {
-            scaled_concentrations<NS>(m, cell, mc);
-            warp_rates<NS, NR>(ms, cell.T, inv, lnT, mc, lane, P, Q, W);
+            heavy_concentrations<NS, NR>(m, tt, cell, mc);
+            warp_rates<NS, NR>(ms, hl, tt, x, cell.T, inv, lnT, mc, lane, P, Q, W);
         }
         if (st.cms && lane < NS)
             st.cms[lane * n3 + c] = W * 1e3;
@@ -1284,7 +1358,7 @@ __device__ __forceinline__ void react_heavy_cell(const DevMech &m, const DevMech
         if (lane < NS) {
             const double di = lane_pick<NS + 4>(cell.cs, lane) * 1e-3;
             const double mcl = lane_pick<NS>(mc, lane);
-            const double qv = ms.mw[lane] * Q;
+            const double qv = hl.mw * Q;
 #ifdef EU_EXACT_CHEM
             const double pv = (mcl == 0) ? 0.0 : P / mcl;
             nd = ((1.0 - half * pv) * di + dts * qv) / (1.0 + half * pv) * 1e3;
@@ -1326,6 +1400,57 @@ __device__ __forceinline__ void copy_mech_to_shared(const DevMech &m, DevMech &m
     for (int w = threadIdx.x; w < int(sizeof(DevMech) / sizeof(int)); w += blockDim.x) dst[w] = src[w];
 }
 
+// The block's tables of the warp-per-cell kinetics: the mechanism and its
+// per-reaction tables transposed. Blocks are 128 threads: four warps, four
+// exchange buffers.
+template <int NS, int NR>
+struct HeavyShared {
+    DevMech ms;
+    HeavyTablesT<NS, NR> tt;
+    HeavyScratch x[4];
+};
+
+__device__ __forceinline__ unsigned coef2(double v) { return v <= 0.0 ? 0u : v <= 1.0 ? 1u : 2u; }
+
+template <int NS, int NR>
+__device__ __forceinline__ void heavy_shared_setup(const DevMech &m, HeavyShared<NS, NR> &sh)
+{
+    static_assert(NS <= 16 && NR <= 32, "4-bit species and 5-bit reaction indices");
+    copy_mech_to_shared(m, sh.ms);
+    HeavyTablesT<NS, NR> &t = sh.tt;
+    for (int i = threadIdx.x; i < NS * 32; i += blockDim.x) {
+        const int sp = i / 32, r = i % 32, rr = r < NR ? r : 0;
+        t.tb[sp][r] = m.tb[rr][sp];
+    }
+    if (threadIdx.x < NS)
+        t.imw[threadIdx.x] = 1e-3 / m.mw[threadIdx.x];
+    if (threadIdx.x < 32) { // lane l's lists
+        const int l = threadIdx.x, r = l < NR ? l : 0, sp = l < NS ? l : 0;
+        int n = 0;
+        for (int s = 0; s < NS; ++s) {
+            const unsigned fi = coef2(m.sf[r][s]), bi = coef2(m.sb[r][s]);
+            if (fi | bi)
+                t.rent[n++][l] = (unsigned char)(s | fi << 4 | bi << 6);
+        }
+        for (; n < NS; ++n) t.rent[n][l] = 0;
+        n = 0;
+        for (int q = 0; q < NR; ++q) {
+            const double bb = m.sb[q][sp], f = m.sf[q][sp];
+            if (bb != 0.0 || f != 0.0) {
+                t.sent[n][l] = (unsigned char)q;
+                t.sbv[n][l] = bb;
+                t.sfv[n][l] = f;
+                ++n;
+            }
+        }
+        for (; n < NR; ++n) {
+            t.sent[n][l] = 31;
+            t.sbv[n][l] = 0.0;
+            t.sfv[n][l] = 0.0;
+        }
+    }
+}
+
 // The order in which the warps of a persistent grid take deferred cells:
 // position p of n is entry p * s mod n, s near 0.618 n and coprime with n (a
 // bijection of [0, n)). The queue holds the cells in about the order the
@@ -1353,13 +1478,15 @@ __global__ void __launch_bounds__(128, 3) k_react_heavy(const __grid_constant__ 
                                                      const DevState st, const double *__restrict__ dt_dev,
                                                      int max_substeps)
 {
-    __shared__ DevMech ms;
+    __shared__ HeavyShared<NS, NR> sh;
     const int count = st.heavy[0];
     if (count == 0) // no deferred cell this step: skip the table copy
         return;
-    copy_mech_to_shared(m, ms);
+    heavy_shared_setup<NS, NR>(m, sh);
     __syncthreads();
     const int lane = threadIdx.x & 31;
+    const HeavyLane<NS, NR> hl = heavy_lane<NS, NR>(sh.ms, lane);
+    HeavyScratch &x = sh.x[threadIdx.x / 32];
     const double dtm = *dt_dev;
     const long long stride = scatter_stride(count);
     for (;;) {
@@ -1370,7 +1497,7 @@ __global__ void __launch_bounds__(128, 3) k_react_heavy(const __grid_constant__ 
         if (q >= count)
             break;
         const int e = int((q * stride) % count);
-        react_heavy_cell<NS, NR>(m, ms, st, g.n3, st.heavy[2 + e], dtm, max_substeps, lane);
+        react_heavy_cell<NS, NR>(m, sh.ms, hl, sh.tt, x, st, g.n3, st.heavy[2 + e], dtm, max_substeps, lane);
     }
 }
 
@@ -1381,15 +1508,17 @@ __global__ void __launch_bounds__(128, 3) k_react_heavy_batch(const __grid_const
                                                            const BatchCell *__restrict__ tab, int n, int *next,
                                                            int max_substeps)
 {
-    __shared__ DevMech ms;
+    __shared__ HeavyShared<NS, NR> sh;
     auto len = [&](int q) { return tab[q].st.heavy ? *(volatile const int *)tab[q].st.heavy : 0; };
     int total = 0;
     for (int q = 0; q < n; ++q) total += len(q);
     if (total == 0)
         return;
-    copy_mech_to_shared(m, ms);
+    heavy_shared_setup<NS, NR>(m, sh);
     __syncthreads();
     const int lane = threadIdx.x & 31;
+    const HeavyLane<NS, NR> hl = heavy_lane<NS, NR>(sh.ms, lane);
+    HeavyScratch &x = sh.x[threadIdx.x / 32];
     const long long stride = scatter_stride(total);
     for (;;) {
         int pos = 0;
@@ -1402,7 +1531,8 @@ __global__ void __launch_bounds__(128, 3) k_react_heavy_batch(const __grid_const
         const int q = batch_locate(n, int((pos * stride) % total), len, local);
         if (q < n) {
             const BatchCell &b = tab[q];
-            react_heavy_cell<NS, NR>(m, ms, b.st, b.n3, b.st.heavy[2 + local], *b.dt, max_substeps, lane);
+            react_heavy_cell<NS, NR>(m, sh.ms, hl, sh.tt, x, b.st, b.n3, b.st.heavy[2 + local], *b.dt, max_substeps,
+                                     lane);
         }
     }
 }
