@@ -47,11 +47,11 @@ __device__ __forceinline__ float tanh_approx(float x)
     asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
-__device__ __forceinline__ float silu_fast(float x)
-{
-    const float h = 0.5f * x;
-    return fmaf(h, tanh_approx(h), h);
-}
+// silu_fast(x) from h = x / 2. A caller that forms x = a + b can form h as
+// fmaf(0.5f, a, b / 2) in one instruction: scaling by 2^-1 commutes with
+// rounding, so h is bitwise 0.5f * (a + b) (outside the subnormal range).
+__device__ __forceinline__ float silu_fast_half(float h) { return fmaf(h, tanh_approx(h), h); }
+__device__ __forceinline__ float silu_fast(float x) { return silu_fast_half(0.5f * x); }
 __device__ __forceinline__ float silu_grad(float z)
 {
     const float s = 1.0f / (1.0f + __expf(-z));

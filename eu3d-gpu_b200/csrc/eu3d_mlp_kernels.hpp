@@ -10,8 +10,9 @@ namespace eu3d {
 // The fused inference kernel (eu3d_mlp_fused.cuh): model shape, packed weight
 // slabs and per-layer biases.
 constexpr int kFusedMaxMembers = 8, kFusedMaxLayers = 9, kFusedSlabK = 32;
-// weight-ring slots, rows per tile, jobs in flight; the opt-in shared-memory
-// limit of a block on sm_100 (227 KB)
+// weight-ring slots, rows per tile, tiles per job (each weight slab feeds
+// the MMAs of kFusedStreams tiles); the opt-in shared-memory limit of a
+// block on sm_100 (227 KB)
 constexpr int kFusedStages = 5, kFusedRows = 128, kFusedStreams = 2;
 constexpr size_t kFusedMaxSmem = 232448;
 struct FusedMlpParams {
@@ -30,15 +31,20 @@ inline size_t fused_bias_floats(int width, int out_pad, int layers)
     return size_t(layers - 1) * width + out_pad;
 }
 
+// Bytes of the feature scaling and output unscaling the fused kernel keeps in
+// shared memory: in_shift, in_scale [in_pad], out_shift, out_scale [out_pad].
+inline size_t fused_scaling_bytes(int in_pad, int out_pad) { return (size_t(2 * in_pad + 2 * out_pad) * 4 + 15) / 16 * 16; }
+
 // Bytes of shared memory the fused kernel needs for a model: the weight ring,
-// each stream's activations and features, the members' biases, the mbarriers.
-// At least 116 KB, so that one block (and its 512 TMEM columns) fits per SM.
+// each stream's activations and features, the members' biases, the scaling,
+// the mbarriers. At least 116 KB, so that one block (and its 512 TMEM
+// columns) fits per SM.
 inline size_t fused_smem_bytes(int in_pad, int width, int out_pad, int layers, int members)
 {
     const size_t bias = (size_t(members) * fused_bias_floats(width, out_pad, layers) * 4 + 15) / 16 * 16;
     const size_t need = size_t(kFusedStages) * width * kFusedSlabK * 2 +
                         size_t(kFusedStreams) * size_t(kFusedRows) * (size_t(width) + in_pad) * 2 + bias +
-                        8 * (2 * kFusedStages + 2 * kFusedStreams) + 16;
+                        fused_scaling_bytes(in_pad, out_pad) + 8 * (2 * kFusedStages + 2 * kFusedStreams) + 16;
     return need > 116 * 1024 ? need : 116 * 1024;
 }
 
@@ -50,6 +56,14 @@ inline bool fused_supported(int in_pad, int width, int out_pad, int members, int
     return width % 16 == 0 && width >= 16 && width <= 256 && in_pad <= 64 && out_pad <= width &&
            members >= 1 && members <= kFusedMaxMembers && layers >= 2 && layers <= kFusedMaxLayers &&
            fused_smem_bytes(in_pad, width, out_pad, layers, members) <= kFusedMaxSmem;
+}
+
+// CTAs of a fused launch over `tiles` 128-row tiles: one per tile pair, at
+// most one per SM.
+inline int fused_grid(long long tiles, int sms)
+{
+    const long long pairs = (tiles + kFusedStreams - 1) / kFusedStreams;
+    return int(pairs < sms ? pairs : sms);
 }
 
 // Predictions of every member for the first `count` rows of feat (count read

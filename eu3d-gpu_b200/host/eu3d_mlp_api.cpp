@@ -274,7 +274,7 @@ eu_status mlp_predict_queue(eu_mlp *m, const float *feat, const int *count_dev, 
     if (!mlp_fused_params(m, &p))
         return mfail(m, EU_ERR_UNSUPPORTED, "the model's shape has no fused inference kernel");
     const int tiles = (max_rows + 127) / 128;
-    const int grid = tiles < m->sms ? tiles : m->sms;
+    const int grid = eu3d::fused_grid(tiles, m->sms);
     MCK(m, eu3d::mlp_fused(p, feat, m->n_in, 0, count_dev, max_rows, out, s_row, s_mem, m->d_err, grid, s));
     return EU_OK;
 }
@@ -649,7 +649,7 @@ eu_status eu_mlp_predict_fused(eu_mlp *m, const float *X, long long n, float *ou
     eu3d::FusedMlpParams p;
     eu3d::mlp_fused_params(m, &p);
     const long long tiles = (n + 127) / 128;
-    const int grid = int(tiles < m->sms ? tiles : m->sms);
+    const int grid = eu3d::fused_grid(tiles, m->sms);
     MCK(m, eu3d::mlp_fused(p, X, m->n_in, int(n), nullptr, int(n), out, m->n_out, n * m->n_out, m->d_err, grid,
                            m->stream));
     return check_err(m);
@@ -667,7 +667,7 @@ eu_status eu_mlp_predict_fused_async(eu_mlp *m, const float *X, long long n, flo
     eu3d::FusedMlpParams p;
     eu3d::mlp_fused_params(m, &p);
     const long long tiles = (n + 127) / 128;
-    const int grid = int(tiles < m->sms ? tiles : m->sms);
+    const int grid = eu3d::fused_grid(tiles, m->sms);
     MCK(m, eu3d::mlp_fused(p, X, m->n_in, int(n), nullptr, int(n), out, m->n_out, n * m->n_out, m->d_err, grid,
                            m->stream));
     return EU_OK;
