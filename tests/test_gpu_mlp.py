@@ -118,3 +118,36 @@ def test_fused_inference_matches_layerwise(gpu, shape):
         m.predict_fused(X, b)
         torch.cuda.synchronize()
         assert torch.equal(a, b), (shape, n, (a - b).abs().max().item())
+
+
+def test_models_and_handles_on_two_devices(gpu):
+    """Kernels whose shared memory exceeds the 48 KB default have their limit
+    raised on every device they run on, not once per process: a model and a
+    step on the second GPU after the first both run and agree with the first
+    GPU's results (skipped with one visible GPU)."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two visible GPUs")
+    import eu3d_cases as cases
+    rng = np.random.default_rng(11)
+    X = rng.normal(size=(300, N_IN)).astype(np.float32)
+    mech = gpu.parse_mechanism(cases.MECH_JA919, cases.THERMO)
+    prim = cases.hot_reacting_block(20, 12, 12, mech["mw"], mech["ns"])
+    out = []
+    for dev in (0, 1):
+        m = gpu.Mlp(device=dev)
+        m.init(N_IN, WIDTH, HIDDEN, N_OUT, MEMBERS, max_batch=1024, seed=3)
+        with torch.cuda.device(dev):
+            xd = torch.from_numpy(X).cuda()
+            od = torch.zeros(MEMBERS, X.shape[0], N_OUT, device="cuda")
+            m.predict(xd, od)
+            pred = od.cpu().numpy()
+        s = gpu.Solver(16, 8, 8, (0.0, 0.016, 0.0, 0.008, 0.0, 0.008), precision="mixed", arith="fast", device=dev)
+        s.set_mechanism(mech)
+        s.set_primitive(*prim)
+        s.step(2, 2e-8)
+        out.append((pred, s.get("CS")))
+        s.close()
+        m.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
