@@ -1258,11 +1258,16 @@ __device__ __forceinline__ void warp_rates(const DevMech &ms, const HeavyLane<NS
     const double p0_rt = rcp_nr(rt_p0);
     double rrf = 1.0, rrb = 1.0, kc_inv = 1.0, rtb = 0.0;
     const double b = hl.bf;
-    double kf;
-    if (hl.eaf == 0.0 && (b == 0.0 || b == 1.0 || b == -1.0 || b == -2.0))
-        kf = hl.af * (b == 0.0 ? 1.0 : b == 1.0 ? T : b == -1.0 ? p.inv : p.inv2);
-    else
-        kf = hl.af * exp(b * p.lnT - hl.eaf * invRuT);
+    // Every candidate is formed before it is chosen, so the choices are
+    // selects: a conditional whose arms compute is a branch, and the lanes,
+    // holding different reactions and species, diverge on it.
+    const double kf_exp = hl.af * exp(b * p.lnT - hl.eaf * invRuT);
+    double tpow = 1.0;
+    tpow = b == 1.0 ? T : tpow;
+    tpow = b == -1.0 ? p.inv : tpow;
+    tpow = b == -2.0 ? p.inv2 : tpow;
+    const double kf_pow = hl.af * tpow;
+    const double kf = (hl.eaf == 0.0 && (b == 0.0 || b == 1.0 || b == -1.0 || b == -2.0)) ? kf_pow : kf_exp;
 #pragma unroll
     for (int s = 0; s < NS; ++s) rtb += mc[s] * tt.tb[s][lane];
     __syncwarp();
@@ -1272,10 +1277,18 @@ __device__ __forceinline__ void warp_rates(const DevMech &ms, const HeavyLane<NS
         const unsigned e = tt.rent[i][lane];
         const int s = int(e & 15u), fi = int((e >> 4) & 3u), bi = int(e >> 6);
         const double m = x.mc[s], eg = x.eg[s], ieg = x.ieg[s];
-        rrf *= (fi == 0 ? 1.0 : (fi == 1 ? m : m * m));
-        rrb *= (bi == 0 ? 1.0 : (bi == 1 ? m : m * m));
+        const double m2 = m * m, eg2 = eg * eg, ieg2 = ieg * ieg;
+        double ff = fi == 1 ? m : 1.0, fb = bi == 1 ? m : 1.0;
+        ff = fi == 2 ? m2 : ff;
+        fb = bi == 2 ? m2 : fb;
+        rrf *= ff;
+        rrb *= fb;
         const int d = bi - fi;
-        kc_inv *= (d == 0 ? 1.0 : d == 1 ? eg : d == -1 ? ieg : d == 2 ? eg * eg : ieg * ieg);
+        double fk = d == 1 ? eg : 1.0;
+        fk = d == -1 ? ieg : fk;
+        fk = d == 2 ? eg2 : fk;
+        fk = d == -2 ? ieg2 : fk;
+        kc_inv *= fk;
     }
     const double Xr = hl.xr;
     kc_inv *= (Xr == 0.0 ? 1.0 : Xr == 1.0 ? rt_p0 : p0_rt);
@@ -1363,8 +1376,10 @@ __device__ __forceinline__ void react_heavy_cell(const DevMech &m, const DevMech
             const double pv = (mcl == 0) ? 0.0 : P / mcl;
             nd = ((1.0 - half * pv) * di + dts * qv) / (1.0 + half * pv) * 1e3;
 #else
-            // refined reciprocals instead of IEEE divisions (1 + half pv >= 1)
-            const double pv = (mcl == 0) ? 0.0 : P * rcp_nr(mcl);
+            // refined reciprocals instead of IEEE divisions (1 + half pv >= 1);
+            // the reciprocal formed before the choice (a select, not a branch)
+            const double pq = P * rcp_nr(mcl);
+            const double pv = (mcl == 0) ? 0.0 : pq;
             nd = ((1.0 - half * pv) * di + dts * qv) * rcp_nr(1.0 + half * pv) * 1e3;
 #endif
         }
