@@ -683,7 +683,10 @@ __device__ __forceinline__ void trapezoid_substep(const DevMech &m, const Specie
     for (int s = 0; s < NS; ++s) {
         const double di = c.cs[s] * 1e-3;
         const double q = m.mw[s] * k.Q[s];
-        const double p = (mc[s] == 0) ? 0.0 : k.P[s] / mc[s];
+        // the quotient formed before the choice: a select, not a branch on
+        // which the threads (cells with and without the species) diverge
+        const double pq = k.P[s] / mc[s];
+        const double p = (mc[s] == 0) ? 0.0 : pq;
         const double nd = ((1.0 - half * p) * di + dts * q) / (1.0 + half * p) * 1e3;
         c.cs[s] = nd;
         D += nd;

@@ -667,11 +667,10 @@ __device__ __forceinline__ int predict_nchem(const DevMech &m, const CellState<N
     double dt = dtm;
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-        if (cell.Y[s] >= 1e-6 && rates.W[s] != 0) {
-            const double dt_temp = fabs(-(cell.cs[s] * 1e-3) / rates.W[s]);
-            if (dt_temp < dt)
-                dt = dt_temp;
-        }
+        // formed for every species, then chosen: a select instead of a branch
+        // that the cells diverge on
+        const double dt_temp = fabs(-(cell.cs[s] * 1e-3) / rates.W[s]);
+        dt = (cell.Y[s] >= 1e-6 && rates.W[s] != 0 && dt_temp < dt) ? dt_temp : dt;
     }
     return nchem_from_dt(dtm, dt, max_substeps, counters);
 }
