@@ -823,23 +823,29 @@ __device__ __forceinline__ void face_ausm(Get get, FOut (&F)[NS + 4])
         MaL = UnL * inv;
         MaR = UnR * inv;
     }
+    // Split Mach and pressure functions: both regimes formed, then selected
+    // (a branch per regime would split a warp whose faces straddle Mach 1)
     R B1, G1, B2, G2;
-    if (fabs(MaL) < R(1.0)) {
+    {
         const R a = MaL + R(1.0), t = MaL * MaL - R(1.0);
-        B1 = R(0.25) * (a * a) + R(0.125) * (t * t);
-        G1 = R(0.25) * (a * a) * (R(2.0) - MaL) + R(3.0) / R(16.0) * MaL * (t * t);
-    } else {
-        B1 = R(0.5) * (MaL + fabs(MaL));
-        // B1 / MaL is exactly 1 (MaL >= 1) or 0 (MaL <= -1)
-        G1 = kStrict ? B1 / MaL : (MaL > R(0) ? R(1) : R(0));
+        const R Bs = R(0.25) * (a * a) + R(0.125) * (t * t);
+        const R Gs = R(0.25) * (a * a) * (R(2.0) - MaL) + R(3.0) / R(16.0) * MaL * (t * t);
+        const R Bp = R(0.5) * (MaL + fabs(MaL));
+        // Bp / MaL is exactly 1 (MaL >= 1) or 0 (MaL <= -1)
+        const R Gp = kStrict ? Bp / MaL : (MaL > R(0) ? R(1) : R(0));
+        const bool sub = fabs(MaL) < R(1.0);
+        B1 = sub ? Bs : Bp;
+        G1 = sub ? Gs : Gp;
     }
-    if (fabs(MaR) < R(1.0)) {
+    {
         const R a = MaR - R(1.0), t = MaR * MaR - R(1.0);
-        B2 = -R(0.25) * (a * a) - R(0.125) * (t * t);
-        G2 = R(0.25) * (a * a) * (R(2.0) + MaR) - R(3.0) / R(16.0) * MaR * (t * t);
-    } else {
-        B2 = R(0.5) * (MaR - fabs(MaR));
-        G2 = kStrict ? B2 / MaR : (MaR < R(0) ? R(1) : R(0));
+        const R Bs = -R(0.25) * (a * a) - R(0.125) * (t * t);
+        const R Gs = R(0.25) * (a * a) * (R(2.0) + MaR) - R(3.0) / R(16.0) * MaR * (t * t);
+        const R Bp = R(0.5) * (MaR - fabs(MaR));
+        const R Gp = kStrict ? Bp / MaR : (MaR < R(0) ? R(1) : R(0));
+        const bool sub = fabs(MaR) < R(1.0);
+        B2 = sub ? Bs : Bp;
+        G2 = sub ? Gs : Gp;
     }
     const R MaI = B1 + B2;
     const R VI = MaI * CI;
