@@ -176,15 +176,16 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
                     tc::tc_fence_after();
                     const int kw = min(kFusedSlabK, K - s * kFusedSlabK);
                     const uint32_t b0 = tc::smem_u32(ring + slot * slot_bytes);
-                    // the slab feeds both tiles' MMAs
-                    for (int x = 0; x < kFusedStreams; ++x) {
-                        const uint32_t a0 = tc::smem_u32(l == 0 ? fin0 + x * fin_bytes : act0 + x * act_bytes);
-                        const uint32_t d = tmem + uint32_t(256 * x);
-                        for (int kk = 0; kk < kw / 16; ++kk) {
-                            const int kg = s * (kFusedSlabK / 16) + kk;
+                    // the slab feeds both tiles' MMAs, the tiles alternating so
+                    // that consecutive MMAs accumulate into different TMEM
+                    // columns (each tile's own MMAs keep their K order)
+                    for (int kk = 0; kk < kw / 16; ++kk) {
+                        const int kg = s * (kFusedSlabK / 16) + kk;
+                        const uint64_t bd = tc::smem_desc(b0 + kk * 2 * N * 16, N * 16, 128);
+                        for (int x = 0; x < kFusedStreams; ++x) {
+                            const uint32_t a0 = tc::smem_u32(l == 0 ? fin0 + x * fin_bytes : act0 + x * act_bytes);
                             const uint64_t ad = tc::smem_desc(a0 + kg * 2 * kFusedRows * 16, kFusedRows * 16, 128);
-                            const uint64_t bd = tc::smem_desc(b0 + kk * 2 * N * 16, N * 16, 128);
-                            tc::mma_bf16(d, ad, bd, idesc, (s > 0 || kk > 0) ? 1u : 0u);
+                            tc::mma_bf16(tmem + uint32_t(256 * x), ad, bd, idesc, (s > 0 || kk > 0) ? 1u : 0u);
                         }
                     }
                     tc::mma_commit(&empty[slot]);
