@@ -179,7 +179,7 @@ def test_deterministic(gpu):
 
 
 def test_mixed_stiff_heavy_cells_match_fp64(gpu):
-    """Igniting gas in mixed precision: cells whose predicted Nchem exceeds 16
+    """Igniting gas in mixed precision: cells whose predicted Nchem exceeds 4
     are advanced one warp per cell (k_react_heavy). Over 8 steps of a hot
     2H2+O2/N2 block (1300-2600 K, dt 2e-8 s) the run must reach such cells and
     stay within a species L1 (mean over cells of sum_s |dY_s|) of 1e-4 and a
@@ -198,7 +198,7 @@ def test_mixed_stiff_heavy_cells_match_fp64(gpu):
             peak[precision] = max(peak[precision], s.step(1, 2e-8)["max_nchem"])
         out[precision] = (interior(s.get("Yi")), interior(s.get("T")))
         s.close()
-    assert peak["mixed"] > 16, peak
+    assert peak["mixed"] > 4, peak
     l1 = np.abs(out["mixed"][0] - out["fp64"][0]).sum(axis=0)
     terr = np.abs(out["mixed"][1] - out["fp64"][1]) / out["fp64"][1]
     assert l1.mean() <= 1e-4 and terr.max() <= 1e-4, (l1.mean(), l1.max(), terr.max(), peak)
