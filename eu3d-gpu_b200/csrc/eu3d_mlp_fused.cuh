@@ -31,7 +31,9 @@
 // "accumulator full" mbarrier, on which the epilogue warps wait. While the
 // epilogue runs, the copy thread fills the ring with the next layer's slabs.
 // Weights stream through a five-slot shared-memory ring in K-slabs of 32
-// columns, pre-packed in global memory in the operands' core-matrix layout so
+// columns (the output layer, whose 16 x 256 weights fit one slot, as a single
+// slab: 2 % faster than eight 1 KB ones), pre-packed in global memory in the
+// operands' core-matrix layout so
 // that each slab is one contiguous bulk copy (cp.async.bulk, completion counted
 // on a "full" mbarrier); the MMAs that read a slot commit to its "empty"
 // mbarrier. Every wait is bounded and watches a shared abort flag: on a
@@ -64,9 +66,17 @@ __device__ __forceinline__ int fused_N(const FusedMlpParams &p, int l)
 {
     return l == p.layers - 1 ? p.out_pad : p.width;
 }
+// K columns per slab of layer l: kFusedSlabK, or the whole K for an output
+// layer whose weights fit one ring slot (one copy instead of K / kFusedSlabK
+// small ones). The packed layout is the same for any slab width.
+__device__ __forceinline__ int fused_slab_k(const FusedMlpParams &p, int l)
+{
+    return (l == p.layers - 1 && fused_N(p, l) * fused_K(p, l) <= p.width * kFusedSlabK) ? fused_K(p, l)
+                                                                                         : kFusedSlabK;
+}
 __device__ __forceinline__ int fused_slabs(const FusedMlpParams &p, int l)
 {
-    return (fused_K(p, l) + kFusedSlabK - 1) / kFusedSlabK;
+    return (fused_K(p, l) + fused_slab_k(p, l) - 1) / fused_slab_k(p, l);
 }
 
 // Bounded mbarrier wait that gives up early when another role has aborted.
@@ -165,7 +175,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
                     break;
                 }
                 tc::tc_fence_after();
-                const int N = fused_N(p, l), K = fused_K(p, l), ns = fused_slabs(p, l);
+                const int N = fused_N(p, l), K = fused_K(p, l), ns = fused_slabs(p, l), sk = fused_slab_k(p, l);
                 const uint32_t idesc = tc::idesc_bf16_f32(kFusedRows, N);
                 for (int s = 0; s < ns; ++s) {
                     const int slot = int(g % kFusedStages);
@@ -174,13 +184,13 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
                         break;
                     }
                     tc::tc_fence_after();
-                    const int kw = min(kFusedSlabK, K - s * kFusedSlabK);
+                    const int kw = min(sk, K - s * sk);
                     const uint32_t b0 = tc::smem_u32(ring + slot * slot_bytes);
                     // the slab feeds both tiles' MMAs, the tiles alternating so
                     // that consecutive MMAs accumulate into different TMEM
                     // columns (each tile's own MMAs keep their K order)
                     for (int kk = 0; kk < kw / 16; ++kk) {
-                        const int kg = s * (kFusedSlabK / 16) + kk;
+                        const int kg = s * (sk / 16) + kk;
                         const uint64_t bd = tc::smem_desc(b0 + kk * 2 * N * 16, N * 16, 128);
                         for (int x = 0; x < kFusedStreams; ++x) {
                             const uint32_t a0 = tc::smem_u32(l == 0 ? fin0 + x * fin_bytes : act0 + x * act_bytes);
@@ -211,7 +221,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
             bool ok = true;
             for (int step = 0; ok && step < nsteps; ++step) {
                 const int l = step % p.layers, e = (step / p.layers) % p.members;
-                const int N = fused_N(p, l), K = fused_K(p, l);
+                const int N = fused_N(p, l), K = fused_K(p, l), sk = fused_slab_k(p, l);
                 for (int ps = 0; ps < fused_slabs(p, l); ++ps) {
                     const int slot = int(gp % kFusedStages);
                     if (gp >= kFusedStages &&
@@ -219,10 +229,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
                         ok = false;
                         break;
                     }
-                    const int k0 = ps * kFusedSlabK, kw = min(kFusedSlabK, K - k0);
+                    const int k0 = ps * sk, kw = min(sk, K - k0);
                     const uint32_t bytes = uint32_t(N) * kw * 2;
                     const __nv_bfloat16 *src = static_cast<const __nv_bfloat16 *>(p.slabs) + p.off[e][l] +
-                                               (long long)ps * N * kFusedSlabK;
+                                               (long long)ps * N * sk;
                     tc::mbar_arrive_expect_tx(&full[slot], bytes);
                     tc::bulk_g2s(ring + slot * slot_bytes, src, bytes, &full[slot]);
                     ++gp;
