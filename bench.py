@@ -903,6 +903,8 @@ def our_arm(args):
                         profile=profile)
         s.set_mechanism(mech)
         s.set_state(state)
+        # every arm the same way; the benchmark reads interior nodes only
+        s.set_ghost_mode(args.ghosts)
         if chem == "learned":
             import learned
             learned.attach(s, model, gate)
@@ -1069,6 +1071,7 @@ def our_arm(args):
                                              "runs through the bubble gas"},
                            "precision": args.precision, "chemistry": args.chem,
                            "arith": args.arith, "parallelism": f"replicas x{world}", "autotune": tuned,
+                           "ghosts": args.ghosts,
                            "l2": f"inputs larger than L2: {sd['CS'].nbytes * 3 // 2**20} MiB state > 126 MiB"},
                 "window_state": {**window,
                                  "note": "the transmitted shock heats the bubble gas to about 600 K and the "
@@ -1134,6 +1137,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched uneven-instance workload")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
+    ap.add_argument("--ghosts", choices=["reference", "stored"], default="stored",
+                    help="z-face ghosts formed by the ghost fill (the reference's placement) or stored with the "
+                         "interior (eu_set_ghost_mode; the same interior state)")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)

@@ -82,6 +82,8 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ DevMec
         // the ghost index runs fastest: the 2 bc ghosts of one (i, j) row sit in
         // two contiguous pairs, so a warp touches 16 pairs instead of 32 rows
         t -= nxf + nyf;
+        if (st.zm_fresh && *st.zm_fresh) // EU_GHOSTS_STORED: stored with the interior
+            return;
         const int jq = fdiv(t, g.d_ghost), ii = fdiv(t, g.d_ghost_nj);
         const int q = int(t - (long long)jq * (2 * bc));
         const int j = bc + (jq - ii * nj);
@@ -609,6 +611,41 @@ __device__ __forceinline__ void store_cell(const DevMech &m, const DevState &st,
     st.E[c] = cell.E;
     if (!(isfinite(cell.D) && isfinite(cell.T)))
         atomicAdd(&st.counters[kCntNonfinite], 1ULL);
+    if (st.zm_fresh) {
+        // EU_GHOSTS_STORED: the z-face ghosts this node is the mirror source
+        // of (k_boundary's z faces: ghost 2 bc - 1 - k below, 2 (nk + bc) - 1 -
+        // k above, W reflected), the values the ghost fill would copy, in the
+        // same 32-byte sectors as the node's own stores
+        const long long row = fdiv(c, st.zm_dnz);
+        const int k = int(c - row * st.zm_nz), bc = st.zm_bc, nk = st.zm_nk;
+        auto mirror = [&](long long gc) {
+            if (st.prim32) {
+#pragma unroll
+                for (int f = 0; f < 7; ++f) st.prim32[f * n3 + gc] = float(f == kW ? -v[f] : v[f]);
+#pragma unroll
+                for (int s = 0; s < NS; ++s) st.prim32[(kY0 + s) * n3 + gc] = float(cell.Y[s]);
+            } else {
+#pragma unroll
+                for (int f = 0; f < 7; ++f) st.prim[f * n3 + gc] = f == kW ? -v[f] : v[f];
+#pragma unroll
+                for (int s = 0; s < NS; ++s) st.prim[(kY0 + s) * n3 + gc] = cell.Y[s];
+            }
+            st.T[gc] = cell.T;
+        };
+        if (k < 2 * bc)
+            mirror(c + (2 * bc - 1 - 2 * k));
+        if (k >= nk)
+            mirror(c + (2 * (nk + bc) - 1 - 2 * k));
+    }
+}
+
+// EU_GHOSTS_STORED: a recovery that stores every interior node has written
+// every z-face ghost, so the next ghost fill (after it in stream order) may
+// skip the z faces.
+__device__ __forceinline__ void mark_z_fresh(const DevState &st)
+{
+    if (st.zm_fresh && blockIdx.x == 0 && threadIdx.x == 0)
+        *st.zm_fresh = 1;
 }
 
 // Post-advection state recovery (Flowfield::Update_after_Adv ->
@@ -830,6 +867,7 @@ __global__ void __launch_bounds__(128, MINB) k_recover_react(const __grid_consta
 {
     const long long ncell = (long long)g.ni * g.nj * g.nk;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    mark_z_fresh(st);
     if (t >= ncell)
         return;
     int i, j, k;
@@ -867,6 +905,7 @@ __global__ void __launch_bounds__(128, MINB) k_recover_classify(const __grid_con
 {
     const long long ncell = (long long)g.ni * g.nj * g.nk;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    mark_z_fresh(st);
     bool active = false;
     long long c = 0;
     if (t < ncell) {

@@ -75,6 +75,13 @@ struct DevState {
     unsigned long long *counters; // see CounterIdx
     int *heavy;       // mixed precision: {count, next, cells...} of cells left to the warp-per-cell kinetics
     const double *inflow; // ODW x-low ghost values per interior (j, k): 7 + ns primitive planes, then T
+    // EU_GHOSTS_STORED: store_cell also writes the z-face ghosts a node is the
+    // mirror source of (W reflected), and the ghost fill skips the z faces while
+    // *zm_fresh is set (by each full recovery; cleared by host uploads). Null:
+    // the ghost fill forms every face, as the reference does.
+    int *zm_fresh;
+    FastDiv zm_dnz; // nz, the node row length along z
+    int zm_nz, zm_nk, zm_bc;
 };
 
 // Device counters. The first kCntPerStep are statistics of the latest step

@@ -120,6 +120,8 @@ def library():
         lib.eu_set_time_scheme.restype = _I
         lib.eu_set_odw_wall.argtypes = [_P, _I]
         lib.eu_set_odw_wall.restype = _I
+        lib.eu_set_ghost_mode.argtypes = [_P, _I]
+        lib.eu_set_ghost_mode.restype = _I
         lib.eu_output_async.argtypes = [_P, _I, ctypes.c_char_p, _I, _I, _D, _D]
         lib.eu_output_async.restype = _I
         lib.eu_output_wait.argtypes = [_P]
@@ -357,6 +359,13 @@ class Solver:
         """Advection time scheme: "ee" (the reference's Euler explicit) or
         "rk3" (three-stage TVD Runge-Kutta; eu_set_time_scheme)."""
         self._check(library().eu_set_time_scheme(self.h, {"ee": 0, "rk3": 1}[scheme]), "set_time_scheme")
+
+    def set_ghost_mode(self, mode):
+        """Where the z-face ghost nodes are formed (eu_set_ghost_mode):
+        "reference" (the ghost fill at each step's start, the reference's
+        outputs) or "stored" (written with each stored interior node; the same
+        interior state, the z ghosts mirroring the step's end)."""
+        self._check(library().eu_set_ghost_mode(self.h, {"reference": 0, "stored": 1}[mode]), "set_ghost_mode")
 
     def set_odw_wall(self, first_wall_node):
         """EU_BC_ODW: the y-low wall starts at this global x node; the face

@@ -57,6 +57,7 @@ struct eu_handle {
     // mixed precision: the timestep keeps only the FP32 primitive planes
     // current; the FP64 ones are formed on demand (k_materialize) for output
     bool prim_stale = false;
+    int *d_zm_fresh = nullptr; // EU_GHOSTS_STORED's flag (eu_set_ghost_mode)
     int sms = 0;
     // one timestep captured as a CUDA graph (recaptured when what its kernels
     // take by value changes: the mechanism, the learned-chemistry settings)
@@ -625,6 +626,8 @@ eu_status eu_set_state(eu_handle *h, const double *cs, const double *T, const do
     CK(h, cudaMemcpyAsync(h->st.E, E, b, cudaMemcpyHostToDevice, h->stream));
     if (h->st.prim32) // the FP32 planes the mixed-precision fluxes read, converted on the device
         CK(h, strict::launch_to_f32(h->st.prim, h->st.prim32, (long long)(7 + ns) * n3, h->stream));
+    if (h->st.zm_fresh) // EU_GHOSTS_STORED: the uploaded ghosts are the caller's; the next fill forms the z faces
+        CK(h, cudaMemsetAsync(h->st.zm_fresh, 0, sizeof(int), h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
     h->has_state = true;
     h->prim_stale = false;
@@ -714,6 +717,40 @@ eu_status eu_set_time_scheme(eu_handle *h, int scheme)
     }
     h->time_scheme = scheme;
     h->graph_dirty = true;
+    return EU_OK;
+}
+
+eu_status eu_set_ghost_mode(eu_handle *h, int mode)
+{
+    if (!h)
+        return EU_ERR_INVALID_ARGUMENT;
+    if (mode != EU_GHOSTS_REFERENCE && mode != EU_GHOSTS_STORED)
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "unknown ghost mode %d", mode);
+    if (!h->has_mech)
+        return fail(h, EU_ERR_NOT_READY, "load a mechanism first");
+    if (mode == EU_GHOSTS_STORED && (h->g.bc_kind == EU_BC_ODW || h->nk < h->bc))
+        // the ODW fill rebuilds the z ghosts' thermo; with fewer than bc
+        // interior z nodes a z ghost mirrors another ghost
+        return fail(h, EU_ERR_INVALID_ARGUMENT, "stored z ghosts need the RSBI or ZND fill and nk >= %d", h->bc);
+    cudaSetDevice(h->cfg.device);
+    if (mode == EU_GHOSTS_STORED) {
+        if (!h->d_zm_fresh) {
+            eu_status st = dalloc(h, &h->d_zm_fresh, size_t(1));
+            if (st != EU_OK)
+                return st;
+        }
+        // the ghosts as they stand are the ghost fill's: the next fill forms the z faces
+        CK(h, cudaMemsetAsync(h->d_zm_fresh, 0, sizeof(int), h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        h->st.zm_fresh = h->d_zm_fresh;
+        h->st.zm_dnz = make_fastdiv(unsigned(h->nz));
+        h->st.zm_nz = int(h->nz);
+        h->st.zm_nk = h->nk;
+        h->st.zm_bc = h->bc;
+    } else {
+        h->st.zm_fresh = nullptr;
+    }
+    h->graph_dirty = true; // the kernels take the state by value
     return EU_OK;
 }
 
@@ -2159,6 +2196,8 @@ eu_status eu_autotune(eu_handle *h, int reps, eu_tune_report *report)
         parts.push_back({h->st.prim32, size_t(7 + ns) * n3 * 4});
     if (h->st.cms) // the stiff kinetics records its sources
         parts.push_back({h->st.cms, size_t(ns) * n3 * 8});
+    if (h->st.zm_fresh) // whether the restored z ghosts match their interior
+        parts.push_back({h->st.zm_fresh, sizeof(int)});
     size_t total = 0;
     for (const Part &q : parts) total += q.bytes;
     unsigned char *snap = nullptr;

@@ -229,6 +229,23 @@ eu_status eu_set_inflow(eu_handle *h, const double *P, const double *T, const do
 #define EU_TIME_RK3 1
 eu_status eu_set_time_scheme(eu_handle *h, int scheme);
 
+/* Where the z-face ghost nodes are formed (no counterpart in the reference).
+ * EU_GHOSTS_REFERENCE (default): by the ghost fill at the start of each step,
+ * as FieldBoundary_3dRSBI does (src/Flowfield.cpp:710-802), so after a step
+ * every ghost node mirrors the interior as it was when the step began, which
+ * is what the reference's outputs show. EU_GHOSTS_STORED: each stored
+ * interior node also writes the z ghosts it is the mirror source of, and the
+ * next ghost fill skips the z faces (whose mirror copies touch two 32-byte
+ * sectors per row for 16 useful bytes); the interior state is bitwise the
+ * same, but after a step the z-face ghost nodes mirror the interior as it is
+ * at the step's end, so outputs that include ghost nodes (eu_get_field,
+ * eu_write_state, eu_write_tecplot) differ from the reference's there. Needs
+ * the RSBI or ZND fill and at least bc interior z nodes; set it before
+ * creating a batch that holds the handle. */
+#define EU_GHOSTS_REFERENCE 0
+#define EU_GHOSTS_STORED 1
+eu_status eu_set_ghost_mode(eu_handle *h, int mode);
+
 /* EU_BC_ODW: where the wall begins on the y-low face. The ghost nodes of the
  * y-low face below global x node first_wall_node take the freestream (the
  * first row of the eu_set_inflow tables, per k) instead of the reflecting
